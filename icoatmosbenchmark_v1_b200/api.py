@@ -1,0 +1,219 @@
+"""Python host interface over libicoadv.so (the C ABI in include/icoadv.h).
+
+Method names, argument order and meaning follow the reference subroutines:
+
+    horizontal_flux            kernels/NICAM/dyn_horiz_adv_flux/src/mod_src_tracer.f90:42-49
+    horizontal_limiter_thuburn kernels/NICAM/dyn_horiz_adv_limiter/src/mod_src_tracer.f90:42-49
+    vertical_limiter_thuburn   kernels/NICAM/dyn_vert_adv_limiter/src/mod_src_tracer.f90:41-45
+    COMM_data_transfer         kernels/NICAM/communication/src/mod_comm.f90:1506-1508
+    COMM_var                   kernels/NICAM/communication/src/mod_comm.f90:1895-1899
+
+Arrays are numpy (host) or torch CUDA tensors (device), C-contiguous, in the
+reference's Fortran layout written in C order: var(gall,kall,lall,m) has
+shape (m, lall, kall, gall).  Host arrays go through the host-pointer entry
+points (copy in, run, copy out); CUDA tensors go through the *_dev entry
+points on the context's stream.  Errors raise IcoAdvError with the library's
+message.  There is no CPU fallback: without the built library or a B200 the
+calls fail.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libicoadv.so"
+_lib = None
+
+ICA_OK = 0
+ERRORS = {-1: "ICA_ERR_ARG", -2: "ICA_ERR_STATE", -3: "ICA_ERR_CUDA", -4: "ICA_ERR_TIMEOUT",
+          -5: "ICA_ERR_INTERNAL", -6: "ICA_ERR_NOMEM"}
+
+
+class IcoAdvError(RuntimeError):
+    def __init__(self, fn, rc):
+        self.rc = rc
+        super().__init__(f"{fn} failed: {ERRORS.get(rc, rc)}: {lib().ica_last_error().decode()}")
+
+
+class Dims(C.Structure):
+    _fields_ = [("glevel", C.c_int), ("rlevel", C.c_int), ("vlayer", C.c_int), ("device", C.c_int)]
+
+
+class Sizes(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("gall_1d", "gall", "gmin", "gmax", "kall", "kmin", "kmax",
+                                       "lall", "gall_pl", "lall_pl")]
+
+
+def lib():
+    """Loads libicoadv.so (built in-tree by icoatmosbenchmark_v1_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is not built; run icoatmosbenchmark_v1_b200.build.build()")
+        _lib = C.CDLL(str(LIB_PATH))
+        _lib.ica_last_error.restype = C.c_char_p
+        _lib.ica_stream.restype = C.c_void_p
+        _lib.ica_stream.argtypes = [C.c_void_p]
+        _lib.ica_launch_count.restype = C.c_longlong
+        _lib.ica_launch_count.argtypes = [C.c_void_p]
+        _lib.ica_init.argtypes = [C.POINTER(Dims), C.POINTER(C.c_void_p)]
+        _lib.ica_finalize.argtypes = [C.c_void_p]
+        _lib.ica_get_sizes.argtypes = [C.c_void_p, C.POINTER(Sizes)]
+    return _lib
+
+
+def exported_symbols():
+    """Names of the functions declared in include/icoadv.h."""
+    import re
+    text = (PKG.parent / "include" / "icoadv.h").read_text()
+    return sorted(set(re.findall(r"^(?:int|void|const char|long long)[\s*]+(ica_\w+)\s*\(", text, re.M)))
+
+
+def _check(fn, rc):
+    if rc != ICA_OK:
+        raise IcoAdvError(fn, rc)
+
+
+# ---- host-only topology helpers ------------------------------------------------
+def comm_plan(glevel, rlevel, pole_fill=False):
+    """Composed single-process halo fill: arrays (dst, src) of point indices."""
+    n = C.c_int(0)
+    _check("ica_comm_plan", lib().ica_comm_plan(glevel, rlevel, int(pole_fill), C.byref(n), None, None))
+    dst = np.zeros(n.value, np.int32)
+    src = np.zeros(n.value, np.int32)
+    _check("ica_comm_plan", lib().ica_comm_plan(glevel, rlevel, int(pole_fill), C.byref(n),
+                                                dst.ctypes.data_as(C.POINTER(C.c_int)),
+                                                src.ctypes.data_as(C.POINTER(C.c_int))))
+    return dst, src
+
+
+def topology_info(glevel, rlevel):
+    nr = 10 * 4 ** rlevel
+    sgp = np.zeros(nr, np.int32)
+    r4 = np.zeros(2, np.int32)
+    ring = np.zeros((2, 5), np.int32)
+    ip = C.POINTER(C.c_int)
+    _check("ica_topology_info", lib().ica_topology_info(glevel, rlevel, sgp.ctypes.data_as(ip),
+                                                        r4.ctypes.data_as(ip), ring.ctypes.data_as(ip)))
+    return sgp, r4, ring
+
+
+def apply_plan_numpy(plan, var, var_pl):
+    """Host-side application of a plan (used to fill halos of synthetic inputs)."""
+    dst, src = plan
+    m, L, K, G = var.shape
+    flat = np.concatenate([var.transpose(0, 2, 1, 3).reshape(m, K, L * G),
+                           var_pl.transpose(0, 2, 1, 3).reshape(m, K, 12)], axis=2)
+    flat[:, :, dst] = flat[:, :, src]
+    var[...] = flat[:, :, :L * G].reshape(m, K, L, G).transpose(0, 2, 1, 3)
+    var_pl[...] = flat[:, :, L * G:].reshape(m, K, 2, 6).transpose(0, 2, 1, 3)
+
+
+# ---- the context ------------------------------------------------------------------
+def _ptr(a, want):
+    """Pointer of a numpy array (host) or a torch CUDA tensor (device)."""
+    if a is None:
+        return None, None
+    if isinstance(a, np.ndarray):
+        if a.dtype != want or not a.flags.c_contiguous:
+            raise TypeError(f"expected C-contiguous {want} array, got {a.dtype}")
+        return a.ctypes.data_as(C.c_void_p), False
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        raise TypeError("unsupported array type")
+    if isinstance(a, torch.Tensor):
+        tw = {np.float64: torch.float64, np.float32: torch.float32}[np.dtype(want).type]
+        if a.dtype != tw or not a.is_contiguous() or not a.is_cuda:
+            raise TypeError(f"expected contiguous CUDA tensor of {tw}, got {a.dtype} on {a.device}")
+        return C.c_void_p(a.data_ptr()), True
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+class IcoAdv:
+    """One grid on one GPU: ADM sizes, metrics, halo plan and a CUDA stream."""
+
+    def __init__(self, glevel, rlevel, vlayer, device=0):
+        self.h = C.c_void_p()
+        d = Dims(glevel, rlevel, vlayer, device)
+        _check("ica_init", lib().ica_init(C.byref(d), C.byref(self.h)))
+        s = Sizes()
+        _check("ica_get_sizes", lib().ica_get_sizes(self.h, C.byref(s)))
+        self.sizes = s
+        self.glevel, self.rlevel, self.vlayer, self.device = glevel, rlevel, vlayer, device
+
+    def close(self):
+        if self.h:
+            lib().ica_finalize(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return lib().ica_stream(self.h)
+
+    @property
+    def launch_count(self):
+        return lib().ica_launch_count(self.h)
+
+    def set_geometry(self, GRD_xr, GRD_xr_pl, GMTR_p, GMTR_p_pl, GMTR_t, GMTR_t_pl, GMTR_a, GMTR_a_pl):
+        args = [_ptr(np.ascontiguousarray(a, np.float64), np.float64)[0]
+                for a in (GRD_xr, GRD_xr_pl, GMTR_p, GMTR_p_pl, GMTR_t, GMTR_t_pl, GMTR_a, GMTR_a_pl)]
+        _check("ica_set_geometry", lib().ica_set_geometry(self.h, *args))
+
+    def _call(self, name, dtype, arrays, *scalars):
+        ptrs, kinds = zip(*[_ptr(a, dtype) for a in arrays])
+        dev = {k for k in kinds if k is not None}
+        if len(dev) != 1:
+            raise TypeError("mix of host and device arrays")
+        dev = dev.pop()
+        suffix = "_dev" if dev else ""
+        if dtype == np.float32:
+            if dev:
+                raise TypeError(f"{name}: FP32 entry points take host arrays")
+            suffix = "_f32"
+        fn = getattr(lib(), name + suffix)
+        _check(name + suffix, fn(self.h, *ptrs, *scalars))
+
+    @staticmethod
+    def _dtype(a):
+        if isinstance(a, np.ndarray):
+            return a.dtype.type
+        import torch
+        return {torch.float64: np.float64, torch.float32: np.float32}[a.dtype]
+
+    def horizontal_flux(self, flx_h, flx_h_pl, GRD_xc, GRD_xc_pl, rho, rho_pl, rhovx, rhovx_pl,
+                        rhovy, rhovy_pl, rhovz, rhovz_pl, dt):
+        t = self._dtype(rho)
+        sc = C.c_double(dt) if t == np.float64 else C.c_float(dt)
+        self._call("ica_horizontal_flux", t, [flx_h, flx_h_pl, GRD_xc, GRD_xc_pl, rho, rho_pl, rhovx, rhovx_pl,
+                                              rhovy, rhovy_pl, rhovz, rhovz_pl], sc)
+
+    def horizontal_limiter_thuburn(self, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask_pl,
+                                   Qout_prev, Qout_prev_pl, Qout_post=None, Qout_post_pl=None):
+        t = self._dtype(q)
+        arrs = [q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask_pl, Qout_prev, Qout_prev_pl]
+        ptrs, kinds = zip(*[_ptr(a, t) for a in arrs])
+        post = [_ptr(Qout_post, t)[0], _ptr(Qout_post_pl, t)[0]]
+        dev = kinds[0]
+        name = "ica_horizontal_limiter_thuburn" + ("_dev" if dev else ("_f32" if t == np.float32 else ""))
+        _check(name, getattr(lib(), name)(self.h, *ptrs, *post))
+
+    def vertical_limiter_thuburn(self, q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl):
+        self._call("ica_vertical_limiter_thuburn", self._dtype(q), [q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl])
+
+    def COMM_data_transfer(self, var, var_pl):
+        vmax, _, kmax, _ = var.shape
+        self._call("ica_comm_data_transfer", self._dtype(var), [var, var_pl], int(kmax), int(vmax))
+
+    def COMM_var(self, var, var_pl):
+        vmax, _, kmax, _ = var.shape
+        self._call("ica_comm_var", self._dtype(var), [var, var_pl], int(kmax), int(vmax))

@@ -1,0 +1,481 @@
+// C ABI of the library: context, metrics registration and the drop-in entry
+// points that keep the reference subroutines' argument lists.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "capi_internal.h"
+
+namespace icoadv {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int cuda_fail(cudaError_t e, const char *what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return ICA_ERR_CUDA;
+}
+
+void *Ctx::buf(const char *name, size_t bytes) {
+  DevBuf &b = bufs[name];
+  if (b.bytes < bytes) {
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    if (cudaMalloc(&b.ptr, bytes ? bytes : 16) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    b.bytes = bytes;
+  }
+  return b.ptr;
+}
+
+int Ctx::check_launch(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  return ICA_OK;
+}
+
+}  // namespace icoadv
+
+using namespace icoadv;
+
+struct ica_ctx : public Ctx {};
+
+extern "C" {
+
+const char *ica_last_error(void) { return icoadv::g_last_error.c_str(); }
+
+int ica_device_check(int device) {
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+  if (prop.major != 10 || prop.minor != 0) {
+    set_error("device is not sm_100 (this library is built for sm_100a only)");
+    return ICA_ERR_STATE;
+  }
+  return ICA_OK;
+}
+
+int ica_init(const ica_dims *dims, ica_ctx **out) {
+  if (!dims || !out) return set_error("ica_init: NULL argument"), ICA_ERR_ARG;
+  *out = nullptr;
+  if (dims->glevel < 1 || dims->glevel > 11 || dims->rlevel < 0 || dims->rlevel > dims->glevel ||
+      dims->vlayer < 1 || dims->vlayer > 4094)
+    return set_error("ica_init: glevel/rlevel/vlayer out of range"), ICA_ERR_ARG;
+  cudaError_t e = cudaSetDevice(dims->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  int rc = ica_device_check(dims->device);
+  if (rc) return rc;
+  ica_ctx *c = new ica_ctx();
+  c->topo.reset(new Topology(dims->glevel, dims->rlevel));
+  const Topology &t = *c->topo;
+  c->device = dims->device;
+  ica_sizes &s = c->sz;
+  s.gall_1d = t.gall_1d;
+  s.gall = t.gall;
+  s.gmin = t.gmin;
+  s.gmax = t.gmax;
+  if (dims->vlayer == 1) s.kall = s.kmin = s.kmax = 1;
+  else s.kall = dims->vlayer + 2, s.kmin = 2, s.kmax = dims->vlayer + 1;
+  s.lall = t.nrgn;
+  s.gall_pl = kGallPl;
+  s.lall_pl = kLallPl;
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
+  for (int pf = 0; pf < 2; ++pf) {
+    std::vector<int> d, sr;
+    rc = t.build_plan(pf != 0, d, sr);
+    if (rc) { delete c; return set_error("halo plan: a source is also a destination"), rc; }
+    Plan &p = c->plan[pf];
+    p.n = (int)d.size();
+    if (cudaMalloc(&p.dst, sizeof(int) * (p.n + 1)) != cudaSuccess ||
+        cudaMalloc(&p.src, sizeof(int) * (p.n + 1)) != cudaSuccess) {
+      delete c;
+      return set_error("cudaMalloc(plan)"), ICA_ERR_NOMEM;
+    }
+    cudaMemcpy(p.dst, d.data(), sizeof(int) * p.n, cudaMemcpyHostToDevice);
+    cudaMemcpy(p.src, sr.data(), sizeof(int) * p.n, cudaMemcpyHostToDevice);
+  }
+  if (cudaMalloc(&c->d_have_sgp, sizeof(int) * t.nrgn) != cudaSuccess) {
+    delete c;
+    return set_error("cudaMalloc(have_sgp)"), ICA_ERR_NOMEM;
+  }
+  cudaMemcpy(c->d_have_sgp, t.have_sgp.data(), sizeof(int) * t.nrgn, cudaMemcpyHostToDevice);
+  c->D.gall_1d = s.gall_1d;
+  c->D.gall = s.gall;
+  c->D.gmin = s.gmin;
+  c->D.gmax = s.gmax;
+  c->D.kall = s.kall;
+  c->D.kmin = s.kmin;
+  c->D.kmax = s.kmax;
+  c->D.lall = s.lall;
+  c->D.have_sgp = c->d_have_sgp;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { delete c; return cuda_fail(e, "ica_init"); }
+  *out = c;
+  return ICA_OK;
+}
+
+int ica_finalize(ica_ctx *c) {
+  if (!c) return ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete c;
+  return ICA_OK;
+}
+
+int ica_get_sizes(const ica_ctx *c, ica_sizes *out) {
+  if (!c || !out) return ICA_ERR_ARG;
+  *out = c->sz;
+  return ICA_OK;
+}
+
+void *ica_stream(ica_ctx *c) { return c ? (void *)c->stream : nullptr; }
+long long ica_launch_count(const ica_ctx *c) { return c ? c->launches : -1; }
+
+int ica_set_geometry(ica_ctx *c, const double *GRD_xr, const double *GRD_xr_pl, const double *GMTR_p,
+                     const double *GMTR_p_pl, const double *GMTR_t, const double *GMTR_t_pl, const double *GMTR_a,
+                     const double *GMTR_a_pl) {
+  if (!c || !GRD_xr || !GRD_xr_pl || !GMTR_p || !GMTR_p_pl || !GMTR_t || !GMTR_t_pl || !GMTR_a || !GMTR_a_pl)
+    return set_error("ica_set_geometry: NULL argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t gl = (size_t)c->sz.gall * c->sz.lall, pl = (size_t)kGallPl * kLallPl;
+  const double *h[8] = {GRD_xr, GRD_xr_pl, GMTR_p, GMTR_p_pl, GMTR_t, GMTR_t_pl, GMTR_a, GMTR_a_pl};
+  const size_t n[8] = {gl * 9, pl * 3, gl * 8, pl * 8, gl * 10, pl * 5, gl * 36, pl * 18};
+  return c->upload_geometry(h, n);
+}
+
+}  // extern "C"
+
+namespace icoadv {
+
+Ctx::~Ctx() {
+  for (auto &kv : bufs)
+    if (kv.second.ptr) cudaFree(kv.second.ptr);
+  for (auto &p : plan) {
+    if (p.dst) cudaFree(p.dst);
+    if (p.src) cudaFree(p.src);
+  }
+  for (int i = 0; i < 8; ++i) {
+    if (geo64[i]) cudaFree(geo64[i]);
+    if (geo32[i]) cudaFree(geo32[i]);
+  }
+  if (d_have_sgp) cudaFree(d_have_sgp);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+int Ctx::upload_geometry(const double *const h[8], const size_t n[8]) {
+  std::vector<float> tmp;
+  for (int i = 0; i < 8; ++i) {
+    if (!geo64[i] && cudaMalloc(&geo64[i], n[i] * sizeof(double)) != cudaSuccess)
+      return set_error("cudaMalloc(geometry)"), ICA_ERR_NOMEM;
+    if (!geo32[i] && cudaMalloc(&geo32[i], n[i] * sizeof(float)) != cudaSuccess)
+      return set_error("cudaMalloc(geometry)"), ICA_ERR_NOMEM;
+    cudaError_t e = cudaMemcpy(geo64[i], h[i], n[i] * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(geometry)");
+    tmp.resize(n[i]);
+    for (size_t j = 0; j < n[i]; ++j) tmp[j] = (float)h[i][j];
+    e = cudaMemcpy(geo32[i], tmp.data(), n[i] * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(geometry)");
+  }
+  geo_n.assign(n, n + 8);
+  geo_set = true;
+  return ICA_OK;
+}
+
+template <> Geo<double> Ctx::geo<double>() const {
+  const double *const *p = (const double *const *)geo64;
+  return Geo<double>{p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7]};
+}
+template <> Geo<float> Ctx::geo<float>() const {
+  const float *const *p = (const float *const *)geo32;
+  return Geo<float>{p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7]};
+}
+
+// ---- device-pointer implementations (asynchronous on the context stream)
+template <typename T>
+int flux_dev(Ctx *c, T *flx_h, T *flx_h_pl, T *GRD_xc, T *GRD_xc_pl, const T *rho, const T *rho_pl, const T *vx,
+             const T *vx_pl, const T *vy, const T *vy_pl, const T *vz, const T *vz_pl, T dt) {
+  if (!c->geo_set) return set_error("horizontal_flux: geometry not registered"), ICA_ERR_STATE;
+  if (!flx_h || !flx_h_pl || !GRD_xc || !GRD_xc_pl || !rho || !rho_pl || !vx || !vx_pl || !vy || !vy_pl || !vz ||
+      !vz_pl)
+    return set_error("horizontal_flux: NULL argument"), ICA_ERR_ARG;
+  FluxIn<T> in{rho, rho_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl};
+  FluxOut<T> out{flx_h, flx_h_pl, GRD_xc, GRD_xc_pl};
+  launch_horizontal_flux<T>(c->D, in, out, c->geo<T>(), dt, c->stream);
+  c->launches += 2;
+  return c->check_launch("horizontal_flux");
+}
+
+template <typename T>
+int comm_dev(Ctx *c, T *var, T *var_pl, int kmax, int vmax, bool pole_fill) {
+  if (!var || !var_pl || kmax < 1 || vmax < 1) return set_error("COMM: bad argument"), ICA_ERR_ARG;
+  const Plan &p = c->plan[pole_fill ? 1 : 0];
+  launch_gather<T>(c->D, p.n, p.dst, p.src, kmax, vmax, var, var_pl, c->stream);
+  c->launches += 1;
+  return c->check_launch("COMM_data_transfer");
+}
+
+template <typename T>
+int hlim_dev(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, const T *d_pl, const T *ch,
+             const T *ch_pl, const T *cmask, const T *cmask_pl, T *Qout_prev, T *Qout_prev_pl, const T *Qout_post,
+             const T *Qout_post_pl, T *scratch_Qout, T *scratch_Qout_pl, T *scratch_Qin_pl) {
+  if (!q_a || !q_a_pl || !q || !q_pl || !d || !d_pl || !ch || !ch_pl || !cmask || !cmask_pl || !Qout_prev ||
+      !Qout_prev_pl || ((Qout_post == nullptr) != (Qout_post_pl == nullptr)))
+    return set_error("horizontal_limiter_thuburn: bad argument"), ICA_ERR_ARG;
+  const size_t n2 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall * 2, n2p = (size_t)kGallPl * c->sz.kall * kLallPl * 2;
+  LimIn<T> in{q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask_pl};
+  launch_hlim_qout<T>(c->D, in, Qout_prev, Qout_prev_pl, scratch_Qin_pl, c->stream);
+  c->launches += 2;
+  const T *Qo = Qout_post, *Qo_pl = Qout_post_pl;
+  if (!Qout_post) {  // NICAM: COMM_data_transfer(Qout, Qout_pl) on a copy of the pre-fill Qout
+    cudaMemcpyAsync(scratch_Qout, Qout_prev, n2 * sizeof(T), cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(scratch_Qout_pl, Qout_prev_pl, n2p * sizeof(T), cudaMemcpyDeviceToDevice, c->stream);
+    const Plan &p = c->plan[0];
+    launch_gather<T>(c->D, p.n, p.dst, p.src, c->sz.kall, 2, scratch_Qout, scratch_Qout_pl, c->stream);
+    c->launches += 1;
+    Qo = scratch_Qout;
+    Qo_pl = scratch_Qout_pl;
+  }
+  launch_hlim_apply<T>(c->D, in, q_a, q_a_pl, Qo, Qo_pl, scratch_Qin_pl, c->stream);
+  c->launches += 2;
+  return c->check_launch("horizontal_limiter_thuburn");
+}
+
+template <typename T>
+int hlim_dev_alloc(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, const T *d_pl, const T *ch,
+                   const T *ch_pl, const T *cmask, const T *cmask_pl, T *Qout_prev, T *Qout_prev_pl,
+                   const T *Qout_post, const T *Qout_post_pl) {
+  const size_t n2 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall * 2, n2p = (size_t)kGallPl * c->sz.kall * kLallPl * 2;
+  T *sq = (T *)c->buf(sizeof(T) == 8 ? "lim_qout64" : "lim_qout32", n2 * sizeof(T));
+  T *sqp = (T *)c->buf(sizeof(T) == 8 ? "lim_qoutpl64" : "lim_qoutpl32", n2p * sizeof(T));
+  T *sqin = (T *)c->buf(sizeof(T) == 8 ? "lim_qinpl64" : "lim_qinpl32", n2p * 2 * sizeof(T));
+  if (!sq || !sqp || !sqin) return set_error("horizontal_limiter_thuburn: cudaMalloc(scratch)"), ICA_ERR_NOMEM;
+  return hlim_dev<T>(c, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask_pl, Qout_prev, Qout_prev_pl,
+                     Qout_post, Qout_post_pl, sq, sqp, sqin);
+}
+
+template <typename T>
+int vlim_dev(Ctx *c, T *q_h, T *q_h_pl, const T *q, const T *q_pl, const T *d, const T *d_pl, const T *ck,
+             const T *ck_pl) {
+  if (!q_h || !q_h_pl || !q || !q_pl || !d || !d_pl || !ck || !ck_pl)
+    return set_error("vertical_limiter_thuburn: NULL argument"), ICA_ERR_ARG;
+  launch_vlim<T>(c->D, q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl, c->stream);
+  c->launches += 2;
+  return c->check_launch("vertical_limiter_thuburn");
+}
+
+// ---- host-pointer staging
+template <typename T> struct Stage {
+  Ctx *c;
+  int rc = ICA_OK;
+  explicit Stage(Ctx *cc) : c(cc) {}
+  T *in(const char *name, const T *h, size_t n) {
+    if (rc) return nullptr;
+    T *d = (T *)c->buf(name, n * sizeof(T));
+    if (!d) { rc = ICA_ERR_NOMEM; set_error(std::string("cudaMalloc ") + name); return nullptr; }
+    if (h) {
+      cudaError_t e = cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, c->stream);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(H2D)");
+    }
+    return d;
+  }
+  void out(T *h, const T *d, size_t n) {
+    if (rc || !h) return;
+    cudaError_t e = cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(D2H)");
+  }
+  int sync() {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamSynchronize");
+    return rc;
+  }
+};
+
+template <typename T>
+int flux_host(Ctx *c, T *flx_h, T *flx_h_pl, T *GRD_xc, T *GRD_xc_pl, const T *rho, const T *rho_pl, const T *vx,
+              const T *vx_pl, const T *vy, const T *vy_pl, const T *vz, const T *vz_pl, T dt) {
+  if (!flx_h || !flx_h_pl || !GRD_xc || !GRD_xc_pl || !rho || !rho_pl || !vx || !vx_pl || !vy || !vy_pl || !vz ||
+      !vz_pl)
+    return set_error("horizontal_flux: NULL argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  Stage<T> s(c);
+  T *d_rho = s.in("a0", rho, n3), *d_rho_pl = s.in("a1", rho_pl, n3p);
+  T *d_vx = s.in("a2", vx, n3), *d_vx_pl = s.in("a3", vx_pl, n3p);
+  T *d_vy = s.in("a4", vy, n3), *d_vy_pl = s.in("a5", vy_pl, n3p);
+  T *d_vz = s.in("a6", vz, n3), *d_vz_pl = s.in("a7", vz_pl, n3p);
+  T *d_f = s.in("o0", nullptr, n3 * 6), *d_fp = s.in("o1", flx_h_pl, n3p);
+  T *d_x = s.in("o2", nullptr, n3 * 9), *d_xp = s.in("o3", GRD_xc_pl, n3p * 3);
+  if (s.rc) return s.rc;
+  int rc = flux_dev<T>(c, d_f, d_fp, d_x, d_xp, d_rho, d_rho_pl, d_vx, d_vx_pl, d_vy, d_vy_pl, d_vz, d_vz_pl, dt);
+  if (rc) return rc;
+  s.out(flx_h, d_f, n3 * 6);
+  s.out(flx_h_pl, d_fp, n3p);
+  s.out(GRD_xc, d_x, n3 * 9);
+  s.out(GRD_xc_pl, d_xp, n3p * 3);
+  return s.sync();
+}
+
+template <typename T>
+int hlim_host(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, const T *d_pl, const T *ch,
+              const T *ch_pl, const T *cmask, const T *cmask_pl, T *Qout_prev, T *Qout_prev_pl, const T *Qout_post,
+              const T *Qout_post_pl) {
+  if (!q_a || !q_a_pl || !q || !q_pl || !d || !d_pl || !ch || !ch_pl || !cmask || !cmask_pl || !Qout_prev ||
+      !Qout_prev_pl || ((Qout_post == nullptr) != (Qout_post_pl == nullptr)))
+    return set_error("horizontal_limiter_thuburn: bad argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  Stage<T> s(c);
+  T *d_qa = s.in("a0", q_a, n3 * 6), *d_qap = s.in("a1", q_a_pl, n3p);
+  T *d_q = s.in("a2", q, n3), *d_qp = s.in("a3", q_pl, n3p);
+  T *d_d = s.in("a4", d, n3), *d_dp = s.in("a5", d_pl, n3p);
+  T *d_ch = s.in("a6", ch, n3 * 6), *d_chp = s.in("a7", ch_pl, n3p);
+  T *d_cm = s.in("a8", cmask, n3 * 6), *d_cmp = s.in("a9", cmask_pl, n3p);
+  T *d_qo = s.in("o0", nullptr, n3 * 2), *d_qop = s.in("o1", nullptr, n3p * 2);
+  T *d_po = Qout_post ? s.in("a10", Qout_post, n3 * 2) : nullptr;
+  T *d_pop = Qout_post ? s.in("a11", Qout_post_pl, n3p * 2) : nullptr;
+  if (s.rc) return s.rc;
+  int rc = hlim_dev_alloc<T>(c, d_qa, d_qap, d_q, d_qp, d_d, d_dp, d_ch, d_chp, d_cm, d_cmp, d_qo, d_qop, d_po,
+                             d_pop);
+  if (rc) return rc;
+  s.out(q_a, d_qa, n3 * 6);
+  s.out(q_a_pl, d_qap, n3p);
+  s.out(Qout_prev, d_qo, n3 * 2);
+  s.out(Qout_prev_pl, d_qop, n3p * 2);
+  return s.sync();
+}
+
+template <typename T>
+int vlim_host(Ctx *c, T *q_h, T *q_h_pl, const T *q, const T *q_pl, const T *d, const T *d_pl, const T *ck,
+              const T *ck_pl) {
+  if (!q_h || !q_h_pl || !q || !q_pl || !d || !d_pl || !ck || !ck_pl)
+    return set_error("vertical_limiter_thuburn: NULL argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  Stage<T> s(c);
+  T *d_qh = s.in("a0", q_h, n3), *d_qhp = s.in("a1", q_h_pl, n3p);
+  T *d_q = s.in("a2", q, n3), *d_qp = s.in("a3", q_pl, n3p);
+  T *d_d = s.in("a4", d, n3), *d_dp = s.in("a5", d_pl, n3p);
+  T *d_ck = s.in("a6", ck, n3 * 2), *d_ckp = s.in("a7", ck_pl, n3p * 2);
+  if (s.rc) return s.rc;
+  int rc = vlim_dev<T>(c, d_qh, d_qhp, d_q, d_qp, d_d, d_dp, d_ck, d_ckp);
+  if (rc) return rc;
+  s.out(q_h, d_qh, n3);
+  s.out(q_h_pl, d_qhp, n3p);
+  return s.sync();
+}
+
+template <typename T>
+int comm_host(Ctx *c, T *var, T *var_pl, int kmax, int vmax, bool pole_fill) {
+  if (!var || !var_pl || kmax < 1 || vmax < 1) return set_error("COMM: bad argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)c->sz.gall * kmax * c->sz.lall * vmax, np = (size_t)kGallPl * kmax * kLallPl * vmax;
+  Stage<T> s(c);
+  T *dv = s.in("a0", var, n), *dp = s.in("a1", var_pl, np);
+  if (s.rc) return s.rc;
+  int rc = comm_dev<T>(c, dv, dp, kmax, vmax, pole_fill);
+  if (rc) return rc;
+  s.out(var, dv, n);
+  s.out(var_pl, dp, np);
+  return s.sync();
+}
+
+}  // namespace icoadv
+
+#define CTX_OK(c) \
+  if (!(c)) return set_error("NULL context"), ICA_ERR_ARG
+
+extern "C" {
+
+int ica_horizontal_flux(ica_ctx *c, double *a, double *b, double *x, double *y, const double *r, const double *rp,
+                        const double *vx, const double *vxp, const double *vy, const double *vyp, const double *vz,
+                        const double *vzp, double dt) {
+  CTX_OK(c);
+  return flux_host<double>(c, a, b, x, y, r, rp, vx, vxp, vy, vyp, vz, vzp, dt);
+}
+int ica_horizontal_flux_f32(ica_ctx *c, float *a, float *b, float *x, float *y, const float *r, const float *rp,
+                            const float *vx, const float *vxp, const float *vy, const float *vyp, const float *vz,
+                            const float *vzp, float dt) {
+  CTX_OK(c);
+  return flux_host<float>(c, a, b, x, y, r, rp, vx, vxp, vy, vyp, vz, vzp, dt);
+}
+int ica_horizontal_flux_dev(ica_ctx *c, double *a, double *b, double *x, double *y, const double *r,
+                            const double *rp, const double *vx, const double *vxp, const double *vy,
+                            const double *vyp, const double *vz, const double *vzp, double dt) {
+  CTX_OK(c);
+  cudaSetDevice(c->device);
+  return flux_dev<double>(c, a, b, x, y, r, rp, vx, vxp, vy, vyp, vz, vzp, dt);
+}
+
+int ica_horizontal_limiter_thuburn(ica_ctx *c, double *q_a, double *q_a_pl, const double *q, const double *q_pl,
+                                   const double *d, const double *d_pl, const double *ch, const double *ch_pl,
+                                   const double *cm, const double *cm_pl, double *qo, double *qo_pl,
+                                   const double *qp, const double *qp_pl) {
+  CTX_OK(c);
+  return hlim_host<double>(c, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cm, cm_pl, qo, qo_pl, qp, qp_pl);
+}
+int ica_horizontal_limiter_thuburn_f32(ica_ctx *c, float *q_a, float *q_a_pl, const float *q, const float *q_pl,
+                                       const float *d, const float *d_pl, const float *ch, const float *ch_pl,
+                                       const float *cm, const float *cm_pl, float *qo, float *qo_pl,
+                                       const float *qp, const float *qp_pl) {
+  CTX_OK(c);
+  return hlim_host<float>(c, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cm, cm_pl, qo, qo_pl, qp, qp_pl);
+}
+int ica_horizontal_limiter_thuburn_dev(ica_ctx *c, double *q_a, double *q_a_pl, const double *q,
+                                       const double *q_pl, const double *d, const double *d_pl, const double *ch,
+                                       const double *ch_pl, const double *cm, const double *cm_pl, double *qo,
+                                       double *qo_pl, const double *qp, const double *qp_pl) {
+  CTX_OK(c);
+  cudaSetDevice(c->device);
+  return hlim_dev_alloc<double>(c, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cm, cm_pl, qo, qo_pl, qp, qp_pl);
+}
+
+int ica_vertical_limiter_thuburn(ica_ctx *c, double *q_h, double *q_h_pl, const double *q, const double *q_pl,
+                                 const double *d, const double *d_pl, const double *ck, const double *ck_pl) {
+  CTX_OK(c);
+  return vlim_host<double>(c, q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl);
+}
+int ica_vertical_limiter_thuburn_f32(ica_ctx *c, float *q_h, float *q_h_pl, const float *q, const float *q_pl,
+                                     const float *d, const float *d_pl, const float *ck, const float *ck_pl) {
+  CTX_OK(c);
+  return vlim_host<float>(c, q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl);
+}
+int ica_vertical_limiter_thuburn_dev(ica_ctx *c, double *q_h, double *q_h_pl, const double *q, const double *q_pl,
+                                     const double *d, const double *d_pl, const double *ck, const double *ck_pl) {
+  CTX_OK(c);
+  cudaSetDevice(c->device);
+  return vlim_dev<double>(c, q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl);
+}
+
+int ica_comm_data_transfer(ica_ctx *c, double *var, double *var_pl, int kmax, int vmax) {
+  CTX_OK(c);
+  return comm_host<double>(c, var, var_pl, kmax, vmax, false);
+}
+int ica_comm_data_transfer_f32(ica_ctx *c, float *var, float *var_pl, int kmax, int vmax) {
+  CTX_OK(c);
+  return comm_host<float>(c, var, var_pl, kmax, vmax, false);
+}
+int ica_comm_data_transfer_dev(ica_ctx *c, double *var, double *var_pl, int kmax, int vmax) {
+  CTX_OK(c);
+  cudaSetDevice(c->device);
+  return comm_dev<double>(c, var, var_pl, kmax, vmax, false);
+}
+int ica_comm_var(ica_ctx *c, double *var, double *var_pl, int kmax, int vmax) {
+  CTX_OK(c);
+  return comm_host<double>(c, var, var_pl, kmax, vmax, true);
+}
+int ica_comm_var_dev(ica_ctx *c, double *var, double *var_pl, int kmax, int vmax) {
+  CTX_OK(c);
+  cudaSetDevice(c->device);
+  return comm_dev<double>(c, var, var_pl, kmax, vmax, true);
+}
+
+}  // extern "C"

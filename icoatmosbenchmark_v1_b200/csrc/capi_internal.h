@@ -1,0 +1,50 @@
+// Context object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "icoadv_internal.h"
+#include "plain_kernels.cuh"
+
+namespace icoadv {
+
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct Plan {  // composed halo fill on the device
+  int n = 0;
+  int *dst = nullptr, *src = nullptr;
+};
+
+struct Ctx {
+  std::unique_ptr<Topology> topo;
+  ica_sizes sz{};
+  Dims D{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Plan plan[2];               // [0] COMM_data_transfer, [1] COMM_var
+  int *d_have_sgp = nullptr;
+  void *geo64[8] = {};        // GRD_xr, _pl, GMTR_p, _pl, GMTR_t, _pl, GMTR_a, _pl
+  void *geo32[8] = {};
+  std::vector<size_t> geo_n;
+  bool geo_set = false;
+  std::map<std::string, DevBuf> bufs;  // staging / scratch, grow-only
+  long long launches = 0;
+
+  ~Ctx();
+  void *buf(const char *name, size_t bytes);
+  int check_launch(const char *what);
+  int upload_geometry(const double *const h[8], const size_t n[8]);
+  template <typename T> Geo<T> geo() const;
+};
+
+int cuda_fail(cudaError_t e, const char *what);
+
+}  // namespace icoadv

@@ -1,0 +1,183 @@
+"""Synthetic fields of the benchmark configurations (seeded), built with torch
+so the large configurations can be generated directly in device memory.
+
+Per configuration (rl 0, R = 6.371e6 m):
+  rho   = 1.2 exp(-z/8000) kg/m^3 at full levels
+  v     = solid-body rotation, 40 m/s at the rotation equator (axis tilted 45 deg
+          towards +x so the flow crosses both poles), plus Gaussian noise of
+          2 m/s std projected on the sphere's tangent plane and smoothed by 3
+          passes of neighbour averaging
+  w     = 0.05 m/s x N(0,1) at interior half levels, 0 at the ground and the top
+  rhogv = rho v, rhogw = rho_face w
+  tracers in [0,1]: "bell" = cosine bell of radius R/3 plus a slotted cylinder
+          (per tracer the two centres rotate in longitude), "smooth" = random
+          band-limited field (plane waves with |k| <= 16 on the unit sphere,
+          standing in for spherical-harmonic degree <= 16) clipped to [0,1];
+          each with a vertical profile that steps at 12 km so the vertical
+          limiter is active.
+Seeds: numpy PCG64(20261203) for the noise, tracer i uses seed 20261203 + 1 + i.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from .grid import Grid
+
+SEED = 20261203
+
+
+def _flat(var, var_pl):
+    """(m, L, K, G), (m, 2, K, 6) -> (m, K, L*G + 12)."""
+    m, L, K, G = var.shape
+    return torch.cat([var.permute(0, 2, 1, 3).reshape(m, K, L * G), var_pl.permute(0, 2, 1, 3).reshape(m, K, 12)], 2)
+
+
+def _unflat(flat, L, G):
+    m, K, _ = flat.shape
+    var = flat[:, :, :L * G].reshape(m, K, L, G).permute(0, 2, 1, 3).contiguous()
+    var_pl = flat[:, :, L * G:].reshape(m, K, 2, 6).permute(0, 2, 1, 3).contiguous()
+    return var, var_pl
+
+
+def halo_fill(grid: Grid, var, var_pl):
+    """Single-process halo/pole fill with the composed COMM plan (host-side preparation of inputs)."""
+    dst, src = grid.plan
+    f = _flat(var, var_pl)
+    d = torch.as_tensor(dst, device=f.device, dtype=torch.long)
+    s = torch.as_tensor(src, device=f.device, dtype=torch.long)
+    f[:, :, d] = f[:, :, s]
+    return _unflat(f, grid.lall, grid.gall)
+
+
+def _positions(grid: Grid, device):
+    x = torch.as_tensor(grid.arrays["GRD_x"], device=device) / grid.R  # (3, L, gall)
+    xp = torch.as_tensor(grid.arrays["GRD_x_pl"], device=device) / grid.R  # (3, 2, 6)
+    return x, xp
+
+
+def _smooth_columns(grid: Grid, v, vp, passes=3):
+    """Neighbour averaging (self + 6 hexagon neighbours) on interior cells; poles average their ring."""
+    L, G = grid.lall, grid.gall_1d
+    g0, g1 = grid.gmin - 1, grid.gmax - 1
+    for _ in range(passes):
+        a = v.reshape(v.shape[0], L, v.shape[2], G, G)
+        c = a[..., g0:g1 + 1, g0:g1 + 1]
+        s = (c + a[..., g0:g1 + 1, g0 + 1:g1 + 2] + a[..., g0 + 1:g1 + 2, g0 + 1:g1 + 2] + a[..., g0 + 1:g1 + 2, g0:g1 + 1]
+             + a[..., g0:g1 + 1, g0 - 1:g1] + a[..., g0 - 1:g1, g0 - 1:g1] + a[..., g0 - 1:g1, g0:g1 + 1]) / 7.0
+        a = a.clone()
+        a[..., g0:g1 + 1, g0:g1 + 1] = s
+        vp = vp.clone()
+        vp[..., 0] = vp.sum(-1) / 6.0
+        v, vp = halo_fill(grid, a.reshape(v.shape), vp)
+    return v, vp
+
+
+def make_fields(grid: Grid, device="cpu", u0=40.0, noise=2.0, wamp=0.05, alpha=math.pi / 4, seed=SEED,
+                dtype=torch.float64):
+    """Shared per-step fields: rho, rhogvx/vy/vz (cell centres), rhogw (half levels)."""
+    L, K, gall = grid.lall, grid.kall, grid.gall
+    vg = grid.arrays
+    z = torch.as_tensor(vg["z"], device=device)
+    rho_k = 1.2 * torch.exp(-z / 8000.0)
+    rho = rho_k.view(1, K, 1).expand(L, K, gall).contiguous()
+    rho_pl = rho_k.view(1, K, 1).expand(2, K, 6).contiguous()
+    x, xp = _positions(grid, device)
+    axis = torch.tensor([math.sin(alpha), 0.0, math.cos(alpha)], device=device, dtype=torch.float64)
+
+    def rot(p):  # axis x p, p (3, ...)
+        return torch.stack([axis[1] * p[2] - axis[2] * p[1], axis[2] * p[0] - axis[0] * p[2],
+                            axis[0] * p[1] - axis[1] * p[0]])
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nz = torch.as_tensor(rng.standard_normal((3, L, K, gall)), device=device)
+    nzp = torch.as_tensor(rng.standard_normal((3, 2, K, 6)), device=device)
+    xe, xpe = x.unsqueeze(2), xp.unsqueeze(2)  # (3, L, 1, gall)
+    nz = nz - (nz * xe).sum(0, keepdim=True) * xe
+    nzp = nzp - (nzp * xpe).sum(0, keepdim=True) * xpe
+    nz, nzp = halo_fill(grid, nz, nzp)
+    nz, nzp = _smooth_columns(grid, nz, nzp)
+    sd = torch.cat([nz.reshape(3, -1), nzp.reshape(3, -1)], 1).norm(dim=0).pow(2).mean().div(2).sqrt()
+    v = u0 * rot(xe) + noise * nz / sd
+    vp = u0 * rot(xpe) + noise * nzp / sd
+    rhogv = v * rho.unsqueeze(0)
+    rhogv_pl = vp * rho_pl.unsqueeze(0)
+    # vertical mass flux at half levels k = kmin+1..kmax (0 at the ground kmin and the top kmax+1)
+    w = torch.as_tensor(rng.standard_normal((L, K, gall)), device=device) * wamp
+    wp = torch.as_tensor(rng.standard_normal((2, K, 6)), device=device) * wamp
+    mask = torch.zeros(K, device=device, dtype=torch.float64)
+    mask[grid.kmin:grid.kmax] = 1.0  # 0-based kmin..kmax-1 = Fortran faces kmin+1..kmax
+    af = torch.as_tensor(vg["afact"], device=device)
+    bf = torch.as_tensor(vg["bfact"], device=device)
+    rho_face = af * rho_k + bf * torch.roll(rho_k, 1)
+    rho_face[0] = rho_k[0]
+    rhogw = w * (mask * rho_face).view(1, K, 1)
+    rhogw_pl = wp * (mask * rho_face).view(1, K, 1)
+    rhogw, rhogw_pl = halo_fill(grid, rhogw.unsqueeze(0), rhogw_pl.unsqueeze(0))
+    out = dict(rhog=rho, rhog_pl=rho_pl, rhogvx=rhogv[0], rhogvx_pl=rhogv_pl[0], rhogvy=rhogv[1],
+               rhogvy_pl=rhogv_pl[1], rhogvz=rhogv[2], rhogvz_pl=rhogv_pl[2], rhogw=rhogw[0], rhogw_pl=rhogw_pl[0])
+    return {k: t.to(dtype).contiguous() for k, t in out.items()}
+
+
+def _bell_cylinder(x, lon0, lat0, R_frac=1.0 / 3.0):
+    """Cosine bell (radius R/3) at (lon0,lat0) plus a slotted cylinder 120 deg east of it, in [0,1]."""
+    def centre(lon, lat):
+        return torch.tensor([math.cos(lat) * math.cos(lon), math.cos(lat) * math.sin(lon), math.sin(lat)],
+                            dtype=x.dtype, device=x.device).view(3, *([1] * (x.dim() - 1)))
+
+    r = R_frac  # angular radius (radians) of R/3 on the sphere
+    d1 = torch.arccos(torch.clamp((x * centre(lon0, lat0)).sum(0), -1, 1))
+    bell = torch.where(d1 < r, 0.5 * (1 + torch.cos(math.pi * d1 / r)), torch.zeros_like(d1))
+    c2 = centre(lon0 + 2 * math.pi / 3, lat0)
+    d2 = torch.arccos(torch.clamp((x * c2).sum(0), -1, 1))
+    # slot: remove a narrow band through the centre along the local meridian
+    lon = torch.atan2(x[1], x[0])
+    dlon = torch.remainder(lon - (lon0 + 2 * math.pi / 3) + math.pi, 2 * math.pi) - math.pi
+    slot = (dlon.abs() < r / 6) & (torch.asin(torch.clamp(x[2], -1, 1)) - lat0 < r * 5 / 6)
+    cyl = torch.where((d2 < r) & ~slot, torch.ones_like(d2), torch.zeros_like(d2))
+    return torch.clamp(bell + cyl, 0.0, 1.0)
+
+
+def _smooth_random(x, seed, kmax=16.0, nwaves=24):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    f = torch.zeros(x.shape[1:], dtype=x.dtype, device=x.device)
+    for _ in range(nwaves):
+        k = torch.randn(3, generator=g, dtype=torch.float64)
+        k = k / k.norm() * (torch.rand(1, generator=g, dtype=torch.float64) * kmax)
+        ph = float(torch.rand(1, generator=g) * 2 * math.pi)
+        a = float(torch.randn(1, generator=g))
+        f = f + a * torch.cos((x * k.to(x.device).view(3, *([1] * (x.dim() - 1)))).sum(0) + ph)
+    f = 0.5 + 0.5 * f / (f.abs().max() + 1e-30) * 1.2
+    return torch.clamp(f, 0.0, 1.0)
+
+
+def tracer_mixing_ratio(grid: Grid, ntr, kind="bell", device="cpu", seed=SEED):
+    """q (ntr, L, K, gall) and q_pl (ntr, 2, K, 6); kind: 'bell', 'smooth' or 'mixed' (half each)."""
+    x, xp = _positions(grid, device)
+    z = torch.as_tensor(grid.arrays["z"], device=device)
+    qs, qps = [], []
+    for t in range(ntr):
+        k = kind if kind != "mixed" else ("smooth" if t % 2 == 0 else "bell")
+        if k == "bell":
+            lon0, lat0 = 2 * math.pi * t / max(ntr, 1) + 0.3, 0.4 * math.sin(1.7 * t + 0.5)
+            q2, q2p = _bell_cylinder(x, lon0, lat0), _bell_cylinder(xp, lon0, lat0)
+        else:
+            q2, q2p = _smooth_random(x, seed + 1 + t), _smooth_random(xp, seed + 1 + t)
+        prof = torch.where(z < 12.0e3 + 500.0 * t, torch.ones_like(z), 0.35 * torch.ones_like(z))
+        qs.append(q2.unsqueeze(1) * prof.view(1, -1, 1))
+        qps.append(q2p.unsqueeze(1) * prof.view(1, -1, 1))
+    q = torch.stack(qs).contiguous()
+    qp = torch.stack(qps).contiguous()
+    return halo_fill(grid, q, qp)
+
+
+def make_state(grid: Grid, ntr, kind="bell", device="cpu", fields=None):
+    """Prognostic state: rhog (L,K,gall), rhogq (ntr,L,K,gall) (+ poles), FP64."""
+    f = fields if fields is not None else make_fields(grid, device)
+    q, qp = tracer_mixing_ratio(grid, ntr, kind, device)
+    rhog = f["rhog"].to(torch.float64).clone()
+    rhog_pl = f["rhog_pl"].to(torch.float64).clone()
+    return dict(rhog=rhog, rhog_pl=rhog_pl, rhogq=(q * rhog.unsqueeze(0)).contiguous(),
+                rhogq_pl=(qp * rhog_pl.unsqueeze(0)).contiguous())

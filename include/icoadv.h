@@ -1,0 +1,201 @@
+/*
+ * icoadv: B200 (sm_100a) implementation of the NICAM horizontal tracer
+ * advection path of IcoAtmosBenchmark_v1, behind a C ABI.
+ *
+ * The kernel entry points keep the argument lists of the reference Fortran
+ * subroutines, in the same order and with the same array layouts
+ * (Fortran column-major, e.g. flx_h(ADM_gall,ADM_kall,ADM_lall,6) is a
+ * contiguous double[6][lall][kall][gall]).  What the reference reads from
+ * module globals (ADM_* sizes, CONST_EPS/CONST_HUGE, ADM_have_sgp, GRD_xr and
+ * the GMTR_* metrics) is held by the context: sizes are fixed by ica_init and
+ * the metrics are registered once with ica_set_geometry.
+ *
+ * One context covers one whole icosahedral grid on one GPU: all
+ * 10*4^rlevel regions (ADM_lall) and both pole regions (ADM_have_pl = true).
+ *
+ * Host-pointer entry points copy their inputs to the device, run on the
+ * context's stream and copy the outputs back before returning.  The *_dev
+ * variants take device pointers of the same shapes and are asynchronous on
+ * the context's stream (ica_stream).  Every function returns ICA_OK (0) or a
+ * negative ICA_ERR_* code; the reference has no status returns (it stops),
+ * the Fortran shim in INTEGRATION.md turns a nonzero status into STOP.
+ *
+ * Precision: the reference selects RP at compile time (mod_precision.f90:19-26);
+ * here the unsuffixed entry points are RP = DP (double), the *_f32 ones are
+ * RP = SP (float, EPS = epsilon(1.0), HUGE = huge(1.0)).
+ */
+#ifndef ICOADV_H
+#define ICOADV_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ICA_OK 0
+#define ICA_ERR_ARG (-1)      /* bad size, NULL pointer or out-of-range argument */
+#define ICA_ERR_STATE (-2)    /* context not initialised / geometry not registered */
+#define ICA_ERR_CUDA (-3)     /* a CUDA call failed; see ica_last_error() */
+#define ICA_ERR_TIMEOUT (-4)  /* a bounded device-side wait gave up */
+#define ICA_ERR_INTERNAL (-5) /* an internal consistency check failed */
+#define ICA_ERR_NOMEM (-6)    /* device or host allocation failed */
+
+typedef struct ica_ctx ica_ctx;
+
+/* Sizes.  Replaces the ADM_* module globals of problem_size.inc:28-59 and the
+ * ADMPARAM namelist of communication/src/mod_adm.f90:172-251:
+ * gall_1d = 2^(glevel-rlevel)+2, gmin = 2, gmax = gall_1d-1,
+ * lall = 10*4^rlevel, kall = vlayer+2, kmin = 2, kmax = vlayer+1
+ * (vlayer = 1 gives kall = kmin = kmax = 1). */
+typedef struct {
+  int glevel;
+  int rlevel;
+  int vlayer;
+  int device; /* CUDA device ordinal */
+} ica_dims;
+
+/* Derived sizes, for callers that allocate arrays. */
+typedef struct {
+  int gall_1d, gall, gmin, gmax; /* 1-based Fortran indices gmin/gmax */
+  int kall, kmin, kmax;
+  int lall, gall_pl, lall_pl;    /* lall_pl = 2, gall_pl = 6 */
+} ica_sizes;
+
+/* Create a context: sizes, the CUDA stream and the halo/pole gather plan.
+ * Replaces ADM_setup + COMM_setup (mod_adm.f90:165, mod_comm.f90:147). */
+int ica_init(const ica_dims *dims, ica_ctx **ctx);
+int ica_finalize(ica_ctx *ctx);
+int ica_get_sizes(const ica_ctx *ctx, ica_sizes *out);
+/* The context's CUDA stream (a cudaStream_t), for the *_dev entry points. */
+void *ica_stream(ica_ctx *ctx);
+/* Text of the last error on this thread. */
+const char *ica_last_error(void);
+/* Number of kernels this library launched since the context was created. */
+long long ica_launch_count(const ica_ctx *ctx);
+/* Is the library's device code loadable on `device` (sm_100)?  0 = yes. */
+int ica_device_check(int device);
+
+/* Metrics read by horizontal_flux from module mod_misc (mod_misc.f90:128-136;
+ * dyn_horiz_adv_flux/src/main.f90:91-98 for the shapes):
+ *   GRD_xr(gall,1,lall,3,3)  GRD_xr_pl(6,1,2,3)
+ *   GMTR_p(gall,1,lall,8)    GMTR_p_pl(6,1,2,8)
+ *   GMTR_t(gall,1,lall,2,5)  GMTR_t_pl(6,1,2,5)
+ *   GMTR_a(gall,1,lall,3,12) GMTR_a_pl(6,1,2,18)
+ * Copied to the device once (FP64, and an FP32 copy for the *_f32 path). */
+int ica_set_geometry(ica_ctx *ctx,
+                     const double *GRD_xr, const double *GRD_xr_pl,
+                     const double *GMTR_p, const double *GMTR_p_pl,
+                     const double *GMTR_t, const double *GMTR_t_pl,
+                     const double *GMTR_a, const double *GMTR_a_pl);
+
+/* ---- horizontal_flux: kernels/NICAM/dyn_horiz_adv_flux/src/mod_src_tracer.f90:42-49,78-90
+ * out flx_h(gall,kall,lall,6) flx_h_pl(6,kall,2)
+ *     GRD_xc(gall,kall,lall,3,3) GRD_xc_pl(6,kall,2,3)
+ * in  rho, rhovx, rhovy, rhovz (gall,kall,lall) + _pl (6,kall,2), dt */
+int ica_horizontal_flux(ica_ctx *ctx,
+                        double *flx_h, double *flx_h_pl,
+                        double *GRD_xc, double *GRD_xc_pl,
+                        const double *rho, const double *rho_pl,
+                        const double *rhovx, const double *rhovx_pl,
+                        const double *rhovy, const double *rhovy_pl,
+                        const double *rhovz, const double *rhovz_pl,
+                        double dt);
+int ica_horizontal_flux_dev(ica_ctx *ctx,
+                            double *flx_h, double *flx_h_pl,
+                            double *GRD_xc, double *GRD_xc_pl,
+                            const double *rho, const double *rho_pl,
+                            const double *rhovx, const double *rhovx_pl,
+                            const double *rhovy, const double *rhovy_pl,
+                            const double *rhovz, const double *rhovz_pl,
+                            double dt);
+int ica_horizontal_flux_f32(ica_ctx *ctx,
+                            float *flx_h, float *flx_h_pl,
+                            float *GRD_xc, float *GRD_xc_pl,
+                            const float *rho, const float *rho_pl,
+                            const float *rhovx, const float *rhovx_pl,
+                            const float *rhovy, const float *rhovy_pl,
+                            const float *rhovz, const float *rhovz_pl,
+                            float dt);
+
+/* ---- horizontal_limiter_thuburn:
+ *      kernels/NICAM/dyn_horiz_adv_limiter/src/mod_src_tracer.f90:42-49,71-84
+ * inout q_a(gall,kall,lall,6) q_a_pl(6,kall,2)
+ * in    q, d (gall,kall,lall); ch, cmask (gall,kall,lall,6); + _pl (6,kall,2)
+ * out   Qout_prev(gall,kall,lall,2) Qout_prev_pl(6,kall,2,2): Qout before the halo fill
+ * in    Qout_post(gall,kall,lall,2) Qout_post_pl(6,kall,2,2): Qout after the halo fill,
+ *       as the extracted kernel reads it from its snapshot (:369-373).  Pass NULL
+ *       for both to run the fill on the GPU instead, which is what NICAM does
+ *       (the commented COMM_data_transfer at :371). */
+int ica_horizontal_limiter_thuburn(ica_ctx *ctx,
+                                   double *q_a, double *q_a_pl,
+                                   const double *q, const double *q_pl,
+                                   const double *d, const double *d_pl,
+                                   const double *ch, const double *ch_pl,
+                                   const double *cmask, const double *cmask_pl,
+                                   double *Qout_prev, double *Qout_prev_pl,
+                                   const double *Qout_post, const double *Qout_post_pl);
+int ica_horizontal_limiter_thuburn_dev(ica_ctx *ctx,
+                                       double *q_a, double *q_a_pl,
+                                       const double *q, const double *q_pl,
+                                       const double *d, const double *d_pl,
+                                       const double *ch, const double *ch_pl,
+                                       const double *cmask, const double *cmask_pl,
+                                       double *Qout_prev, double *Qout_prev_pl,
+                                       const double *Qout_post, const double *Qout_post_pl);
+int ica_horizontal_limiter_thuburn_f32(ica_ctx *ctx,
+                                       float *q_a, float *q_a_pl,
+                                       const float *q, const float *q_pl,
+                                       const float *d, const float *d_pl,
+                                       const float *ch, const float *ch_pl,
+                                       const float *cmask, const float *cmask_pl,
+                                       float *Qout_prev, float *Qout_prev_pl,
+                                       const float *Qout_post, const float *Qout_post_pl);
+
+/* ---- vertical_limiter_thuburn:
+ *      kernels/NICAM/dyn_vert_adv_limiter/src/mod_src_tracer.f90:41-45,60-67
+ * inout q_h(gall,kall,lall) q_h_pl(6,kall,2)
+ * in    q, d (gall,kall,lall) + _pl; ck(gall,kall,lall,2) ck_pl(6,kall,2,2) */
+int ica_vertical_limiter_thuburn(ica_ctx *ctx,
+                                 double *q_h, double *q_h_pl,
+                                 const double *q, const double *q_pl,
+                                 const double *d, const double *d_pl,
+                                 const double *ck, const double *ck_pl);
+int ica_vertical_limiter_thuburn_dev(ica_ctx *ctx,
+                                     double *q_h, double *q_h_pl,
+                                     const double *q, const double *q_pl,
+                                     const double *d, const double *d_pl,
+                                     const double *ck, const double *ck_pl);
+int ica_vertical_limiter_thuburn_f32(ica_ctx *ctx,
+                                     float *q_h, float *q_h_pl,
+                                     const float *q, const float *q_pl,
+                                     const float *d, const float *d_pl,
+                                     const float *ck, const float *ck_pl);
+
+/* ---- COMM_data_transfer: kernels/NICAM/communication/src/mod_comm.f90:1506-1540
+ * inout var(gall,kmax,lall,vmax) var_pl(6,kmax,2,vmax).  The reference takes
+ * kmax and vmax from shape(var); here they are arguments.  The MPI exchange
+ * of the reference becomes one bit-exact index gather on the GPU. */
+int ica_comm_data_transfer(ica_ctx *ctx, double *var, double *var_pl, int kmax, int vmax);
+int ica_comm_data_transfer_dev(ica_ctx *ctx, double *var, double *var_pl, int kmax, int vmax);
+int ica_comm_data_transfer_f32(ica_ctx *ctx, float *var, float *var_pl, int kmax, int vmax);
+/* ---- COMM_var: mod_comm.f90:1895-1917 (halo -> pole centre, then the transfer) */
+int ica_comm_var(ica_ctx *ctx, double *var, double *var_pl, int kmax, int vmax);
+int ica_comm_var_dev(ica_ctx *ctx, double *var, double *var_pl, int kmax, int vmax);
+
+/* ---- Host-only topology helpers (no GPU needed).
+ * Point index of region cell (i,j) of region r (all 1-based):
+ *   (r-1)*gall + (j-1)*gall_1d + (i-1);  pole p (0 north, 1 south), slot v:
+ *   10*4^rlevel*gall + 6*p + (v-1).
+ * ica_comm_plan: the composed single-process halo fill dst[e] <- src[e]
+ * (pole_fill = 1 adds COMM_var's halo -> pole-centre copy first).  Call with
+ * dst = src = NULL to get the count in *n. */
+int ica_comm_plan(int glevel, int rlevel, int pole_fill, int *n, int *dst, int *src);
+/* have_sgp[10*4^rl] (ADM_have_sgp), rgn4pl[2] (RGNMNG_rgn4pl),
+ * pole_ring[2][5] (RGNMNG_vert_tab_pl region ids); any may be NULL. */
+int ica_topology_info(int glevel, int rlevel, int *have_sgp, int *rgn4pl, int *pole_ring);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ICOADV_H */
