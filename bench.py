@@ -1,0 +1,320 @@
+"""Throughput benchmark of the NICAM tracer-advection step on B200.
+
+Workload (the configuration the headline metric is quoted on): glevel 8,
+rlevel 0 (10 regions of 258x258, 655,362 columns), kall 96, 32 tracers, FP32
+flux/limiter arithmetic with the FP64 rhogq/rhog mass update, dt = 150 s
+(1200 s scaled by 2^(5-gl)).  One step advances every tracer cell-level once:
+2,013,272,064 updates.  Synthetic seeded inputs of the reference's shapes
+(there are no input snapshots to load).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fast|plain] [--impl ours|reference]
+
+value : updates/s of the device-resident step loop (CUDA events on the library's
+        stream, max over ranks); e2e: the same metric through the host-pointer
+        C ABI call with pinned host buffers, copies inside the timed region.
+--impl reference: the CPU restatement of the reference (oracle) on all host
+        cores, on a bounded sample of the workload (glevel 6, same kall/tracers per
+        step), reported in the same unit.
+N > 1: one process per GPU, each running an independent replica of the workload
+(the single-GPU path does not shard), value = total updates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "tracer cell-level updates/s"
+UNIT = "updates/s"
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_reference(glevel, kall, ntr, steps, warmup, threads):
+    """The oracle (C restatement of the reference) on `threads` host cores; returns updates/s."""
+    import numpy as np
+
+    from icoatmosbenchmark_v1_b200 import fields as F
+    from icoatmosbenchmark_v1_b200.grid import Grid, default_dt
+    from oracle import oracle as O
+    g = Grid(glevel, 0, kall)
+    f = {k: v.numpy() for k, v in F.make_fields(g).items()}
+    S = {k: v.numpy().copy() for k, v in F.make_state(g, ntr, "mixed").items()}
+    d = O.make_dims(glevel, 0, kall)
+    topo = O.Topo(glevel, 0, 1)
+    dt = default_dt(glevel)
+    for _ in range(warmup):
+        O.step(d, g.have_sgp, topo, dt, S, f, g.arrays, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.step(d, g.have_sgp, topo, dt, S, f, g.arrays, nthreads=threads)
+    el = time.perf_counter() - t0
+    upd = (10 * 4 ** glevel + 2) * kall * ntr * steps
+    return upd / el, el, upd, np
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    gl = args.ref_glevel
+    val, el, upd, _ = cpu_reference(gl, args.kall, args.ntr, args.steps, args.warmup, threads)
+    sample = f"glevel {gl}, kall {args.kall}, {args.ntr} tracers, {args.steps} steps ({upd:.3e} updates)"
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    return {"workload": f"gl{args.glevel}_k{args.kall}_t{args.ntr}", "glevel": args.glevel, "rlevel": 0,
+            "kall": args.kall, "tracers": args.ntr, "columns": 10 * 4 ** args.glevel + 2,
+            "updates_per_step": (10 * 4 ** args.glevel + 2) * args.kall * args.ntr,
+            "mode": args.mode, "dt": 1200.0 * 2.0 ** (5 - args.glevel),
+            "l2": "inputs larger than L2 (state %.1f GB)" % ((10 * 4 ** args.glevel + 2) * args.kall * args.ntr * 8e-9)}
+
+
+# ---------------------------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from icoatmosbenchmark_v1_b200 import api
+    from icoatmosbenchmark_v1_b200 import fields as F
+    from icoatmosbenchmark_v1_b200.grid import Grid, default_dt
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    g = Grid(args.glevel, 0, args.kall)
+    dt = default_dt(args.glevel)
+    f = F.make_fields(g, device=dev)
+    st = F.make_state(g, args.ntr, "mixed", device=dev, fields=f)
+    del f["rhog"], f["rhog_pl"]
+    ctx = api.IcoAdv(args.glevel, 0, args.kall - 2, device=local)
+    ctx.set_grid(g)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    upd = (10 * 4 ** args.glevel + 2) * args.kall * args.ntr
+
+    if args.mode == "plain":
+        def step():
+            ctx.advect_step(dt, st["rhog"], st["rhog_pl"], st["rhogq"], st["rhogq_pl"], f["rhogvx"], f["rhogvx_pl"],
+                            f["rhogvy"], f["rhogvy_pl"], f["rhogvz"], f["rhogvz_pl"], f["rhogw"], f["rhogw_pl"])
+        dtype = "f64"
+        s_bytes = 48
+    else:
+        runner = ctx.fast_runner(g, st, f, dt)
+        step = runner.step
+        dtype = "f32"
+        s_bytes = 32
+
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    n0 = ctx.launch_count
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    launches = ctx.launch_count - n0
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = allreduce_max(ms, world)
+    value = upd * world / (ms * 1e-3)
+    peak, peak_kind = load_peaks()
+    b_alg = 16.0 + s_bytes / args.ntr
+    kern = None
+    if args.mode != "plain":
+        kern = runner.kernel_stats()
+    if kern:  # dominant kernel timed with its own events inside the step loop
+        achieved = kern["bytes_per_launch"] / (kern["ms_per_launch"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": kern["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": args.traffic,
+                "alg_bytes_per_update": b_alg}
+    else:
+        achieved = upd * b_alg / (ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": args.traffic,
+                "alg_bytes_per_update": b_alg}
+    # ---- e2e through the host-pointer C ABI (pinned host buffers, copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        e2e = measure_e2e(args, ctx, g, st, f, dt, upd, world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        cval, cel, cupd, _ = cpu_reference(args.ref_glevel, args.kall, args.ntr, 1, 0, threads)
+        cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"oracle, glevel {args.ref_glevel}, kall {args.kall}, {args.ntr} tracers, 1 step "
+                         f"({cupd:.3e} updates, {cel:.1f} s)"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": workload_config(args),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def measure_e2e(args, ctx, g, st, f, dt, upd, world):
+    """Per step: pinned host -> device copy of the state and fields, the step, device -> host copy of
+    the state, all inside one host-pointer C ABI call (ica_advect_step / ica_advect_fast)."""
+    import numpy as np
+    import torch
+    n = max(1, min(args.steps, args.e2e_steps))
+    host = {k: v.cpu().pin_memory() for k, v in st.items()}
+    hf = {k: v.cpu().pin_memory() for k, v in f.items()}
+    hn = {k: v.numpy() for k, v in host.items()}
+    hfn = {k: v.numpy() for k, v in hf.items()}
+    h2d = sum(v.numel() * v.element_size() for v in host.values()) + sum(
+        v.numel() * v.element_size() for v in hf.values())
+    d2h = sum(v.numel() * v.element_size() for v in host.values())
+    call = ctx.advect_step if args.mode == "plain" else ctx.advect_fast_host
+    call(dt, **{}, **_step_kwargs(hn, hfn))  # warm (allocates staging once)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(n):
+        call(dt, **_step_kwargs(hn, hfn))
+    el = (time.perf_counter() - t0) / n
+    el = allreduce_max(el, world)
+    return {"value": upd * world / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "steps": n, "ms_per_step": el * 1e3}
+
+
+def _step_kwargs(s, f):
+    return dict(rhog=s["rhog"], rhog_pl=s["rhog_pl"], rhogq=s["rhogq"], rhogq_pl=s["rhogq_pl"],
+                rhogvx=f["rhogvx"], rhogvx_pl=f["rhogvx_pl"], rhogvy=f["rhogvy"], rhogvy_pl=f["rhogvy_pl"],
+                rhogvz=f["rhogvz"], rhogvz_pl=f["rhogvz_pl"], rhogw=f["rhogw"], rhogw_pl=f["rhogw_pl"])
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["fast", "plain"], default="fast")
+    ap.add_argument("--glevel", type=int, default=8)
+    ap.add_argument("--kall", type=int, default=96)
+    ap.add_argument("--ntr", type=int, default=32)
+    ap.add_argument("--ref-glevel", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="ncu dram bytes per launch of the dominant kernel, if measured")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -217,3 +217,26 @@ class IcoAdv:
     def COMM_var(self, var, var_pl):
         vmax, _, kmax, _ = var.shape
         self._call("ica_comm_var", self._dtype(var), [var, var_pl], int(kmax), int(vmax))
+
+    # ---- composed step -----------------------------------------------------------
+    def set_step_geometry(self, GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact, bfact):
+        args = [_ptr(np.ascontiguousarray(a, np.float64), np.float64)[0]
+                for a in (GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact, bfact)]
+        _check("ica_set_step_geometry", lib().ica_set_step_geometry(self.h, *args))
+
+    def set_grid(self, grid):
+        """Registers the metrics and step geometry of an icoatmosbenchmark_v1_b200.grid.Grid."""
+        A = grid.arrays
+        self.set_geometry(*[A[k] for k in ("GRD_xr", "GRD_xr_pl", "GMTR_p", "GMTR_p_pl", "GMTR_t", "GMTR_t_pl",
+                                           "GMTR_a", "GMTR_a_pl")])
+        self.set_step_geometry(A["GRD_x"], A["GRD_x_pl"], A["coef_grad"], A["coef_grad_pl"], A["rdgz"], A["afact"],
+                               A["bfact"])
+
+    def advect_step(self, dt, rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz,
+                    rhogvz_pl, rhogw, rhogw_pl):
+        """One composed FP64 step in place (plain per-tracer path)."""
+        ntr = rhogq.shape[0]
+        arrs =[rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz, rhogvz_pl, rhogw, rhogw_pl]
+        ptrs, kinds = zip(*[_ptr(a, np.float64) for a in arrs])
+        name = "ica_advect_step" + ("_dev" if kinds[0] else "")
+        _check(name, getattr(lib(), name)(self.h, int(ntr), C.c_double(dt), *ptrs))

@@ -168,6 +168,8 @@ Ctx::~Ctx() {
     if (geo32[i]) cudaFree(geo32[i]);
   }
   if (d_have_sgp) cudaFree(d_have_sgp);
+  for (void *p : stepgeo)
+    if (p) cudaFree(p);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -476,6 +478,111 @@ int ica_comm_var_dev(ica_ctx *c, double *var, double *var_pl, int kmax, int vmax
   CTX_OK(c);
   cudaSetDevice(c->device);
   return comm_dev<double>(c, var, var_pl, kmax, vmax, true);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// composed step
+namespace icoadv {
+
+int Ctx::step_ctx(StepCtx &S) {
+  if (!geo_set || !stepgeo_set) return set_error("advect_step: geometry not registered"), ICA_ERR_STATE;
+  const size_t n3 = (size_t)sz.gall * sz.kall * sz.lall, n3p = (size_t)kGallPl * sz.kall * kLallPl;
+  S.D = D;
+  S.geo = geo<double>();
+  S.plan = DevPlan{plan[0].n, plan[0].dst, plan[0].src};
+  const double *const *g = (const double *const *)stepgeo;
+  S.GRD_x = g[0], S.GRD_x_pl = g[1], S.cg = g[2], S.cg_pl = g[3], S.rdgz = g[4], S.afact = g[5], S.bfact = g[6];
+  struct B {
+    double **p;
+    const char *name;
+    size_t n;
+  } bl[] = {{&S.flx, "st_flx", n3 * 6}, {&S.flx_pl, "st_flxp", n3p}, {&S.xc, "st_xc", n3 * 9},
+            {&S.xc_pl, "st_xcp", n3p * 3}, {&S.ch, "st_ch", n3 * 6}, {&S.ch_pl, "st_chp", n3p},
+            {&S.cm, "st_cm", n3 * 6}, {&S.cm_pl, "st_cmp", n3p}, {&S.zero, "st_zero", n3},
+            {&S.zero_pl, "st_zerop", n3p}, {&S.q, "st_q", n3}, {&S.q_pl, "st_qp", n3p},
+            {&S.grad, "st_grad", n3 * 3}, {&S.grad_pl, "st_gradp", n3p * 3}, {&S.qa, "st_qa", n3 * 6},
+            {&S.qa_pl, "st_qap", n3p}, {&S.qout, "st_qout", n3 * 2}, {&S.qout_pl, "st_qoutp", n3p * 2},
+            {&S.qin_pl, "st_qinp", n3p * 4}};
+  bool fresh_zero = bufs.find("st_zero") == bufs.end();
+  for (auto &b : bl) {
+    *b.p = (double *)buf(b.name, b.n * sizeof(double));
+    if (!*b.p) return set_error(std::string("cudaMalloc ") + b.name), ICA_ERR_NOMEM;
+  }
+  if (fresh_zero) {
+    cudaMemsetAsync(S.zero, 0, n3 * sizeof(double), stream);
+    cudaMemsetAsync(S.zero_pl, 0, n3p * sizeof(double), stream);
+  }
+  return ICA_OK;
+}
+
+}  // namespace icoadv
+
+extern "C" {
+
+int ica_set_step_geometry(ica_ctx *c, const double *GRD_x, const double *GRD_x_pl, const double *coef_grad,
+                          const double *coef_grad_pl, const double *rdgz, const double *afact, const double *bfact) {
+  CTX_OK(c);
+  if (!GRD_x || !GRD_x_pl || !coef_grad || !coef_grad_pl || !rdgz || !afact || !bfact)
+    return set_error("ica_set_step_geometry: NULL argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t gl = (size_t)c->sz.gall * c->sz.lall;
+  const double *h[7] = {GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact, bfact};
+  const size_t n[7] = {gl * 3, (size_t)kGallPl * kLallPl * 3, gl * 21, (size_t)6 * 3 * kLallPl,
+                       (size_t)c->sz.kall, (size_t)c->sz.kall, (size_t)c->sz.kall};
+  for (int i = 0; i < 7; ++i) {
+    if (!c->stepgeo[i] && cudaMalloc(&c->stepgeo[i], n[i] * sizeof(double)) != cudaSuccess)
+      return set_error("cudaMalloc(step geometry)"), ICA_ERR_NOMEM;
+    cudaError_t e = cudaMemcpy(c->stepgeo[i], h[i], n[i] * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(step geometry)");
+  }
+  c->stepgeo_set = true;
+  return ICA_OK;
+}
+
+int ica_advect_step_dev(ica_ctx *c, int ntr, double dt, double *rhog, double *rhog_pl, double *rhogq,
+                        double *rhogq_pl, const double *vx, const double *vx_pl, const double *vy,
+                        const double *vy_pl, const double *vz, const double *vz_pl, const double *w,
+                        const double *w_pl) {
+  CTX_OK(c);
+  if (ntr < 1 || !rhog || !rhog_pl || !rhogq || !rhogq_pl || !vx || !vx_pl || !vy || !vy_pl || !vz || !vz_pl || !w ||
+      !w_pl)
+    return set_error("ica_advect_step: bad argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  StepCtx S;
+  int rc = c->step_ctx(S);
+  if (rc) return rc;
+  rc = step_plain(S, ntr, dt, rhog, rhog_pl, rhogq, rhogq_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl, c->stream,
+                  c->launches);
+  if (rc) return set_error("ica_advect_step: kall above 128"), rc;
+  return c->check_launch("ica_advect_step");
+}
+
+int ica_advect_step(ica_ctx *c, int ntr, double dt, double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
+                    const double *vx, const double *vx_pl, const double *vy, const double *vy_pl, const double *vz,
+                    const double *vz_pl, const double *w, const double *w_pl) {
+  CTX_OK(c);
+  if (ntr < 1 || !rhog || !rhog_pl || !rhogq || !rhogq_pl || !vx || !vx_pl || !vy || !vy_pl || !vz || !vz_pl || !w ||
+      !w_pl)
+    return set_error("ica_advect_step: bad argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  Stage<double> s(c);
+  double *d_r = s.in("h0", rhog, n3), *d_rp = s.in("h1", rhog_pl, n3p);
+  double *d_q = s.in("h2", rhogq, n3 * ntr), *d_qp = s.in("h3", rhogq_pl, n3p * ntr);
+  double *d_x = s.in("h4", vx, n3), *d_xp = s.in("h5", vx_pl, n3p);
+  double *d_y = s.in("h6", vy, n3), *d_yp = s.in("h7", vy_pl, n3p);
+  double *d_z = s.in("h8", vz, n3), *d_zp = s.in("h9", vz_pl, n3p);
+  double *d_w = s.in("h10", w, n3), *d_wp = s.in("h11", w_pl, n3p);
+  if (s.rc) return s.rc;
+  int rc = ica_advect_step_dev(c, ntr, dt, d_r, d_rp, d_q, d_qp, d_x, d_xp, d_y, d_yp, d_z, d_zp, d_w, d_wp);
+  if (rc) return rc;
+  s.out(rhog, d_r, n3);
+  s.out(rhog_pl, d_rp, n3p);
+  s.out(rhogq, d_q, n3 * ntr);
+  s.out(rhogq_pl, d_qp, n3p * ntr);
+  return s.sync();
 }
 
 }  // extern "C"

@@ -10,6 +10,7 @@
 
 #include "icoadv_internal.h"
 #include "plain_kernels.cuh"
+#include "step.cuh"
 
 namespace icoadv {
 
@@ -35,6 +36,8 @@ struct Ctx {
   void *geo32[8] = {};
   std::vector<size_t> geo_n;
   bool geo_set = false;
+  void *stepgeo[7] = {};      // GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact, bfact
+  bool stepgeo_set = false;
   std::map<std::string, DevBuf> bufs;  // staging / scratch, grow-only
   long long launches = 0;
 
@@ -43,6 +46,7 @@ struct Ctx {
   int check_launch(const char *what);
   int upload_geometry(const double *const h[8], const size_t n[8]);
   template <typename T> Geo<T> geo() const;
+  int step_ctx(StepCtx &S);
 };
 
 int cuda_fail(cudaError_t e, const char *what);

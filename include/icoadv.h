@@ -183,6 +183,39 @@ int ica_comm_data_transfer_f32(ica_ctx *ctx, float *var, float *var_pl, int kmax
 int ica_comm_var(ica_ctx *ctx, double *var, double *var_pl, int kmax, int vmax);
 int ica_comm_var_dev(ica_ctx *ctx, double *var, double *var_pl, int kmax, int vmax);
 
+/* ---- The composed tracer step (not in the reference, which runs each kernel
+ * alone on a snapshot).  One step = horizontal_flux -> Courant numbers and
+ * upwind masks -> gradient (OPRT_gradient_setup stencil, dyn_metrics/src/
+ * mod_oprt.f90:499-734) + halo fill -> Miura upwind remap -> Thuburn horizontal
+ * limiter with the Qout halo fill -> rhogq/rhog update, then the vertical
+ * sub-step (vertical_limiter_thuburn on linearly interpolated half-level
+ * values) and the halo fill of the state.
+ *
+ * Step geometry: cell positions GRD_x(gall,1,lall,3) GRD_x_pl(6,1,2,3);
+ * coef_grad(gall,0:6,3,lall) coef_grad_pl(0:5,3,2); vertical grid rdgz(kall),
+ * afact(kall), bfact(kall) with q_h(k) = afact(k) q(k) + bfact(k) q(k-1) at
+ * the face between levels k-1 and k. */
+int ica_set_step_geometry(ica_ctx *ctx, const double *GRD_x, const double *GRD_x_pl,
+                          const double *coef_grad, const double *coef_grad_pl,
+                          const double *rdgz, const double *afact, const double *bfact);
+/* Plain FP64 step, tracer by tracer.  State (in/out, halos valid on entry and
+ * exit): rhog(gall,kall,lall) rhog_pl(6,kall,2), rhogq(gall,kall,lall,ntr)
+ * rhogq_pl(6,kall,2,ntr).  Fields: rhogvx/vy/vz(gall,kall,lall) + _pl at cell
+ * centres, rhogw(gall,kall,lall) + _pl at the face below each level (zero at
+ * the ground face kmin and the top face kmax+1). */
+int ica_advect_step(ica_ctx *ctx, int ntr, double dt,
+                    double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
+                    const double *rhogvx, const double *rhogvx_pl,
+                    const double *rhogvy, const double *rhogvy_pl,
+                    const double *rhogvz, const double *rhogvz_pl,
+                    const double *rhogw, const double *rhogw_pl);
+int ica_advect_step_dev(ica_ctx *ctx, int ntr, double dt,
+                        double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
+                        const double *rhogvx, const double *rhogvx_pl,
+                        const double *rhogvy, const double *rhogvy_pl,
+                        const double *rhogvz, const double *rhogvz_pl,
+                        const double *rhogw, const double *rhogw_pl);
+
 /* ---- Host-only topology helpers (no GPU needed).
  * Point index of region cell (i,j) of region r (all 1-based):
  *   (r-1)*gall + (j-1)*gall_1d + (i-1);  pole p (0 north, 1 south), slot v:
