@@ -195,6 +195,7 @@ def run_ours(args, world, rank, local):
     else:
         runner = ctx.fast_runner(g, st, f, dt)
         step = runner.step
+        st = runner.state
         dtype = "f32"
         s_bytes = 32
 
@@ -207,6 +208,8 @@ def run_ours(args, world, rank, local):
     sampler.start()
     n0 = ctx.launch_count
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.mode != "plain":
+        runner.start_timing()
     torch.cuda.synchronize()
     barrier(world)
     e0.record(stream)
@@ -246,10 +249,14 @@ def run_ours(args, world, rank, local):
         cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"oracle, glevel {args.ref_glevel}, kall {args.kall}, {args.ntr} tracers, 1 step "
                          f"({cupd:.3e} updates, {cel:.1f} s)"}
+    cfg = workload_config(args)
+    if args.mode != "plain":
+        cfg["tile"] = {"shape_txtytg": list(runner.tuning[runner.shape]["shape"]) if runner.tuning else None,
+                       "autotune_ms": [round(t["ms"], 3) for t in runner.tuning]}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": workload_config(args),
+                "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": cfg,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -263,13 +270,15 @@ def measure_e2e(args, ctx, g, st, f, dt, upd, world):
     n = max(1, min(args.steps, args.e2e_steps))
     host = {k: v.cpu().pin_memory() for k, v in st.items()}
     hf = {k: v.cpu().pin_memory() for k, v in f.items()}
+    if args.mode != "plain":  # the fused path takes FP32 fields
+        hf = {k: v.to(torch.float32).pin_memory() for k, v in hf.items()}
     hn = {k: v.numpy() for k, v in host.items()}
     hfn = {k: v.numpy() for k, v in hf.items()}
     h2d = sum(v.numel() * v.element_size() for v in host.values()) + sum(
         v.numel() * v.element_size() for v in hf.values())
     d2h = sum(v.numel() * v.element_size() for v in host.values())
     call = ctx.advect_step if args.mode == "plain" else ctx.advect_fast_host
-    call(dt, **{}, **_step_kwargs(hn, hfn))  # warm (allocates staging once)
+    call(dt, **_step_kwargs(hn, hfn))  # warm (allocates staging once)
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()

@@ -165,9 +165,9 @@ class IcoAdv:
         return lib().ica_launch_count(self.h)
 
     def set_geometry(self, GRD_xr, GRD_xr_pl, GMTR_p, GMTR_p_pl, GMTR_t, GMTR_t_pl, GMTR_a, GMTR_a_pl):
-        args = [_ptr(np.ascontiguousarray(a, np.float64), np.float64)[0]
+        keep = [np.ascontiguousarray(a, np.float64)
                 for a in (GRD_xr, GRD_xr_pl, GMTR_p, GMTR_p_pl, GMTR_t, GMTR_t_pl, GMTR_a, GMTR_a_pl)]
-        _check("ica_set_geometry", lib().ica_set_geometry(self.h, *args))
+        _check("ica_set_geometry", lib().ica_set_geometry(self.h, *[_ptr(a, np.float64)[0] for a in keep]))
 
     def _call(self, name, dtype, arrays, *scalars):
         ptrs, kinds = zip(*[_ptr(a, dtype) for a in arrays])
@@ -220,9 +220,9 @@ class IcoAdv:
 
     # ---- composed step -----------------------------------------------------------
     def set_step_geometry(self, GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact, bfact):
-        args = [_ptr(np.ascontiguousarray(a, np.float64), np.float64)[0]
-                for a in (GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact, bfact)]
-        _check("ica_set_step_geometry", lib().ica_set_step_geometry(self.h, *args))
+        keep = [np.ascontiguousarray(a, np.float64) for a in (GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact,
+                                                               bfact)]
+        _check("ica_set_step_geometry", lib().ica_set_step_geometry(self.h, *[_ptr(a, np.float64)[0] for a in keep]))
 
     def set_grid(self, grid):
         """Registers the metrics and step geometry of an icoatmosbenchmark_v1_b200.grid.Grid."""
@@ -236,7 +236,110 @@ class IcoAdv:
                     rhogvz_pl, rhogw, rhogw_pl):
         """One composed FP64 step in place (plain per-tracer path)."""
         ntr = rhogq.shape[0]
-        arrs =[rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz, rhogvz_pl, rhogw, rhogw_pl]
+        arrs = [rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz, rhogvz_pl, rhogw, rhogw_pl]
         ptrs, kinds = zip(*[_ptr(a, np.float64) for a in arrs])
         name = "ica_advect_step" + ("_dev" if kinds[0] else "")
         _check(name, getattr(lib(), name)(self.h, int(ntr), C.c_double(dt), *ptrs))
+
+    # ---- fused batched path ------------------------------------------------------
+    def advect_fast_dev(self, dt, state_in, state_out, fields32):
+        """One fused step on device tensors: state dicts (rhog, rhog_pl, rhogq, rhogq_pl) FP64,
+        fields32 dict (rhogvx..rhogw_pl) FP32; writes state_out."""
+        ntr = state_in["rhogq"].shape[0]
+        sp = [_ptr(state_in[k], np.float64)[0] for k in STATE_KEYS]
+        so = [_ptr(state_out[k], np.float64)[0] for k in STATE_KEYS]
+        fp = [_ptr(fields32[k], np.float32)[0] for k in FIELD_KEYS]
+        _check("ica_advect_fast_dev", lib().ica_advect_fast_dev(self.h, int(ntr), C.c_double(dt), *sp, *so, *fp))
+
+    def advect_fast_host(self, dt, rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz,
+                         rhogvz_pl, rhogw, rhogw_pl):
+        """One fused step on host arrays, in place on the FP64 state (FP32 fields)."""
+        ntr = rhogq.shape[0]
+        sp = [_ptr(a, np.float64)[0] for a in (rhog, rhog_pl, rhogq, rhogq_pl)]
+        fp = [_ptr(a, np.float32)[0] for a in (rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz, rhogvz_pl, rhogw,
+                                             rhogw_pl)]
+        _check("ica_advect_fast", lib().ica_advect_fast(self.h, int(ntr), C.c_double(dt), *sp, *fp))
+
+    def fast_shapes(self):
+        n = C.c_int()
+        _check("ica_fast_shapes", lib().ica_fast_shapes(self.h, C.byref(n), None, None, None))
+        tx, ty, tg = (np.zeros(n.value, np.int32) for _ in range(3))
+        ip = C.POINTER(C.c_int)
+        _check("ica_fast_shapes", lib().ica_fast_shapes(self.h, C.byref(n), tx.ctypes.data_as(ip),
+                                                        ty.ctypes.data_as(ip), tg.ctypes.data_as(ip)))
+        return list(zip(tx.tolist(), ty.tolist(), tg.tolist()))
+
+    def fast_set_shape(self, shape):
+        _check("ica_fast_set_shape", lib().ica_fast_set_shape(self.h, int(shape)))
+
+    def fast_timing(self, enable):
+        ms = C.c_double()
+        n = C.c_longlong()
+        _check("ica_fast_timing", lib().ica_fast_timing(self.h, int(enable), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def fast_runner(self, grid, state, fields, dt, autotune=True):
+        return FastRunner(self, grid, state, fields, dt, autotune)
+
+
+STATE_KEYS = ("rhog", "rhog_pl", "rhogq", "rhogq_pl")
+FIELD_KEYS = ("rhogvx", "rhogvx_pl", "rhogvy", "rhogvy_pl", "rhogvz", "rhogvz_pl", "rhogw", "rhogw_pl")
+
+
+class FastRunner:
+    """Device-resident loop of the fused step: double-buffered FP64 state, FP32 fields, tile
+    shape chosen by timing every available shape on the real inputs (the autotuner)."""
+
+    def __init__(self, ctx, grid, state, fields, dt, autotune=True):
+        import torch
+        self.ctx, self.dt = ctx, dt
+        self.a = state
+        self.b = {k: torch.empty_like(v) for k, v in state.items()}
+        self.f32 = {k: fields[k].to(torch.float32).contiguous() for k in FIELD_KEYS}
+        self.updates = (10 * 4 ** grid.glevel + 2) * grid.kall * state["rhogq"].shape[0]
+        self.alg_bytes = 16.0 + 32.0 / state["rhogq"].shape[0]
+        self.shape = 0
+        self.tuning = []
+        if autotune:
+            self.autotune()
+
+    @property
+    def state(self):
+        return self.a
+
+    def step(self):
+        self.ctx.advect_fast_dev(self.dt, self.a, self.b, self.f32)
+        self.a, self.b = self.b, self.a
+
+    def autotune(self, reps=2):
+        import torch
+        shapes = self.ctx.fast_shapes()
+        saved = {k: v.clone() for k, v in self.a.items()}
+        best = None
+        for s in range(len(shapes)):
+            self.ctx.fast_set_shape(s)
+            self.step()
+            self.ctx.fast_timing(1)
+            for _ in range(reps):
+                self.step()
+            ms, n = self.ctx.fast_timing(0)
+            t = ms / max(n, 1)
+            self.tuning.append({"shape": shapes[s], "ms": t})
+            if best is None or t < best[1]:
+                best = (s, t)
+        self.shape = best[0]
+        self.ctx.fast_set_shape(self.shape)
+        for k in self.a:
+            self.a[k].copy_(saved[k])
+        torch.cuda.synchronize()
+
+    def start_timing(self):
+        self.ctx.fast_timing(1)
+
+    def kernel_stats(self):
+        """Average CUDA-event duration of the tile kernel over the steps since start_timing()."""
+        ms, n = self.ctx.fast_timing(0)
+        if n == 0:
+            return None
+        return {"name": "k_fast_tile", "ms_per_launch": ms / n, "launches": n,
+                "bytes_per_launch": self.updates * self.alg_bytes}

@@ -170,6 +170,9 @@ Ctx::~Ctx() {
   if (d_have_sgp) cudaFree(d_have_sgp);
   for (void *p : stepgeo)
     if (p) cudaFree(p);
+  for (void *p : {(void *)fast.bsrc, (void *)fast.blist, (void *)fast.ring, (void *)fast.cg32})
+    if (p) cudaFree(p);
+  for (auto &ev : fast.events) cudaEventDestroy(ev.first), cudaEventDestroy(ev.second);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -537,6 +540,13 @@ int ica_set_step_geometry(ica_ctx *c, const double *GRD_x, const double *GRD_x_p
     cudaError_t e = cudaMemcpy(c->stepgeo[i], h[i], n[i] * sizeof(double), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(step geometry)");
   }
+  // FP32 copy of the gradient coefficients for the fused path
+  std::vector<float> cg32(n[2]);
+  for (size_t j = 0; j < n[2]; ++j) cg32[j] = (float)coef_grad[j];
+  if (!c->fast.cg32 && cudaMalloc(&c->fast.cg32, n[2] * sizeof(float)) != cudaSuccess)
+    return set_error("cudaMalloc(coef_grad fp32)"), ICA_ERR_NOMEM;
+  cudaError_t e = cudaMemcpy(c->fast.cg32, cg32.data(), n[2] * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(coef_grad fp32)");
   c->stepgeo_set = true;
   return ICA_OK;
 }
@@ -582,6 +592,200 @@ int ica_advect_step(ica_ctx *c, int ntr, double dt, double *rhog, double *rhog_p
   s.out(rhog_pl, d_rp, n3p);
   s.out(rhogq, d_q, n3 * ntr);
   s.out(rhogq_pl, d_qp, n3p * ntr);
+  return s.sync();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// fused batched path
+#include "fast_kernels.cuh"
+
+namespace icoadv {
+
+// Boundary tables of the fused path: which cells' gradient / Qout come from the
+// boundary pass (region-boundary cells, halo cells through the COMM plan, pole centres).
+int Ctx::build_fast_tables() {
+  if (fast.built) return ICA_OK;
+  const Topology &t = *topo;
+  const int G = t.gall_1d, gall = t.gall, L = t.nrgn, g0 = t.gmin, g1 = t.gmax;
+  const int npt = L * gall;
+  std::vector<int> bsrc((size_t)L * gall, -1), blist;
+  for (int l = 0; l < L; ++l)
+    for (int j = 1; j <= G; ++j)
+      for (int i = 1; i <= G; ++i) {
+        const int c = l * gall + (j - 1) * G + (i - 1);
+        const bool in = i >= g0 && i <= g1 && j >= g0 && j <= g1;
+        if (!in) bsrc[c] = -2;
+        else if (i == g0 || i == g1 || j == g0 || j == g1) {
+          bsrc[c] = (int)blist.size();
+          blist.push_back(c);
+        }
+      }
+  const int nbr = (int)blist.size();
+  blist.push_back(npt + 0);
+  blist.push_back(npt + kGallPl);
+  std::vector<int> ring(2 * kVlink, -1);
+  std::vector<int> d, s;
+  int rc = t.build_plan(false, d, s);
+  if (rc) return rc;
+  for (size_t e = 0; e < d.size(); ++e) {
+    int b;
+    if (s[e] < npt) {
+      b = bsrc[s[e]];
+      if (b < 0) return set_error("fast tables: halo source is not a boundary cell"), ICA_ERR_INTERNAL;
+    } else {
+      const int q = s[e] - npt;
+      if (q % kGallPl != 0) return set_error("fast tables: halo source is a pole ring point"), ICA_ERR_INTERNAL;
+      b = nbr + q / kGallPl;
+    }
+    if (d[e] < npt) bsrc[d[e]] = b;
+    else {
+      const int q = d[e] - npt, p = q / kGallPl, v = q % kGallPl;
+      if (v >= 1) ring[p * kVlink + (v - 1)] = b;
+    }
+  }
+  for (int x : ring)
+    if (x < 0) return set_error("fast tables: pole ring slot without a source"), ICA_ERR_INTERNAL;
+  fast.nb = (int)blist.size();
+  if (cudaMalloc(&fast.bsrc, bsrc.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&fast.blist, blist.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&fast.ring, ring.size() * sizeof(int)) != cudaSuccess)
+    return set_error("cudaMalloc(fast tables)"), ICA_ERR_NOMEM;
+  cudaMemcpy(fast.bsrc, bsrc.data(), bsrc.size() * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(fast.blist, blist.data(), blist.size() * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(fast.ring, ring.data(), ring.size() * sizeof(int), cudaMemcpyHostToDevice);
+  fast.built = true;
+  return ICA_OK;
+}
+
+int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
+  if (!geo_set || !stepgeo_set) return set_error("advect_fast: geometry not registered"), ICA_ERR_STATE;
+  if (sz.kall < 4 || sz.kall > 128) return set_error("advect_fast: kall must be in [4, 128]"), ICA_ERR_ARG;
+  int rc = build_fast_tables();
+  if (rc) return rc;
+  int tx[16], ty[16], tg[16];
+  const int ns = fast_tile_shapes(tx, ty, tg, sz.gmax - sz.gmin + 1);
+  if (fast.shape < 0 || fast.shape >= ns) fast.shape = 0;
+  const int nmax = sz.gmax - sz.gmin + 1;
+  I.G = sz.gall_1d, I.gall = sz.gall, I.gmin = sz.gmin, I.gmax = sz.gmax;
+  I.K = sz.kall, I.kmin = sz.kmin, I.kmax = sz.kmax, I.lall = sz.lall, I.ntr = ntr;
+  I.ntx = (nmax + tx[fast.shape] - 1) / tx[fast.shape];
+  I.nty = (nmax + ty[fast.shape] - 1) / ty[fast.shape];
+  I.dt = dt;
+  I.have_sgp = d_have_sgp;
+  const double *const *g = (const double *const *)geo64;
+  I.GRD_xr = g[0], I.GRD_xr_pl = g[1], I.GMTR_p = g[2], I.GMTR_p_pl = g[3], I.GMTR_t = g[4], I.GMTR_t_pl = g[5];
+  I.GMTR_a = g[6], I.GMTR_a_pl = g[7];
+  const double *const *sg = (const double *const *)stepgeo;
+  I.GRD_x = sg[0], I.GRD_x_pl = sg[1], I.cg = sg[2], I.cg_pl = sg[3], I.rdgz = sg[4], I.afact = sg[5], I.bfact = sg[6];
+  I.cg32 = fast.cg32;
+  I.bsrc = fast.bsrc, I.blist = fast.blist, I.pole_ring_b = fast.ring, I.nb = fast.nb;
+  const size_t nbb = (size_t)ntr * sz.kall * fast.nb * 5;
+  I.bbuf = (double *)buf("fast_bbuf", nbb * sizeof(double));
+  if (!I.bbuf) return set_error("cudaMalloc(fast boundary buffer)"), ICA_ERR_NOMEM;
+  return ICA_OK;
+}
+
+}  // namespace icoadv
+
+extern "C" {
+
+int ica_fast_shapes(ica_ctx *c, int *n, int *tx, int *ty, int *tg) {
+  CTX_OK(c);
+  if (!n) return ICA_ERR_ARG;
+  *n = fast_tile_shapes(tx, ty, tg, c->sz.gmax - c->sz.gmin + 1);
+  return ICA_OK;
+}
+
+int ica_fast_set_shape(ica_ctx *c, int shape) {
+  CTX_OK(c);
+  int n = fast_tile_shapes(nullptr, nullptr, nullptr, 0);
+  if (shape < 0 || shape >= n) return set_error("ica_fast_set_shape: no such tile shape"), ICA_ERR_ARG;
+  c->fast.shape = shape;
+  return ICA_OK;
+}
+
+int ica_fast_timing(ica_ctx *c, int enable, double *ms_total, long long *count) {
+  CTX_OK(c);
+  cudaSetDevice(c->device);
+  double tot = 0.0;
+  long long n = 0;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_fast_timing");
+  for (auto &p : c->fast.events) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess) tot += ms, ++n;
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  c->fast.events.clear();
+  cudaGetLastError();
+  c->fast.timing = enable != 0;
+  if (ms_total) *ms_total = tot;
+  if (count) *count = n;
+  return ICA_OK;
+}
+
+int ica_advect_fast_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, const double *rhog_in_pl,
+                        const double *rhogq_in, const double *rhogq_in_pl, double *rhog_out, double *rhog_out_pl,
+                        double *rhogq_out, double *rhogq_out_pl, const float *vx, const float *vx_pl, const float *vy,
+                        const float *vy_pl, const float *vz, const float *vz_pl, const float *w, const float *w_pl) {
+  CTX_OK(c);
+  if (ntr < 1 || !rhog_in || !rhog_in_pl || !rhogq_in || !rhogq_in_pl || !rhog_out || !rhog_out_pl || !rhogq_out ||
+      !rhogq_out_pl || !vx || !vx_pl || !vy || !vy_pl || !vz || !vz_pl || !w || !w_pl)
+    return set_error("ica_advect_fast: NULL argument"), ICA_ERR_ARG;
+  if (rhogq_in == rhogq_out || rhog_in == rhog_out)
+    return set_error("ica_advect_fast: input and output state must be different buffers"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  FastInst I;
+  int rc = c->fast_inst(I, ntr, dt);
+  if (rc) return rc;
+  I.vx = vx, I.vy = vy, I.vz = vz, I.w = w, I.vx_pl = vx_pl, I.vy_pl = vy_pl, I.vz_pl = vz_pl, I.w_pl = w_pl;
+  I.rho_in = rhog_in, I.rho_in_pl = rhog_in_pl, I.Q_in = rhogq_in, I.Q_in_pl = rhogq_in_pl;
+  I.rho_out = rhog_out, I.rho_out_pl = rhog_out_pl, I.Q_out = rhogq_out, I.Q_out_pl = rhogq_out_pl;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c->fast.timing) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    c->fast.events.push_back({e0, e1});
+  }
+  cudaError_t e = fast_step(I, c->fast.shape, c->stream, e0, e1, c->launches);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_advect_fast");
+  const Plan &p = c->plan[0];
+  launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, 1, rhog_out, rhog_out_pl, c->stream);
+  launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, ntr, rhogq_out, rhogq_out_pl, c->stream);
+  c->launches += 2;
+  return c->check_launch("ica_advect_fast");
+}
+
+int ica_advect_fast(ica_ctx *c, int ntr, double dt, double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
+                    const float *vx, const float *vx_pl, const float *vy, const float *vy_pl, const float *vz,
+                    const float *vz_pl, const float *w, const float *w_pl) {
+  CTX_OK(c);
+  if (ntr < 1 || !rhog || !rhog_pl || !rhogq || !rhogq_pl || !vx || !vx_pl || !vy || !vy_pl || !vz || !vz_pl || !w ||
+      !w_pl)
+    return set_error("ica_advect_fast: NULL argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  Stage<double> s(c);
+  double *r0 = s.in("f0", rhog, n3), *r0p = s.in("f1", rhog_pl, n3p);
+  double *q0 = s.in("f2", rhogq, n3 * ntr), *q0p = s.in("f3", rhogq_pl, n3p * ntr);
+  double *r1 = s.in("f4", nullptr, n3), *r1p = s.in("f5", nullptr, n3p);
+  double *q1 = s.in("f6", nullptr, n3 * ntr), *q1p = s.in("f7", nullptr, n3p * ntr);
+  Stage<float> sf(c);
+  float *dx = sf.in("g0", vx, n3), *dxp = sf.in("g1", vx_pl, n3p);
+  float *dy = sf.in("g2", vy, n3), *dyp = sf.in("g3", vy_pl, n3p);
+  float *dz = sf.in("g4", vz, n3), *dzp = sf.in("g5", vz_pl, n3p);
+  float *dw = sf.in("g6", w, n3), *dwp = sf.in("g7", w_pl, n3p);
+  if (s.rc) return s.rc;
+  if (sf.rc) return sf.rc;
+  int rc = ica_advect_fast_dev(c, ntr, dt, r0, r0p, q0, q0p, r1, r1p, q1, q1p, dx, dxp, dy, dyp, dz, dzp, dw, dwp);
+  if (rc) return rc;
+  s.out(rhog, r1, n3);
+  s.out(rhog_pl, r1p, n3p);
+  s.out(rhogq, q1, n3 * ntr);
+  s.out(rhogq_pl, q1p, n3p * ntr);
   return s.sync();
 }
 

@@ -24,6 +24,17 @@ struct Plan {  // composed halo fill on the device
   int *dst = nullptr, *src = nullptr;
 };
 
+struct FastState {  // fused path: boundary tables, tile shape, kernel timing
+  bool built = false;
+  int nb = 0, shape = 0;
+  int *bsrc = nullptr, *blist = nullptr, *ring = nullptr;
+  float *cg32 = nullptr;
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+};
+
+struct FastInst;
+
 struct Ctx {
   std::unique_ptr<Topology> topo;
   ica_sizes sz{};
@@ -47,6 +58,9 @@ struct Ctx {
   int upload_geometry(const double *const h[8], const size_t n[8]);
   template <typename T> Geo<T> geo() const;
   int step_ctx(StepCtx &S);
+  FastState fast;
+  int build_fast_tables();
+  int fast_inst(FastInst &I, int ntr, double dt);
 };
 
 int cuda_fail(cudaError_t e, const char *what);

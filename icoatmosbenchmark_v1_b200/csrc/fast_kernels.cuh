@@ -1,0 +1,17 @@
+// Launch interface of the fused batched path.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fast_common.cuh"
+
+namespace icoadv {
+
+// Tile shapes available to the autotuner: fills tx/ty/tg (arrays of the returned length) when non-NULL.
+int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax);
+// One fused step of instance I on stream st with tile shape `shape`; ev0/ev1 (optional)
+// are recorded around the tile kernel, the dominant launch.
+cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
+                      long long &launches);
+
+}  // namespace icoadv

@@ -276,12 +276,14 @@ int step_plain(StepCtx &S, int ntr, double dt, double *rhog, double *rhog_pl, do
   const Dims &D = S.D;
   const size_t n3 = (size_t)D.gall * D.kall * D.lall, n3p = (size_t)kGallPl * D.kall * kLallPl;
   const int T = 128;
+  const unsigned nb6 = (unsigned)((n3p + 255) / 256);                // one thread per pole point
+  const unsigned nb1 = (unsigned)((kLallPl * D.kall + 255) / 256);   // one thread per pole level
   // shared per step
   FluxIn<double> fin{rhog, rhog_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl};
   FluxOut<double> fout{S.flx, S.flx_pl, S.xc, S.xc_pl};
   launch_horizontal_flux<double>(D, fin, fout, S.geo, dt, st);
   k_courant<<<(unsigned)((6 * n3 + 255) / 256), 256, 0, st>>>((int)n3, S.flx, rhog, S.ch, S.cm);
-  k_courant_pl<<<1, 256, 0, st>>>(D.kall, S.flx_pl, rhog_pl, S.ch_pl, S.cm_pl);
+  k_courant_pl<<<nb6, 256, 0, st>>>(D.kall, S.flx_pl, rhog_pl, S.ch_pl, S.cm_pl);
   launches += 4;
   LimIn<double> lin{S.q, S.q_pl, S.zero, S.zero_pl, S.ch, S.ch_pl, S.cm, S.cm_pl};
   for (int t = 0; t < ntr; ++t) {
@@ -289,19 +291,19 @@ int step_plain(StepCtx &S, int ntr, double dt, double *rhog, double *rhog_pl, do
     k_divide<<<(unsigned)((n3 + n3p + 255) / 256), 256, 0, st>>>((long long)n3, (int)n3p, Q, rhog, Qp, rhog_pl,
                                                                  S.q, S.q_pl);
     k_gradient<<<slab(D, T), T, 0, st>>>(D, S.q, S.cg, S.grad);
-    k_gradient_pl<<<1, 256, 0, st>>>(D.kall, S.q_pl, S.cg_pl, S.grad_pl);
+    k_gradient_pl<<<nb1, 256, 0, st>>>(D.kall, S.q_pl, S.cg_pl, S.grad_pl);
     launch_gather<double>(D, S.plan.n, S.plan.dst, S.plan.src, D.kall, 3, S.grad, S.grad_pl, st);
     k_remap<<<slab(D, T), T, 0, st>>>(D, S.q, S.grad, S.cm, S.xc, S.GRD_x, S.qa);
-    k_remap_pl<<<1, 256, 0, st>>>(D.kall, S.q_pl, S.grad_pl, S.cm_pl, S.xc_pl, S.GRD_x_pl, S.qa_pl);
+    k_remap_pl<<<nb6, 256, 0, st>>>(D.kall, S.q_pl, S.grad_pl, S.cm_pl, S.xc_pl, S.GRD_x_pl, S.qa_pl);
     launch_hlim_qout<double>(D, lin, S.qout, S.qout_pl, S.qin_pl, st);
     launch_gather<double>(D, S.plan.n, S.plan.dst, S.plan.src, D.kall, 2, S.qout, S.qout_pl, st);
     launch_hlim_apply<double>(D, lin, S.qa, S.qa_pl, S.qout, S.qout_pl, S.qin_pl, st);
     k_update_h<<<slab(D, T), T, 0, st>>>(D, S.flx, S.qa, Q);
-    k_update_h_pl<<<1, 256, 0, st>>>(D.kall, S.flx_pl, S.qa_pl, Qp);
+    k_update_h_pl<<<nb1, 256, 0, st>>>(D.kall, S.flx_pl, S.qa_pl, Qp);
     launches += 14;
   }
   k_update_rho<<<slab(D, T), T, 0, st>>>(D, S.flx, rhog);
-  k_update_rho_pl<<<1, 256, 0, st>>>(D.kall, S.flx_pl, rhog_pl);
+  k_update_rho_pl<<<nb1, 256, 0, st>>>(D.kall, S.flx_pl, rhog_pl);
   const int ncol = D.lall * D.gall + kLallPl;
   if (D.kall <= 48)
     k_vertical<48><<<(ncol + 127) / 128, 128, 0, st>>>(D, ntr, dt, rhog, rhogq, w, rhog_pl, rhogq_pl, w_pl, S.rdgz,

@@ -11,7 +11,7 @@ from oracle import oracle as O
 
 
 @functools.lru_cache(maxsize=8)
-def case(glevel=5, rlevel=0, kall=12, ntr=1, kind="bell"):
+def case(glevel=5, rlevel=0, kall=12, ntr=1, kind="mixed"):
     g = Grid(glevel, rlevel, kall)
     f = {k: v.numpy() for k, v in F.make_fields(g).items()}
     st = {k: v.numpy() for k, v in F.make_state(g, ntr, kind).items()}
