@@ -31,8 +31,6 @@ SOURCES = {
     "plain_kernels.cu": ["--fmad=false"],
     "step.cu": ["--fmad=false"],
     "fast_kernels.cu": [],
-    "adjoint.cu": ["--fmad=false"],
-    "noalloc.cu": ["--fmad=false"],
 }
 
 

@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(TX *TY) k_fast_tile(FastInst I) {
       // ---- (b) gradient and Qout of cells in [-1, T]^2
       for (int e = tid; e < N; e += NT) {
         const int lx = e % W, ly = e / W;
-        if (lx < 2 || ly < 2 || lx > TX + 2 || ly > TY + 2) continue;
+        if (lx < 2 || ly < 2 || lx > TX + 3 || ly > TY + 3) continue;
         const int i = i0 - 3 + lx, j = j0 - 3 + ly;
         if (!inreg(i, j)) continue;
         const int bs = I.bsrc[(size_t)l * I.gall + (j - 1) * G + (i - 1)];
@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(TX *TY) k_fast_tile(FastInst I) {
       // ---- (c) limited face values of owners in [-1, T-1]^2
       for (int e = tid; e < N; e += NT) {
         const int lx = e % W, ly = e / W;
-        if (lx < 2 || ly < 2 || lx > TX + 1 || ly > TY + 1) continue;
+        if (lx < 2 || ly < 2 || lx > TX + 2 || ly > TY + 2) continue;
         const int i = i0 - 3 + lx, j = j0 - 3 + ly;
         if (!inreg(i, j)) continue;
         const int nbe[3] = {e + 1, e + W + 1, e + W};
@@ -684,8 +684,8 @@ __global__ void k_fast_pole(FastInst I) {
     const double maxL = mx64(qk, qm) - (1.0 - infl) * BIG, maxU = mx64(qk, qp) - (1.0 - infu) * BIG;
     const double qnmin = mn64(mn64(minL, minU), qk), qnmax = mx64(mx64(maxL, maxU), qk);
     const double Cin = infl * ck1[k] + infu * ck2[k], Cout = (1.0 - infl) * ck1[k] + (1.0 - infu) * ck2[k];
-    const double CQmax = infl * (ck1[k] * maxL) + infu * (ck2[k] * maxU);
-    const double CQmin = infl * (ck1[k] * minL) + infu * (ck2[k] * minU);
+    const double CQmax = infl * ck1[k] * maxL + infu * ck2[k] * maxU;  // region form, as the composed step
+    const double CQmin = infl * ck1[k] * minL + infu * ck2[k] * minU;
     const double zerosw = 0.5 - fsg(0.5, fabs(Cout) - EPS);
     Qmin = ((qk - qnmax) + qnmax * (Cin + Cout) - CQmax) / (Cout + zerosw) * (1.0 - zerosw) + qk * zerosw;
     Qmax = ((qk - qnmin) + qnmin * (Cin + Cout) - CQmin) / (Cout + zerosw) * (1.0 - zerosw) + qk * zerosw;

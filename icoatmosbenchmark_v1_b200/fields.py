@@ -7,8 +7,8 @@ Per configuration (rl 0, R = 6.371e6 m):
           towards +x so the flow crosses both poles), plus Gaussian noise of
           2 m/s std projected on the sphere's tangent plane and smoothed by 3
           passes of neighbour averaging
-  w     = 0.05 m/s x N(0,1) at interior half levels, 0 at the ground and the top
-  rhogv = rho v, rhogw = rho_face w
+  rhogv = rho v; the noise is a column-mass-neutral baroclinic mode and rhogw comes
+          from the discrete continuity equation, so rho stays steady (see make_fields)
   tracers in [0,1]: "bell" = cosine bell of radius R/3 plus a slotted cylinder
           (per tracer the two centres rotate in longitude), "smooth" = random
           band-limited field (plane waves with |k| <= 16 on the unit sphere,
@@ -75,12 +75,73 @@ def _smooth_columns(grid: Grid, v, vp, passes=3):
     return v, vp
 
 
-def make_fields(grid: Grid, device="cpu", u0=40.0, noise=2.0, wamp=0.05, alpha=math.pi / 4, seed=SEED,
+def mass_flux_divergence(grid: Grid, rho, rhov, rho_pl, rhov_pl):
+    """Horizontal mass-flux divergence sum_m flx_h(m) / dt per cell and level (FP64), with the
+    face fluxes of horizontal_flux (triangle interpolation, singular point, pentagon face);
+    interior cells and the pole centres.  rho (L,K,gall), rhov (3,L,K,gall); poles (2,K,6)."""
+    A = grid.arrays
+    L, K, G = grid.lall, rho.shape[1], grid.gall_1d
+    dev = rho.device
+    gt = torch.as_tensor(A["GMTR_t"], device=dev).view(5, 2, L, 1, G, G)
+    ga = torch.as_tensor(A["GMTR_a"], device=dev).view(12, 3, L, 1, G, G)
+    ra = torch.as_tensor(A["GMTR_p"][1], device=dev).view(L, 1, G, G)
+    f = torch.stack([rho, rhov[0], rhov[1], rhov[2]]).view(4, L, K, G, G)  # [..., j, i]
+    s0, s1 = slice(0, G - 1), slice(1, G)
+    TI = f[..., s0, s0] * gt[2, 0][..., s0, s0] + f[..., s0, s1] * gt[3, 0][..., s0, s0]
+    TI = TI + f[..., s1, s1] * gt[4, 0][..., s0, s0]
+    TJ = f[..., s0, s0] * gt[2, 1][..., s0, s0]
+    TJ = TJ + f[..., s1, s1] * gt[3, 1][..., s0, s0] + f[..., s1, s0] * gt[4, 1][..., s0, s0]
+    sg = torch.as_tensor(grid.have_sgp, device=dev).bool()
+    TI[:, sg, :, 0, 0] = TJ[:, sg, :, 0, 1]  # rhot_TI(gmin-1,gmin-1) = rhot_TJ(gmin,gmin-1)
+
+    def face(v, a, jj, ii):  # 0.5 (v . HN) of face a at owners [jj, ii]
+        return 0.5 * (v[1] * ga[0, a][..., jj, ii] + v[2] * ga[1, a][..., jj, ii] + v[3] * ga[2, a][..., jj, ii])
+
+    n = G - 2  # interior cells 0-based 1..G-2
+    ci, cm = slice(1, G - 1), slice(0, G - 2)
+    fai = face(TJ[..., cm, ci] + TI[..., ci, ci], 0, ci, ci)           # AI of (i,j)
+    faim = face(TJ[..., cm, cm] + TI[..., ci, cm], 0, ci, cm)          # AI of (i-1,j)
+    faij = face(TI[..., ci, ci] + TJ[..., ci, ci], 1, ci, ci)          # AIJ of (i,j)
+    faijm = face(TI[..., cm, cm] + TJ[..., cm, cm], 1, cm, cm)         # AIJ of (i-1,j-1)
+    faj = face(TJ[..., ci, ci] + TI[..., ci, cm], 2, ci, ci)           # AJ of (i,j)
+    fajm = face(TJ[..., cm, ci] + TI[..., cm, cm], 2, cm, ci)          # AJ of (i,j-1)
+    fajm[sg, :, 0, 0] = 0.0  # flx_h(gmin,gmin,6) = 0
+    div = ra[..., ci, ci] * (fai + faij + faj - faim - faijm - fajm)
+    out = torch.zeros(L, K, G, G, dtype=rho.dtype, device=dev)
+    out[:, :, 1:G - 1, 1:G - 1] = div
+    # poles
+    gtp = torch.as_tensor(A["GMTR_t_pl"], device=dev)
+    gap = torch.as_tensor(A["GMTR_a_pl"], device=dev)
+    rap = torch.as_tensor(A["GMTR_p_pl"][1][:, 0], device=dev)
+    fp = torch.stack([rho_pl, rhov_pl[0], rhov_pl[1], rhov_pl[2]])  # (4, 2, K, 6)
+    out_pl = torch.zeros_like(rho_pl)
+    for p in range(2):
+        T = {}
+        for v in range(2, 7):
+            vp = 2 if v == 6 else v + 1
+            T[v] = fp[:, p, :, 0] * gtp[2, p, v - 1] + fp[:, p, :, v - 1] * gtp[3, p, v - 1] + fp[:, p, :, vp - 1] * gtp[4, p, v - 1]
+        tot = 0.0
+        for v in range(2, 7):
+            vm = 6 if v == 2 else v - 1
+            vv = T[vm] + T[v]
+            tot = tot + 0.5 * (vv[1] * gap[0, p, v - 1] + vv[2] * gap[1, p, v - 1] + vv[3] * gap[2, p, v - 1])
+        out_pl[p, :, 0] = rap[p] * tot
+    return out.view(L, K, G * G), out_pl
+
+
+def make_fields(grid: Grid, device="cpu", u0=40.0, noise=2.0, alpha=math.pi / 4, seed=SEED,
                 dtype=torch.float64):
-    """Shared per-step fields: rho, rhogvx/vy/vz (cell centres), rhogw (half levels)."""
+    """Shared per-step fields: rho, rhogvx/vy/vz (cell centres), rhogw (faces below each level).
+
+    The horizontal noise is a baroclinic, column-mass-neutral mode: a smoothed random tangent field
+    times a vertical profile A(z) with sum_k rho A dz = 0, RMS 2 m/s.  rhogw then follows from the
+    discrete continuity equation integrated upward from the ground (rhogw = 0 there and at the top),
+    so the density stays steady step after step (the literal per-level random w and divergent
+    noise drive rho to zero within a few steps once rho is advanced by the continuity equation)."""
     L, K, gall = grid.lall, grid.kall, grid.gall
     vg = grid.arrays
     z = torch.as_tensor(vg["z"], device=device)
+    dz = torch.as_tensor(vg["dz"], device=device)
     rho_k = 1.2 * torch.exp(-z / 8000.0)
     rho = rho_k.view(1, K, 1).expand(L, K, gall).contiguous()
     rho_pl = rho_k.view(1, K, 1).expand(2, K, 6).contiguous()
@@ -92,29 +153,44 @@ def make_fields(grid: Grid, device="cpu", u0=40.0, noise=2.0, wamp=0.05, alpha=m
                             axis[0] * p[1] - axis[1] * p[0]])
 
     rng = np.random.Generator(np.random.PCG64(seed))
-    nz = torch.as_tensor(rng.standard_normal((3, L, K, gall)), device=device)
-    nzp = torch.as_tensor(rng.standard_normal((3, 2, K, 6)), device=device)
+    nz = torch.as_tensor(rng.standard_normal((3, L, 1, gall)), device=device)
+    nzp = torch.as_tensor(rng.standard_normal((3, 2, 1, 6)), device=device)
     xe, xpe = x.unsqueeze(2), xp.unsqueeze(2)  # (3, L, 1, gall)
     nz = nz - (nz * xe).sum(0, keepdim=True) * xe
     nzp = nzp - (nzp * xpe).sum(0, keepdim=True) * xpe
     nz, nzp = halo_fill(grid, nz, nzp)
     nz, nzp = _smooth_columns(grid, nz, nzp)
-    sd = torch.cat([nz.reshape(3, -1), nzp.reshape(3, -1)], 1).norm(dim=0).pow(2).mean().div(2).sqrt()
-    v = u0 * rot(xe) + noise * nz / sd
-    vp = u0 * rot(xpe) + noise * nzp / sd
+    sd = torch.cat([nz.reshape(3, -1), nzp.reshape(3, -1)], 1).norm(dim=0).pow(2).mean().sqrt()
+    # vertical profile of the noise: one sign change, zero mass-weighted column mean, unit RMS
+    phys = torch.zeros(K, dtype=torch.bool, device=device)
+    phys[grid.kmin - 1:grid.kmax] = True
+    prof = torch.cos(math.pi * z / 40.0e3)
+    c = (rho_k * prof * dz)[phys].sum() / (rho_k * dz)[phys].sum()
+    prof = torch.where(phys, prof - c, torch.zeros_like(prof))
+    prof = prof / prof[phys].pow(2).mean().sqrt()
+    v = u0 * rot(xe) + noise * (nz / sd) * prof.view(1, 1, K, 1)
+    vp = u0 * rot(xpe) + noise * (nzp / sd) * prof.view(1, 1, K, 1)
     rhogv = v * rho.unsqueeze(0)
     rhogv_pl = vp * rho_pl.unsqueeze(0)
-    # vertical mass flux at half levels k = kmin+1..kmax (0 at the ground kmin and the top kmax+1)
-    w = torch.as_tensor(rng.standard_normal((L, K, gall)), device=device) * wamp
-    wp = torch.as_tensor(rng.standard_normal((2, K, 6)), device=device) * wamp
-    mask = torch.zeros(K, device=device, dtype=torch.float64)
-    mask[grid.kmin:grid.kmax] = 1.0  # 0-based kmin..kmax-1 = Fortran faces kmin+1..kmax
-    af = torch.as_tensor(vg["afact"], device=device)
-    bf = torch.as_tensor(vg["bfact"], device=device)
-    rho_face = af * rho_k + bf * torch.roll(rho_k, 1)
-    rho_face[0] = rho_k[0]
-    rhogw = w * (mask * rho_face).view(1, K, 1)
-    rhogw_pl = wp * (mask * rho_face).view(1, K, 1)
+    rhogv, rhogv_pl = halo_fill(grid, rhogv, rhogv_pl)
+    # vertical mass flux from continuity: rhogw(k+1) = rhogw(k) - hdiv(k) dz(k), ground and top = 0
+    hdiv, hdiv_pl = mass_flux_divergence(grid, rho, rhogv, rho_pl, rhogv_pl)
+    rhogw = torch.zeros(L, K, gall, dtype=torch.float64, device=device)
+    rhogw_pl = torch.zeros(2, K, 6, dtype=torch.float64, device=device)
+    for k in range(grid.kmin - 1, grid.kmax):  # faces kmin+1 .. kmax+1 (0-based k+1)
+        rhogw[:, k + 1] = rhogw[:, k] - hdiv[:, k] * dz[k]
+        rhogw_pl[:, k + 1] = rhogw_pl[:, k] - hdiv_pl[:, k] * dz[k]
+    # the column's net divergence (residual flux through the top) is spread over the column by
+    # mass, so the top flux is zero and rho changes by the same small fraction at every level
+    top = grid.kmax  # 0-based index of the top face kmax+1
+    cum = torch.zeros(K, dtype=torch.float64, device=device)
+    cum[grid.kmin - 1:top + 1] = torch.cat([torch.zeros(1, dtype=torch.float64, device=device),
+                                            torch.cumsum((rho_k * dz)[grid.kmin - 1:top], 0)])
+    cum = cum / cum[top]
+    rhogw = rhogw - rhogw[:, top:top + 1] * cum.view(1, K, 1)
+    rhogw_pl = rhogw_pl - rhogw_pl[:, top:top + 1] * cum.view(1, K, 1)
+    rhogw[:, top] = 0.0
+    rhogw_pl[:, top] = 0.0
     rhogw, rhogw_pl = halo_fill(grid, rhogw.unsqueeze(0), rhogw_pl.unsqueeze(0))
     out = dict(rhog=rho, rhog_pl=rho_pl, rhogvx=rhogv[0], rhogvx_pl=rhogv_pl[0], rhogvy=rhogv[1],
                rhogvy_pl=rhogv_pl[1], rhogvz=rhogv[2], rhogvz_pl=rhogv_pl[2], rhogw=rhogw[0], rhogw_pl=rhogw_pl[0])
