@@ -170,7 +170,7 @@ Ctx::~Ctx() {
   if (d_have_sgp) cudaFree(d_have_sgp);
   for (void *p : stepgeo)
     if (p) cudaFree(p);
-  for (void *p : {(void *)fast.bsrc, (void *)fast.blist, (void *)fast.ring, (void *)fast.cg32})
+  for (void *p : {(void *)fast.bsrc, (void *)fast.blist, (void *)fast.ring, (void *)fast.carry, (void *)fast.cg32})
     if (p) cudaFree(p);
   for (auto &ev : fast.events) cudaEventDestroy(ev.first), cudaEventDestroy(ev.second);
   if (stream) cudaStreamDestroy(stream);
@@ -647,14 +647,22 @@ int Ctx::build_fast_tables() {
   }
   for (int x : ring)
     if (x < 0) return set_error("fast tables: pole ring slot without a source"), ICA_ERR_INTERNAL;
+  // halo points no list writes (region corners at rlevel 0): the reference leaves them as they were
+  std::vector<int> carry;
+  for (int c = 0; c < npt; ++c)
+    if (bsrc[c] == -2) carry.push_back(c);
+  if (carry.empty()) carry.push_back(-1);  // keeps the device table non-empty; the kernel skips it
   fast.nb = (int)blist.size();
+  fast.ncarry = (int)carry.size();
   if (cudaMalloc(&fast.bsrc, bsrc.size() * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&fast.blist, blist.size() * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&fast.ring, ring.size() * sizeof(int)) != cudaSuccess)
+      cudaMalloc(&fast.ring, ring.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&fast.carry, carry.size() * sizeof(int)) != cudaSuccess)
     return set_error("cudaMalloc(fast tables)"), ICA_ERR_NOMEM;
   cudaMemcpy(fast.bsrc, bsrc.data(), bsrc.size() * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(fast.blist, blist.data(), blist.size() * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(fast.ring, ring.data(), ring.size() * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(fast.carry, carry.data(), carry.size() * sizeof(int), cudaMemcpyHostToDevice);
   fast.built = true;
   return ICA_OK;
 }
@@ -681,6 +689,7 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
   I.GRD_x = sg[0], I.GRD_x_pl = sg[1], I.cg = sg[2], I.cg_pl = sg[3], I.rdgz = sg[4], I.afact = sg[5], I.bfact = sg[6];
   I.cg32 = fast.cg32;
   I.bsrc = fast.bsrc, I.blist = fast.blist, I.pole_ring_b = fast.ring, I.nb = fast.nb;
+  I.carry = fast.carry, I.ncarry = fast.ncarry;
   const size_t nbb = (size_t)ntr * sz.kall * fast.nb * 5;
   I.bbuf = (double *)buf("fast_bbuf", nbb * sizeof(double));
   if (!I.bbuf) return set_error("cudaMalloc(fast boundary buffer)"), ICA_ERR_NOMEM;

@@ -27,7 +27,8 @@ struct Plan {  // composed halo fill on the device
 struct FastState {  // fused path: boundary tables, tile shape, kernel timing
   bool built = false;
   int nb = 0, shape = 0;
-  int *bsrc = nullptr, *blist = nullptr, *ring = nullptr;
+  int *bsrc = nullptr, *blist = nullptr, *ring = nullptr, *carry = nullptr;
+  int ncarry = 0;
   float *cg32 = nullptr;
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;

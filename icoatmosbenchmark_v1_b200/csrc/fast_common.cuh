@@ -29,6 +29,8 @@ struct FastInst {
   const int *blist;  // (nb): point index of boundary entry b (region cell, or pole centre when >= lall*gall)
   const int *pole_ring_b;  // (2, 5): boundary index feeding pole ring slot v = 2..6
   int nb;
+  const int *carry;  // (ncarry): region points no halo list writes; they keep their input values
+  int ncarry;
   double *bbuf;  // (ntr, K, nb, 5): grad x, y, z, Qout min, Qout max
 };
 

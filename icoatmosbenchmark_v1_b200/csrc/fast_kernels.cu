@@ -12,6 +12,7 @@
 //                    levels: fluxes (FP64, once per level), per tracer gradient,
 //                    Qout, upwind remap and limiter (FP32), FP64 update, and the
 //                    vertical sub-step streamed two levels behind in registers.
+//   k_fast_carry     halo points that no halo list writes keep their input values.
 //   gather           halo/pole fill of the new state (the COMM plan).
 //
 // Faces are "seam" faces when one of their two cells is a halo cell; the
@@ -713,6 +714,18 @@ __global__ void k_fast_pole(FastInst I) {
   }
 }
 
+// ---- halo points no list writes keep their input values (the reference never touches them)
+__global__ void k_fast_carry(FastInst I) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)I.ncarry * I.K) return;
+  const int p = I.carry[tid % I.ncarry], k = (int)(tid / I.ncarry);
+  if (p < 0) return;
+  const int l = p / I.gall, c = p % I.gall;
+  const size_t off = ((size_t)l * I.K + k) * I.gall + c, tstride = (size_t)I.lall * I.K * I.gall;
+  I.rho_out[off] = I.rho_in[off];
+  for (int t = 0; t < I.ntr; ++t) I.Q_out[(size_t)t * tstride + off] = I.Q_in[(size_t)t * tstride + off];
+}
+
 // ---------------------------------------------------------------------------------------
 template <int TX, int TY, int TG>
 static cudaError_t launch_tile(const FastInst &I, cudaStream_t st) {
@@ -754,7 +767,9 @@ cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t
     default: return cudaErrorInvalidValue;
   }
   if (ev1) cudaEventRecord(ev1, st);
-  launches += 3;
+  const long long nc = (long long)I.ncarry * I.K;
+  k_fast_carry<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(I);
+  launches += 4;
   return e;
 }
 

@@ -67,6 +67,18 @@ def rel_err(a, b):
     return float(np.abs(a - b).max() / den)
 
 
+def qout_mask(ch, ch_pl, thr=1e-2):
+    """Cells whose Thuburn outflow bounds are well conditioned: outflow Courant sum
+    Cout = sum_m max(ch_m, 0) either 0 or >= thr (regions (lall,K,gall); poles (2,K)).
+    The bounds are (q - qnmax) / Cout + ... : loose (harmless) when Cout is small, but
+    the FP32 and FP64 builds of the reference switch to the zero-outflow form below
+    their own EPS (1.2e-7 vs 2.2e-16) and in between return values that differ by
+    orders of magnitude, so those cells' Qout is not compared between precisions."""
+    cout = np.maximum(ch, 0).sum(axis=0)
+    cout_pl = np.maximum(ch_pl[..., 1:], 0).sum(axis=-1)
+    return (cout == 0) | (cout >= thr), (cout_pl == 0) | (cout_pl >= thr)
+
+
 def interior(a, grid):
     """Values of a (..., lall, K, gall) at interior cells: shape (..., K, n_interior)."""
     m = grid.interior_mask()
