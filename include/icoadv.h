@@ -18,7 +18,7 @@
  * variants take device pointers of the same shapes and are asynchronous on
  * the context's stream (ica_stream).  Every function returns ICA_OK (0) or a
  * negative ICA_ERR_* code; the reference has no status returns (it stops),
- * the Fortran shim in INTEGRATION.md turns a nonzero status into STOP.
+ * so a Fortran shim over this header turns a nonzero status into STOP.
  *
  * Precision: the reference selects RP at compile time (mod_precision.f90:19-26);
  * here the unsuffixed entry points are RP = DP (double), the *_f32 ones are
