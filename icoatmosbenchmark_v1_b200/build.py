@@ -31,6 +31,7 @@ SOURCES = {
     "plain_kernels.cu": ["--fmad=false"],
     "step.cu": ["--fmad=false"],
     "fast_kernels.cu": [],
+    "noalloc.cu": [],
 }
 
 

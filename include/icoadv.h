@@ -152,6 +152,27 @@ int ica_horizontal_limiter_thuburn_f32(ica_ctx *ctx,
                                        float *Qout_prev, float *Qout_prev_pl,
                                        const float *Qout_post, const float *Qout_post_pl);
 
+/* ica_horizontal_limiter_thuburn_dev without any device allocation.  No reference
+ * counterpart: it serves callers that cannot let a library allocate device memory
+ * after start-up (a host model whose pool allocator owns the GPU, a run whose
+ * footprint must stay fixed).  The scratch (the Qout copy the halo fill runs on and
+ * the pole inflow bounds) is a fixed array in the library's device memory, about
+ * 32 MiB on every GPU the library is loaded on.  The first call on a device looks up
+ * that array's address; make it before any stream capture.  Grids with
+ * gall*kall*lall > ICA_NOALLOC_MAX_CELLS or kall > ICA_NOALLOC_MAX_KALL get
+ * ICA_ERR_ARG.  Nothing needs to start at zero.  All calls share the one array, so
+ * calls that overlap on a GPU (other streams, other host threads) race. */
+#define ICA_NOALLOC_MAX_CELLS 2097152
+#define ICA_NOALLOC_MAX_KALL 256
+int ica_horizontal_limiter_thuburn_noalloc(ica_ctx *ctx,
+                                           double *q_a, double *q_a_pl,
+                                           const double *q, const double *q_pl,
+                                           const double *d, const double *d_pl,
+                                           const double *ch, const double *ch_pl,
+                                           const double *cmask, const double *cmask_pl,
+                                           double *Qout_prev, double *Qout_prev_pl,
+                                           const double *Qout_post, const double *Qout_post_pl);
+
 /* ---- vertical_limiter_thuburn:
  *      kernels/NICAM/dyn_vert_adv_limiter/src/mod_src_tracer.f90:41-45,60-67
  * inout q_h(gall,kall,lall) q_h_pl(6,kall,2)
