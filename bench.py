@@ -193,7 +193,10 @@ def run_ours(args, world, rank, local):
         dtype = "f64"
         s_bytes = 48
     else:
-        runner = ctx.fast_runner(g, st, f, dt)
+        runner = ctx.fast_runner(g, st, f, dt, autotune=args.tile_shape < 0)
+        if args.tile_shape >= 0:
+            ctx.fast_set_shape(args.tile_shape)
+            runner.shape = args.tile_shape
         step = runner.step
         st = runner.state
         dtype = "f32"
@@ -251,8 +254,8 @@ def run_ours(args, world, rank, local):
                          f"({cupd:.3e} updates, {cel:.1f} s)"}
     cfg = workload_config(args)
     if args.mode != "plain":
-        cfg["tile"] = {"shape_txtytg": list(runner.tuning[runner.shape]["shape"]) if runner.tuning else None,
-                       "autotune_ms": [round(t["ms"], 3) for t in runner.tuning]}
+        cfg["tile"] = {"shape_txtytg": list(ctx.fast_shapes()[runner.shape]),
+                       "autotune_ms": [round(t["ms"], 3) for t in runner.tuning] or None}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -310,6 +313,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tile-shape", type=int, default=-1, help="fused tile shape index (default: autotune)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")
     args = ap.parse_args()

@@ -12,12 +12,16 @@ Arrays are numpy (host) or torch CUDA tensors (device), C-contiguous, in the
 reference's Fortran layout written in C order: var(gall,kall,lall,m) has
 shape (m, lall, kall, gall).  Host arrays go through the host-pointer entry
 points (copy in, run, copy out); CUDA tensors go through the *_dev entry
-points on the context's stream.  Errors raise IcoAdvError with the library's
+points on the context's stream, ordered after the work already queued on
+torch's current stream and before anything queued there afterwards (event
+waits, no host synchronisation), so tensors can be handed back and forth
+with torch without explicit synchronisation.  Errors raise IcoAdvError with the library's
 message.  There is no CPU fallback: without the built library or a B200 the
 calls fail.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 from pathlib import Path
 
@@ -144,11 +148,13 @@ class IcoAdv:
         _check("ica_get_sizes", lib().ica_get_sizes(self.h, C.byref(s)))
         self.sizes = s
         self.glevel, self.rlevel, self.vlayer, self.device = glevel, rlevel, vlayer, device
+        self._ext = None
 
     def close(self):
         if self.h:
             lib().ica_finalize(self.h)
             self.h = C.c_void_p()
+            self._ext = None
 
     def __del__(self):
         try:
@@ -159,6 +165,21 @@ class IcoAdv:
     @property
     def stream(self):
         return lib().ica_stream(self.h)
+
+    @contextlib.contextmanager
+    def _ordered(self, dev=True):
+        """Stream order of a device call against torch's current stream: the context
+        stream waits for what torch queued before it, torch waits for the call."""
+        if not dev:
+            yield
+            return
+        import torch
+        if self._ext is None:
+            self._ext = torch.cuda.ExternalStream(self.stream, device=self.device)
+        cur = torch.cuda.current_stream(self.device)
+        self._ext.wait_stream(cur)
+        yield
+        cur.wait_stream(self._ext)
 
     @property
     def launch_count(self):
@@ -181,7 +202,8 @@ class IcoAdv:
                 raise TypeError(f"{name}: FP32 entry points take host arrays")
             suffix = "_f32"
         fn = getattr(lib(), name + suffix)
-        _check(name + suffix, fn(self.h, *ptrs, *scalars))
+        with self._ordered(dev):
+            _check(name + suffix, fn(self.h, *ptrs, *scalars))
 
     @staticmethod
     def _dtype(a):
@@ -205,7 +227,8 @@ class IcoAdv:
         post = [_ptr(Qout_post, t)[0], _ptr(Qout_post_pl, t)[0]]
         dev = kinds[0]
         name = "ica_horizontal_limiter_thuburn" + ("_dev" if dev else ("_f32" if t == np.float32 else ""))
-        _check(name, getattr(lib(), name)(self.h, *ptrs, *post))
+        with self._ordered(dev):
+            _check(name, getattr(lib(), name)(self.h, *ptrs, *post))
 
     def vertical_limiter_thuburn(self, q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl):
         self._call("ica_vertical_limiter_thuburn", self._dtype(q), [q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl])
@@ -239,7 +262,8 @@ class IcoAdv:
         arrs = [rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz, rhogvz_pl, rhogw, rhogw_pl]
         ptrs, kinds = zip(*[_ptr(a, np.float64) for a in arrs])
         name = "ica_advect_step" + ("_dev" if kinds[0] else "")
-        _check(name, getattr(lib(), name)(self.h, int(ntr), C.c_double(dt), *ptrs))
+        with self._ordered(bool(kinds[0])):
+            _check(name, getattr(lib(), name)(self.h, int(ntr), C.c_double(dt), *ptrs))
 
     # ---- fused batched path ------------------------------------------------------
     def advect_fast_dev(self, dt, state_in, state_out, fields32):
@@ -249,7 +273,9 @@ class IcoAdv:
         sp = [_ptr(state_in[k], np.float64)[0] for k in STATE_KEYS]
         so = [_ptr(state_out[k], np.float64)[0] for k in STATE_KEYS]
         fp = [_ptr(fields32[k], np.float32)[0] for k in FIELD_KEYS]
-        _check("ica_advect_fast_dev", lib().ica_advect_fast_dev(self.h, int(ntr), C.c_double(dt), *sp, *so, *fp))
+        with self._ordered():
+            _check("ica_advect_fast_dev", lib().ica_advect_fast_dev(self.h, int(ntr), C.c_double(dt), *sp, *so,
+                                                                    *fp))
 
     def advect_fast_host(self, dt, rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz,
                          rhogvz_pl, rhogw, rhogw_pl):
