@@ -149,6 +149,7 @@ int ica_set_geometry(ica_ctx *c, const double *GRD_xr, const double *GRD_xr_pl, 
   const size_t gl = (size_t)c->sz.gall * c->sz.lall, pl = (size_t)kGallPl * kLallPl;
   const double *h[8] = {GRD_xr, GRD_xr_pl, GMTR_p, GMTR_p_pl, GMTR_t, GMTR_t_pl, GMTR_a, GMTR_a_pl};
   const size_t n[8] = {gl * 9, pl * 3, gl * 8, pl * 8, gl * 10, pl * 5, gl * 36, pl * 18};
+  c->fast.off_ready = false;
   return c->upload_geometry(h, n);
 }
 
@@ -170,7 +171,8 @@ Ctx::~Ctx() {
   if (d_have_sgp) cudaFree(d_have_sgp);
   for (void *p : stepgeo)
     if (p) cudaFree(p);
-  for (void *p : {(void *)fast.bsrc, (void *)fast.blist, (void *)fast.ring, (void *)fast.carry, (void *)fast.cg32})
+  for (void *p : {(void *)fast.bsrc, (void *)fast.blist, (void *)fast.ring, (void *)fast.carry, (void *)fast.cg32,
+                  (void *)fast.off32})
     if (p) cudaFree(p);
   for (auto &ev : fast.events) cudaEventDestroy(ev.first), cudaEventDestroy(ev.second);
   if (stream) cudaStreamDestroy(stream);
@@ -548,6 +550,7 @@ int ica_set_step_geometry(ica_ctx *c, const double *GRD_x, const double *GRD_x_p
   cudaError_t e = cudaMemcpy(c->fast.cg32, cg32.data(), n[2] * sizeof(float), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(coef_grad fp32)");
   c->stepgeo_set = true;
+  c->fast.off_ready = false;
   return ICA_OK;
 }
 
@@ -688,6 +691,15 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
   const double *const *sg = (const double *const *)stepgeo;
   I.GRD_x = sg[0], I.GRD_x_pl = sg[1], I.cg = sg[2], I.cg_pl = sg[3], I.rdgz = sg[4], I.afact = sg[5], I.bfact = sg[6];
   I.cg32 = fast.cg32;
+  if (!fast.off_ready) {
+    const size_t noff = (size_t)sz.lall * 18 * sz.gall;
+    if (!fast.off32 && cudaMalloc(&fast.off32, noff * sizeof(float)) != cudaSuccess)
+      return set_error("cudaMalloc(fast remap offsets)"), ICA_ERR_NOMEM;
+    cudaError_t e = fast_build_offsets(I, fast.off32, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "fast remap offsets");
+    fast.off_ready = true;
+  }
+  I.off32 = fast.off32;
   I.bsrc = fast.bsrc, I.blist = fast.blist, I.pole_ring_b = fast.ring, I.nb = fast.nb;
   I.carry = fast.carry, I.ncarry = fast.ncarry;
   const size_t nbb = (size_t)ntr * sz.kall * fast.nb * 5;

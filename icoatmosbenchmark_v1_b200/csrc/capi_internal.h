@@ -30,6 +30,8 @@ struct FastState {  // fused path: boundary tables, tile shape, kernel timing
   int *bsrc = nullptr, *blist = nullptr, *ring = nullptr, *carry = nullptr;
   int ncarry = 0;
   float *cg32 = nullptr;
+  float *off32 = nullptr;  // per-face remap offsets, rebuilt when the geometry changes
+  bool off_ready = false;
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
 };

@@ -19,7 +19,8 @@ struct FastInst {
   const int *have_sgp;
   const double *GMTR_p, *GMTR_t, *GMTR_a, *GRD_xr, *GRD_x, *cg;
   const double *GMTR_p_pl, *GMTR_t_pl, *GMTR_a_pl, *GRD_xr_pl, *GRD_x_pl, *cg_pl;
-  const float *cg32;  // coef_grad in FP32, (lall, 3, 7, gall)
+  const float *cg32;   // coef_grad in FP32, (lall, 3, 7, gall)
+  const float *off32;  // remap offsets GRD_xr - GRD_x per face, FP32, (lall, 18, gall)
   const double *rdgz, *afact, *bfact;
   const float *vx, *vy, *vz, *w, *vx_pl, *vy_pl, *vz_pl, *w_pl;
   const double *rho_in, *rho_in_pl, *Q_in, *Q_in_pl;

@@ -6,20 +6,26 @@
 //                    region-boundary cell and both pole centres, into bbuf.  These
 //                    are exactly the values the reference's two mid-step halo
 //                    exchanges (grad q and Qout, mod_src_tracer.f90:371) would move
-//                    into other regions' halos, so no exchange is needed.
+//                    into other regions' halos, so no exchange is needed.  One
+//                    thread per (cell, level): the face geometry once, then the tracers.
 //   k_fast_pole      the two pole centres (horizontal + vertical), FP64.
-//   k_fast_tile      one CTA per (region tile, group of TG tracers), looping over the
-//                    levels: fluxes (FP64, once per level), per tracer gradient,
-//                    Qout, upwind remap and limiter (FP32), FP64 update, and the
-//                    vertical sub-step streamed two levels behind in registers.
+//   k_fast_tile      one CTA per (region tile, group of TG tracers), one thread per
+//                    cell of the tile and its 1-wide ring, looping over the levels:
+//                    per level the tracer-independent part (triangle values, face
+//                    fluxes, Courant numbers, upwind masks and remap offsets) once,
+//                    then three phases over the TG tracers (q; gradient + Qout;
+//                    limited face values), the FP64 update and the vertical sub-step
+//                    streamed two levels behind in registers.
 //   k_fast_carry     halo points that no halo list writes keep their input values.
 //   gather           halo/pole fill of the new state (the COMM plan).
 //
 // Faces are "seam" faces when one of their two cells is a halo cell; the
 // neighbouring region computes the same face from its own halo copy, so those
-// faces are done in FP64 (k_fast_tile calls seam_face) to keep the flux form
-// conservative to rounding of FP64.  Interior faces are computed by the same
-// code in every tile that touches them, so they cancel exactly.
+// faces are done in FP64 (seam_face) from the FP64 boundary values.  An interior
+// face is computed by every tile that needs it from the same inputs by the same
+// instructions (cell positions enter only through the per-face offsets
+// GRD_xr - GRD_x, fixed per face), so both of its cells see the same value and
+// the flux form conserves mass to FP64 rounding.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -79,12 +85,10 @@ __device__ void pole_faces(const FastInst &I, int p, int k, double flux[7], doub
   }
 }
 
-// Qout of pole centre p at level k for tracer t (mod_src_tracer.f90:307-363), d = 0
-__device__ void pole_qout(const FastInst &I, int p, int k, int t, const double flux[7], double &Qmin, double &Qmax) {
+// Qout of pole centre p at level k (mod_src_tracer.f90:307-363), d = 0, from q at its 6 points
+__device__ void pole_qout(const FastInst &I, int p, int k, const double q[7], const double flux[7], double &Qmin,
+                          double &Qmax) {
   const size_t off = ((size_t)p * I.K + k) * kGallPl;
-  const size_t toff = (size_t)t * kLallPl * I.K * kGallPl;
-  double q[7];
-  for (int v = 1; v <= 6; ++v) q[v] = I.Q_in_pl[toff + off + v - 1] / I.rho_in_pl[off + v - 1];
   const double rarea = I.GMTR_p_pl[((size_t)(P_RAREA - 1) * kLallPl + p) * kGallPl];
   const double BIG = DBL_MAX, EPS = DBL_EPSILON;
   double qmin1[7], qmax1[7], chm[7], ch[7];
@@ -113,89 +117,108 @@ __device__ void pole_qout(const FastInst &I, int p, int k, int t, const double f
   Qmax = (qn - CQmin - qnmin * (1.0 - Cin - Cout + 0.0)) / (Cout + zerosw) * (1.0 - zerosw) + qn * zerosw;
 }
 
-// ---- FP64 gradient and Qout of an interior region cell (i,j) (boundary pass)
-__device__ void cell_grad_qout64(const FastInst &I, int l, int k, int t, int i, int j, double out[5]) {
+// ---- boundary pass: FP64 gradient and Qout (mod_src_tracer.f90:143-282, d = 0) of the
+// region-boundary cells and the pole centres, one thread per (entry, level), all tracers.
+__global__ void k_fast_boundary(FastInst I) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)I.nb * (I.K - 2)) return;
+  const int b = (int)(tid % I.nb);
+  const int k = 1 + (int)(tid / I.nb);
+  const int p = I.blist[b];
+  const size_t tstride = (size_t)I.lall * I.K * I.gall;
+  double *dst0 = I.bbuf + ((size_t)k * I.nb + b) * 5;
+  const size_t dstride = (size_t)I.K * I.nb * 5;  // next tracer
+  if (p >= I.lall * I.gall) {  // pole centre
+    const int pl = (p - I.lall * I.gall) / kGallPl;
+    const size_t off = ((size_t)pl * I.K + k) * kGallPl;
+    const size_t tsp = (size_t)kLallPl * I.K * kGallPl;
+    double flux[7], xc[7][3], rinv[7];
+    pole_faces(I, pl, k, flux, xc);
+    for (int v = 1; v <= 6; ++v) rinv[v] = 1.0 / I.rho_in_pl[off + v - 1];
+    for (int t = 0; t < I.ntr; ++t) {
+      double q[7], out[5];
+      for (int v = 1; v <= 6; ++v) q[v] = I.Q_in_pl[t * tsp + off + v - 1] * rinv[v];
+      for (int x = 0; x < 3; ++x) {
+        const double *cx = I.cg_pl + ((size_t)pl * 3 + x) * 6;
+        double s = cx[0] * q[1];
+        for (int v = 2; v <= 6; ++v) s = s + cx[v - 1] * q[v];
+        out[x] = s;
+      }
+      pole_qout(I, pl, k, q, flux, out[3], out[4]);
+      double *dst = dst0 + t * dstride;
+      for (int x = 0; x < 5; ++x) dst[x] = out[x];
+    }
+    return;
+  }
+  const int l = p / I.gall, c = p % I.gall;
+  const int G = I.G, i = c % G + 1, j = c / G + 1;
   const bool sgp = I.have_sgp[l] != 0;
   const GFields f{&I, l, k};
-  const GQ q{&I, l, k, t};
-  const int G = I.G, c = (j - 1) * G + (i - 1);
-  // gradient (stencil of OPRT_gradient_setup), neighbour order ij, ip1j, ip1jp1, ijp1, im1j, im1jm1, ijm1
-  const int di[7] = {0, 1, 1, 0, -1, -1, 0}, dj[7] = {0, 0, 1, 1, 0, -1, -1};
-  double qs[7];
-  for (int n = 0; n < 7; ++n) qs[n] = q(i + di[n], j + dj[n]);
-  for (int x = 0; x < 3; ++x) {
-    const double *cx = I.cg + ((size_t)l * 3 + x) * 7 * I.gall + c;
-    double s = cx[0] * qs[0];
-    for (int n = 1; n <= 6; ++n) s = s + cx[(size_t)n * I.gall] * qs[n];
-    out[x] = s;
-  }
-  // Qout (mod_src_tracer.f90:143-282) with d = 0
   const double BIG = DBL_MAX, EPS = DBL_EPSILON;
+  // tracer-independent: Courant numbers and upwind masks of the 6 faces, 1/rho on the 3x3 block
   const int oi[7] = {0, i, i, i, i - 1, i - 1, i}, oj[7] = {0, j, j, j, j, j - 1, j - 1};
   const int fa[7] = {0, AI, AIJ, AJ, AI, AIJ, AJ};
   const double rho_c = f(0, i, j), ra_c = rarea(I, l, i, j);
-  double qmn[7], qmx[7], ch[7], chm[7];
+  double ch[7], chm[7], cmk[7];
   for (int m = 1; m <= 6; ++m) {
-    double xc[3];
+    double xcv[3];
     const bool ex = face_exists(I, oi[m], oj[m], fa[m]);
-    const double fl = ex ? face_geo(I, l, oi[m], oj[m], fa[m], sgp, f, xc) : 0.0;
+    const double fl = ex ? face_geo(I, l, oi[m], oj[m], fa[m], sgp, f, xcv) : 0.0;
     const double flx = ex ? cell_flx(I, l, i, j, m, sgp, fl, ra_c) : 0.0;
     ch[m] = flx / rho_c;
     chm[m] = mn64(ch[m], 0.0);
-    // upwind mask of the face, from its owner's Courant number
     const double ch_own = (m <= 3) ? ch[m] : (fl * rarea(I, l, oi[m], oj[m]) * I.dt) / f(0, oi[m], oj[m]);
-    const double cm = 0.5 - fsg(0.5, ch_own - EPS);
-    double lo, hi;
-    bounds64(I, oi[m], oj[m], fa[m], sgp, q, lo, hi);
-    if (m <= 3) qmn[m] = cm * lo + (1.0 - cm) * BIG, qmx[m] = cm * hi + (1.0 - cm) * (-BIG);
-    else qmn[m] = cm * BIG + (1.0 - cm) * lo, qmx[m] = cm * (-BIG) + (1.0 - cm) * hi;
+    cmk[m] = 0.5 - fsg(0.5, ch_own - EPS);
   }
-  const double q0 = qs[0];
-  double qnmin = q0, qnmax = q0;
-  for (int m = 1; m <= 6; ++m) qnmin = mn64(qnmin, qmn[m]);
-  for (int m = 1; m <= 6; ++m) qnmax = mx64(qnmax, qmx[m]);
   const double Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
   const double Cout =
       ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
-  const double CQmin = chm[1] * qmn[1] + chm[2] * qmn[2] + chm[3] * qmn[3] + chm[4] * qmn[4] + chm[5] * qmn[5] +
-                       chm[6] * qmn[6];
-  const double CQmax = chm[1] * qmx[1] + chm[2] * qmx[2] + chm[3] * qmx[3] + chm[4] * qmx[4] + chm[5] * qmx[5] +
-                       chm[6] * qmx[6];
   const double zerosw = 0.5 - fsg(0.5, fabs(Cout) - EPS);
-  out[3] = (q0 - CQmax - qnmax * (1.0 - Cin - Cout + 0.0)) / (Cout + zerosw) * (1.0 - zerosw) + q0 * zerosw;
-  out[4] = (q0 - CQmin - qnmin * (1.0 - Cin - Cout + 0.0)) / (Cout + zerosw) * (1.0 - zerosw) + q0 * zerosw;
-}
-
-__global__ void k_fast_boundary(FastInst I) {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long total = (long long)I.nb * (I.K - 2) * I.ntr;
-  if (tid >= total) return;
-  const int b = (int)(tid % I.nb);
-  const long long r = tid / I.nb;
-  const int k = 1 + (int)(r % (I.K - 2)), t = (int)(r / (I.K - 2));
-  double out[5];
-  const int p = I.blist[b];
-  if (p < I.lall * I.gall) {
-    const int l = p / I.gall, c = p % I.gall;
-    cell_grad_qout64(I, l, k, t, c % I.G + 1, c / I.G + 1, out);
-  } else {  // pole centre
-    const int pl = (p - I.lall * I.gall) / kGallPl;
-    const size_t off = ((size_t)pl * I.K + k) * kGallPl;
-    const size_t toff = (size_t)t * kLallPl * I.K * kGallPl;
-    double q[7];
-    for (int v = 1; v <= 6; ++v) q[v] = I.Q_in_pl[toff + off + v - 1] / I.rho_in_pl[off + v - 1];
+  double rinv[3][3];
+  for (int dj = 0; dj < 3; ++dj)
+    for (int di = 0; di < 3; ++di) rinv[dj][di] = 1.0 / f(0, i - 1 + di, j - 1 + dj);
+  double cgr[3][7];
+  for (int x = 0; x < 3; ++x)
+    for (int n = 0; n < 7; ++n) cgr[x][n] = I.cg[(((size_t)l * 3 + x) * 7 + n) * I.gall + c];
+  const int di7[7] = {0, 1, 1, 0, -1, -1, 0}, dj7[7] = {0, 0, 1, 1, 0, -1, -1};
+  for (int t = 0; t < I.ntr; ++t) {
+    const double *Qt = I.Q_in + t * tstride + ((size_t)l * I.K + k) * I.gall;
+    double q9[3][3];
+    for (int dj = 0; dj < 3; ++dj)
+      for (int di = 0; di < 3; ++di) q9[dj][di] = Qt[(size_t)(j - 2 + dj) * G + (i - 2 + di)] * rinv[dj][di];
+    // q at (ii,jj): the 3x3 block around the cell, else directly
+    auto q = [&](int ii, int jj) -> double {
+      const int a = ii - i + 1, bb = jj - j + 1;
+      if (a >= 0 && a < 3 && bb >= 0 && bb < 3) return q9[bb][a];
+      return Qt[(size_t)(jj - 1) * G + (ii - 1)] / f(0, ii, jj);
+    };
+    double out[5];
     for (int x = 0; x < 3; ++x) {
-      const double *cx = I.cg_pl + ((size_t)pl * 3 + x) * 6;
-      double s = cx[0] * q[1];
-      for (int v = 2; v <= 6; ++v) s = s + cx[v - 1] * q[v];
+      double s = cgr[x][0] * q9[1][1];
+      for (int n = 1; n <= 6; ++n) s = s + cgr[x][n] * q9[1 + dj7[n]][1 + di7[n]];
       out[x] = s;
     }
-    double flux[7], xc[7][3];
-    pole_faces(I, pl, k, flux, xc);
-    pole_qout(I, pl, k, t, flux, out[3], out[4]);
+    double qmn[7], qmx[7];
+    for (int m = 1; m <= 6; ++m) {
+      double lo, hi;
+      bounds64(I, oi[m], oj[m], fa[m], sgp, q, lo, hi);
+      const double cm = cmk[m];
+      if (m <= 3) qmn[m] = cm * lo + (1.0 - cm) * BIG, qmx[m] = cm * hi + (1.0 - cm) * (-BIG);
+      else qmn[m] = cm * BIG + (1.0 - cm) * lo, qmx[m] = cm * (-BIG) + (1.0 - cm) * hi;
+    }
+    const double q0 = q9[1][1];
+    double qnmin = q0, qnmax = q0;
+    for (int m = 1; m <= 6; ++m) qnmin = mn64(qnmin, qmn[m]);
+    for (int m = 1; m <= 6; ++m) qnmax = mx64(qnmax, qmx[m]);
+    const double CQmin = chm[1] * qmn[1] + chm[2] * qmn[2] + chm[3] * qmn[3] + chm[4] * qmn[4] + chm[5] * qmn[5] +
+                         chm[6] * qmn[6];
+    const double CQmax = chm[1] * qmx[1] + chm[2] * qmx[2] + chm[3] * qmx[3] + chm[4] * qmx[4] + chm[5] * qmx[5] +
+                         chm[6] * qmx[6];
+    out[3] = (q0 - CQmax - qnmax * (1.0 - Cin - Cout + 0.0)) / (Cout + zerosw) * (1.0 - zerosw) + q0 * zerosw;
+    out[4] = (q0 - CQmin - qnmin * (1.0 - Cin - Cout + 0.0)) / (Cout + zerosw) * (1.0 - zerosw) + q0 * zerosw;
+    double *dst = dst0 + t * dstride;
+    for (int x = 0; x < 5; ++x) dst[x] = out[x];
   }
-  double *dst = I.bbuf + (((size_t)t * I.K + k) * I.nb + b) * 5;
-  for (int x = 0; x < 5; ++x) dst[x] = out[x];
 }
 
 __device__ __forceinline__ const double *bval(const FastInst &I, int t, int k, int b) {
@@ -235,25 +258,63 @@ __device__ double seam_face(const FastInst &I, int l, int k, int t, int i, int j
   return v;
 }
 
+// ---- per-face remap offsets GRD_xr - GRD_x of the owner and of the neighbour (FP32),
+// fixed per face, so an interior face value does not depend on the tile that computes it.
+// off32 (lall, 18, gall): [a*6 + x] owner side, [a*6 + 3 + x] neighbour side, a = face 0..2
+__global__ void k_fast_offsets(FastInst I, float *off) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)I.lall * I.gall) return;
+  const int l = (int)(tid / I.gall), c = (int)(tid % I.gall);
+  const int G = I.G, i = c % G + 1, j = c / G + 1;
+  for (int a = 1; a <= 3; ++a) {
+    const int ni = (a == AI || a == AIJ) ? i + 1 : i, nj = (a == AIJ || a == AJ) ? j + 1 : j;
+    const bool nok = ni <= G && nj <= G;
+    for (int x = 0; x < 3; ++x) {
+      const double xr = gxr(I, l, i, j, a, x + 1);
+      off[((size_t)l * 18 + (a - 1) * 6 + x) * I.gall + c] = (float)(xr - gx(I, l, i, j, x));
+      off[((size_t)l * 18 + (a - 1) * 6 + 3 + x) * I.gall + c] = nok ? (float)(xr - gx(I, l, ni, nj, x)) : 0.0f;
+    }
+  }
+}
+
 // ---- the fused tile kernel ----------------------------------------------------------
-// local frame: region coords (i,j) -> local (i - i0 + 3, j - j0 + 3), size (TX+5) x (TY+5)
+// Local frame: cell (i,j) of the region -> (x,y) = (i - i0, j - j0); the tile is
+// x in [0,TX), y in [0,TY); the ring (one thread per cell) x in [-1,TX], y in [-1,TY];
+// the window of shared per-cell data x in [-3,TX+1], y in [-3,TY+1].
 template <int TX, int TY>
-struct TileSmem {
-  static constexpr int W = TX + 5, H = TY + 5, N = W * H;
-  double rho[N];
-  double flux[3][N];
-  double qa[3][N];
-  float v[3][N];
-  float xc[3][3][N];
-  float cm[3][N];
-  float q[N];
-  float gq[5][N];
+struct TileGeo {
+  static constexpr int RW = TX + 2, RH = TY + 2, NT = RW * RH;
+  static constexpr int WW = TX + 5, WH = TY + 5, NW = WW * WH;
 };
 
 template <int TX, int TY, int TG>
-__global__ void __launch_bounds__(TX *TY) k_fast_tile(FastInst I) {
-  using S = TileSmem<TX, TY>;
-  constexpr int W = S::W, N = S::N, NT = TX * TY;
+struct TileSmem {
+  static constexpr int NT = TileGeo<TX, TY>::NT, NW = TileGeo<TX, TY>::NW;
+  float cg[21][NT];   // gradient coefficients of ring cells, [x*7 + n] (level-invariant)
+  float off[18][NT];  // remap offsets of the faces of ring cells (level-invariant)
+  double rinv[NW];    // 1 / rho
+  double F[3][NW];    // face flux 0.5 (rhov . HN) by owner (FP32 arithmetic on interior faces)
+  double flx[6][NT];  // flx_h of the tile cells (FP64)
+  float rho[NW];
+  float v[3][NW];
+  float q[TG][NW];
+  union {
+    struct {
+      float gq[TG][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
+      float qa[TG][3][NT];  // limited face values of the faces owned by ring cells
+    } t;
+    struct {
+      float tri[2][4][NW];   // rho, rhovx, rhovy, rhovz at TI / TJ
+      float disp[3][3][NW];  // -rhov rr dt / 2 of each face: GRD_xc - GRD_xr
+    } f;
+  } u;
+};
+
+template <int TX, int TY, int TG>
+__global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I) {
+  using Gm = TileGeo<TX, TY>;
+  using S = TileSmem<TX, TY, TG>;
+  constexpr int RW = Gm::RW, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S &s = *reinterpret_cast<S *>(smem_raw);
 
@@ -267,32 +328,52 @@ __global__ void __launch_bounds__(TX *TY) k_fast_tile(FastInst I) {
   const int t0 = grp * TG;
   const int ntg = min(TG, I.ntr - t0);
   const int tid = threadIdx.x;
-  const int ti = tid % TX, tj = tid / TX;
-  const int ci = i0 + ti, cj = j0 + tj;  // this thread's cell
-  const bool active = ci <= I.gmax && cj <= I.gmax;
-  const bool sgp = I.have_sgp[l] != 0;
   const int G = I.G, K = I.K;
+  const bool sgp = I.have_sgp[l] != 0;
   const size_t slab = (size_t)I.gall, lk = (size_t)K * I.gall, tstride = (size_t)I.lall * K * I.gall;
   const double dt = I.dt;
-  const double ra_c = active ? rarea(I, l, ci, cj) : 1.0;
-  const size_t ccell = (size_t)(cj - 1) * G + (ci - 1);
-  auto LI = [&](int i, int j) { return (j - j0 + 3) * W + (i - i0 + 3); };
-  auto inreg = [&](int i, int j) { return i >= 1 && i <= G && j >= 1 && j <= G; };
+  const float dtf = (float)dt;
+  const float BIGf = FLT_MAX, EPSf = FLT_EPSILON;
+
+  // this thread's ring cell
+  const int x = tid % RW - 1, y = tid / RW - 1;
+  const int ci = i0 + x, cj = j0 + y;
+  const int ec = (y + 3) * WW + (x + 3);
+  const bool in_arr = ci >= 1 && ci <= G && cj >= 1 && cj <= G;
   auto interior = [&](int i, int j) { return i >= I.gmin && i <= I.gmax && j >= I.gmin && j <= I.gmax; };
+  const bool c_int = in_arr && interior(ci, cj);
+  const int bs = in_arr ? I.bsrc[(size_t)l * I.gall + (cj - 1) * G + (ci - 1)] : -3;
+  const bool fp32_cell = c_int && bs == -1;                      // gradient / Qout in FP32 here
+  const bool active = x >= 0 && x < TX && y >= 0 && y < TY && c_int;  // updated by this thread
+  const bool owner = x < TX && y < TY && in_arr;                     // face values of its 3 faces
+  const size_t ccell = (size_t)(cj - 1) * G + (ci - 1);
+  const double ra64 = c_int ? rarea(I, l, ci, cj) : 1.0;
+  const float ra32 = (float)ra64;
+
+  // ---- level-invariant tables of the ring cells
+  for (int n = 0; n < 21; ++n)
+    s.cg[n][tid] = fp32_cell ? I.cg32[((size_t)l * 21 + n) * I.gall + ccell] : 0.0f;
+  for (int n = 0; n < 18; ++n)
+    s.off[n][tid] = (owner && ci <= G - 1 && cj <= G - 1) ? I.off32[((size_t)l * 18 + n) * I.gall + ccell] : 0.0f;
 
   // vertical window, per tracer of the group (registers)
   double Qh[TG][3];
   float qv[TG][3], qmn_km1[TG], qmx_km1[TG], qh_last[TG];
-  double rh[3];    // rho after the horizontal sub-step at levels k-2, k-1, k
-  float ck1w[3];   // ck(k,1) at levels k-2..k
+  double rh[3];   // rho after the horizontal sub-step at levels k-2, k-1, k
+  float ck1w[3];  // ck(k,1) at levels k-2..k
   float ck2w[3];
-  float wf[3];     // rhogw at faces k-2..k (face k = below level k)
-  double rnew_prev = 0.0;
-  (void)rnew_prev;
+  float wf[3];    // rhogw at faces k-2..k (face k = below level k)
+#pragma unroll
+  for (int tt = 0; tt < TG; ++tt) {
+    qv[tt][0] = qv[tt][1] = qv[tt][2] = 0.0f;
+    qmn_km1[tt] = qmx_km1[tt] = qh_last[tt] = 0.0f;
+    Qh[tt][0] = Qh[tt][1] = Qh[tt][2] = 0.0;
+  }
+  rh[0] = rh[1] = rh[2] = 0.0;
+  ck1w[0] = ck1w[1] = ck1w[2] = ck2w[0] = ck2w[1] = ck2w[2] = 0.0f;
+  wf[0] = wf[1] = wf[2] = 0.0f;
 
-  const float BIGf = FLT_MAX, EPSf = FLT_EPSILON;
-
-  // vertical Qout of level slot `mid` (window index 1 = level L) using q at L-1, L, L+1 (FP32)
+  // vertical Qout of the middle level using q at the level below, itself and above (FP32)
   auto vqout32 = [&](float qm, float qk, float qp, float c1, float c2, float c1p, float &infl, float &Qmin,
                      float &Qmax) {
     infl = 0.5f - copysignf(0.5f, c1);
@@ -311,71 +392,144 @@ __global__ void __launch_bounds__(TX *TY) k_fast_tile(FastInst I) {
     Qmin = ((qk - qnmax) + qnmax * (Cin + Cout) - CQmax) / (Cout + zerosw) * (1.0f - zerosw) + qk * zerosw;
     Qmax = ((qk - qnmin) + qnmin * (Cin + Cout) - CQmin) / (Cout + zerosw) * (1.0f - zerosw) + qk * zerosw;
   };
-
-  // write one finished level of one tracer
   auto store = [&](int tt, int L, double val) {
     if (!active) return;
     I.Q_out[(size_t)(t0 + tt) * tstride + (size_t)l * lk + (size_t)L * slab + ccell] = val;
   };
 
   for (int k = 1; k <= K - 2; ++k) {
-    // ---- (1) shared fields of this level in the tile window
     const size_t base = (size_t)l * lk + (size_t)k * slab;
-    for (int e = tid; e < N; e += NT) {
-      const int i = i0 - 3 + e % W, j = j0 - 3 + e / W;
-      if (inreg(i, j)) {
+    // ---- (0a) fields of this level in the window
+    for (int e = tid; e < NW; e += NT) {
+      const int i = i0 - 3 + e % WW, j = j0 - 3 + e / WW;
+      if (i >= 1 && i <= G && j >= 1 && j <= G) {
         const size_t o = base + (size_t)(j - 1) * G + (i - 1);
-        s.rho[e] = I.rho_in[o];
+        const double r = I.rho_in[o];
+        s.rinv[e] = 1.0 / r;
+        s.rho[e] = (float)r;
         s.v[0][e] = I.vx[o];
         s.v[1][e] = I.vy[o];
         s.v[2][e] = I.vz[o];
       } else {
-        s.rho[e] = 1.0;
+        s.rinv[e] = 1.0;
+        s.rho[e] = 1.0f;
         s.v[0][e] = s.v[1][e] = s.v[2][e] = 0.0f;
       }
     }
     __syncthreads();
-    // ---- (2) faces of owners in [-2, T]^2 (local 1..T+3): FP64 flux, FP32 centroid, upwind mask
-    {
-      auto acc = [&](int var, int i, int j) -> double {
-        const int e = LI(i, j);
-        return var == 0 ? s.rho[e] : (double)s.v[var - 1][e];
-      };
-      for (int e = tid; e < N; e += NT) {
-        const int lx = e % W, ly = e / W;
-        const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-        const bool own = lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3 && i >= 1 && j >= 1 && i < G && j < G;
-        for (int a = 1; a <= 3; ++a) {
-          double fl = 0.0, xc[3] = {0, 0, 0};
-          if (own && face_exists(I, i, j, a)) fl = face_geo(I, l, i, j, a, sgp, acc, xc);
-          s.flux[a - 1][e] = fl;
-          s.xc[0][a - 1][e] = (float)xc[0];
-          s.xc[1][a - 1][e] = (float)xc[1];
-          s.xc[2][a - 1][e] = (float)xc[2];
-          double cmv = 1.0;
-          if (own && inreg(i, j)) {
-            const double chv = (fl * rarea(I, l, i, j) * dt) / s.rho[e];
-            cmv = 0.5 - fsg(0.5, chv - DBL_EPSILON);
-          }
-          s.cm[a - 1][e] = (float)cmv;
+    // ---- (0b) triangle values TI, TJ (dyn_horiz_adv_flux/src/mod_src_tracer.f90:141-201), FP32
+    for (int e = tid; e < NW; e += NT) {
+      const int i = i0 - 3 + e % WW, j = j0 - 3 + e / WW;
+      const bool ok = i >= 1 && j >= 1 && i + 1 <= G && j + 1 <= G;
+      float ti[4] = {0, 0, 0, 0}, tj[4] = {0, 0, 0, 0};
+      if (ok && e % WW + 1 < WW && e / WW + 1 < Gm::WH) {
+        const float a1 = (float)gt(I, l, i, j, TI, W1), a2 = (float)gt(I, l, i, j, TI, W2),
+                    a3 = (float)gt(I, l, i, j, TI, W3);
+        const float b1 = (float)gt(I, l, i, j, TJ, W1), b2 = (float)gt(I, l, i, j, TJ, W2),
+                    b3 = (float)gt(I, l, i, j, TJ, W3);
+        const int e1 = e + 1, e2 = e + WW + 1, e3 = e + WW;
+        ti[0] = s.rho[e] * a1 + s.rho[e1] * a2 + s.rho[e2] * a3;
+        tj[0] = s.rho[e] * b1 + s.rho[e2] * b2 + s.rho[e3] * b3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ti[c + 1] = s.v[c][e] * a1 + s.v[c][e1] * a2 + s.v[c][e2] * a3;
+          tj[c + 1] = s.v[c][e] * b1 + s.v[c][e2] * b2 + s.v[c][e3] * b3;
         }
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s.u.f.tri[0][c][e] = ti[c], s.u.f.tri[1][c][e] = tj[c];
+    }
+    __syncthreads();
+    // ---- (0c) face fluxes and centroid displacements of owners x, y in [-2, T]
+    for (int e = tid; e < NW; e += NT) {
+      const int lx = e % WW, ly = e / WW;  // local slot: x = lx - 3
+      const int i = i0 - 3 + lx, j = j0 - 3 + ly;
+      const bool own = lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3 && i >= 1 && j >= 1 && i < G && j < G;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        double F = 0.0;
+        float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
+        if (own && face_exists(I, i, j, a + 1)) {
+          const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
+          if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64, as the neighbouring region
+            double xc[3];
+            const GFields gf{&I, l, k};
+            F = face_geo(I, l, i, j, a + 1, sgp, gf, xc);
+          } else {
+            const int ep = (a == 0) ? e - WW : e, eq = (a == 2) ? e - 1 : e;  // TJ slot, TI slot
+            const int sp = (a == 0) ? 1 : (a == 1 ? 0 : 1), sq = (a == 0) ? 0 : (a == 1 ? 1 : 0);
+            const float pr = s.u.f.tri[sp][0][ep], qr = s.u.f.tri[sq][0][eq];
+            const float vx = s.u.f.tri[sp][1][ep] + s.u.f.tri[sq][1][eq];
+            const float vy = s.u.f.tri[sp][2][ep] + s.u.f.tri[sq][2][eq];
+            const float vz = s.u.f.tri[sp][3][ep] + s.u.f.tri[sq][3][eq];
+            const float rr = 1.0f / mx32(pr + qr, FLT_EPSILON);
+            const float Ff = 0.5f * (vx * (float)ga(I, l, i, j, a + 1, HNX) + vy * (float)ga(I, l, i, j, a + 1, HNY) +
+                                     vz * (float)ga(I, l, i, j, a + 1, HNZ));
+            F = (double)Ff;
+            d0 = -(vx * rr * dtf * 0.5f);
+            d1 = -(vy * rr * dtf * 0.5f);
+            d2 = -(vz * rr * dtf * 0.5f);
+          }
+        }
+        s.F[a][e] = F;
+        s.u.f.disp[a][0][e] = d0;
+        s.u.f.disp[a][1][e] = d1;
+        s.u.f.disp[a][2][e] = d2;
       }
     }
     __syncthreads();
-    // ---- per-thread fluxes of its cell (FP64) and the density after the horizontal sub-step
-    double flx[7];
+    // ---- (0d) per ring cell: Courant numbers, masks, outflow sums; per owner: upwind
+    // offsets; per tile cell: flx_h (FP64) and rho after the horizontal sub-step
+    float chm[7], omc = 0.0f, rden = 0.0f, zsw = 1.0f;
+    unsigned inmask = 0, cmown = 0;
+    float dup[3][3];
+    const int nbe[7] = {0, ec, ec, ec, ec - 1, ec - WW - 1, ec - WW};  // owner slot of face m
+    if (fp32_cell) {
+      const float rc = s.rho[ec];
+      float ch[7];
+#pragma unroll
+      for (int m = 1; m <= 6; ++m) {
+        const float Fm = (float)s.F[(m - 1) % 3][nbe[m]];
+        ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) / rc;
+        chm[m] = mn32(ch[m], 0.0f);
+        float chown = ch[m];
+        if (m >= 4) {  // the owner's own Courant number of this face
+          const int oi = (m == 6) ? ci : ci - 1, oj = (m == 4) ? cj : cj - 1;
+          chown = (Fm * (float)rarea(I, l, oi, oj) * dtf) / s.rho[nbe[m]];
+        }
+        const float cm = 0.5f - copysignf(0.5f, chown - EPSf);
+        const bool in = (m <= 3) ? (cm != 0.0f) : (cm == 0.0f);
+        inmask |= in ? (1u << m) : 0u;
+      }
+      const float Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
+      const float Cout =
+          ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
+      zsw = 0.5f - copysignf(0.5f, fabsf(Cout) - EPSf);
+      omc = 1.0f - Cin - Cout;
+      rden = (1.0f - zsw) / (Cout + zsw);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      dup[a][0] = dup[a][1] = dup[a][2] = 0.0f;
+      if (owner && c_int) {
+        const float Fa = (float)s.F[a][ec];
+        const float chown = (Fa * ra32 * dtf) / s.rho[ec];
+        const bool cm = (0.5f - copysignf(0.5f, chown - EPSf)) != 0.0f;
+        cmown |= cm ? (1u << a) : 0u;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dup[a][c] = s.off[a * 6 + (cm ? 3 : 0) + c][tid] + s.u.f.disp[a][c][ec];
+      }
+    }
     double rho_h = 0.0;
     if (active) {
-      const int e = LI(ci, cj);
-      flx[1] = cell_flx(I, l, ci, cj, 1, sgp, s.flux[0][e], ra_c);
-      flx[2] = cell_flx(I, l, ci, cj, 2, sgp, s.flux[1][e], ra_c);
-      flx[3] = cell_flx(I, l, ci, cj, 3, sgp, s.flux[2][e], ra_c);
-      flx[4] = cell_flx(I, l, ci, cj, 4, sgp, s.flux[0][e - 1], ra_c);
-      flx[5] = cell_flx(I, l, ci, cj, 5, sgp, s.flux[1][e - W - 1], ra_c);
-      flx[6] = cell_flx(I, l, ci, cj, 6, sgp, s.flux[2][e - W], ra_c);
-      double sum = flx[1];
-      for (int m = 2; m <= 6; ++m) sum = sum + flx[m];
-      rho_h = s.rho[e] - sum;
+      double sum = 0.0;
+#pragma unroll
+      for (int m = 1; m <= 6; ++m) {
+        const double fl = cell_flx(I, l, ci, cj, m, sgp, s.F[(m - 1) % 3][nbe[m]], ra64);
+        s.flx[m - 1][tid] = fl;
+        sum = (m == 1) ? fl : sum + fl;
+      }
+      rho_h = I.rho_in[base + ccell] - sum;
     }
     // vertical window of shared quantities (slot 2 = level k)
     rh[0] = rh[1];
@@ -389,140 +543,139 @@ __global__ void __launch_bounds__(TX *TY) k_fast_tile(FastInst I) {
     ck1w[1] = ck1w[2];
     ck2w[0] = ck2w[1];
     ck2w[1] = ck2w[2];
-    ck1w[2] = (float)(-(double)wf[2] * dt * I.rdgz[k] / rho_h);
-    ck2w[2] = (float)((double)wtop * dt * I.rdgz[k] / rho_h);
+    ck1w[2] = active ? (float)(-(double)wf[2] * dt * I.rdgz[k] / rho_h) : 0.0f;
+    ck2w[2] = active ? (float)((double)wtop * dt * I.rdgz[k] / rho_h) : 0.0f;
 
+    // ---- (A) q of the group's tracers in the window x, y in [-2, T+1]
+    for (int idx = tid; idx < TG * NW; idx += NT) {
+      const int tt = idx / NW, e = idx % NW;
+      const int lx = e % WW, ly = e / WW;
+      const int i = i0 - 3 + lx, j = j0 - 3 + ly;
+      float qv0 = 0.0f;
+      if (tt < ntg && lx >= 1 && ly >= 1 && i >= 1 && i <= G && j >= 1 && j <= G)
+        qv0 = (float)(I.Q_in[(size_t)(t0 + tt) * tstride + base + (size_t)(j - 1) * G + (i - 1)] * s.rinv[e]);
+      s.q[tt][e] = qv0;
+    }
+    __syncthreads();
+    // ---- (B) gradient and Qout of the ring cells
+    if (in_arr) {
+      if (bs >= 0) {  // region-boundary cell or halo cell: the FP64 boundary values
 #pragma unroll
-    for (int tt = 0; tt < TG; ++tt) {
-      if (tt >= ntg) break;
-      const int t = t0 + tt;
-      const double *Qt = I.Q_in + (size_t)t * tstride + base;
-      // ---- (a) q in the window (FP32)
-      for (int e = tid; e < N; e += NT) {
-        const int i = i0 - 3 + e % W, j = j0 - 3 + e / W;
-        s.q[e] = inreg(i, j) ? (float)(Qt[(size_t)(j - 1) * G + (i - 1)] / s.rho[e]) : 0.0f;
+        for (int tt = 0; tt < TG; ++tt) {
+          if (tt >= ntg) break;
+          const double *bv = bval(I, t0 + tt, k, bs);
+#pragma unroll
+          for (int c = 0; c < 5; ++c) s.u.t.gq[tt][c][tid] = (float)bv[c];
+        }
+      } else if (!fp32_cell) {  // halo point no list reaches: grad 0, Qout = q
+#pragma unroll
+        for (int tt = 0; tt < TG; ++tt) {
+          s.u.t.gq[tt][0][tid] = s.u.t.gq[tt][1][tid] = s.u.t.gq[tt][2][tid] = 0.0f;
+          s.u.t.gq[tt][3][tid] = s.u.t.gq[tt][4][tid] = s.q[tt][ec];
+        }
+      } else {
+        float g[TG][3];
+#pragma unroll
+        for (int tt = 0; tt < TG; ++tt) g[tt][0] = g[tt][1] = g[tt][2] = 0.0f;
+        const int st7[7] = {ec, ec + 1, ec + WW + 1, ec + WW, ec - 1, ec - WW - 1, ec - WW};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+          for (int n = 0; n < 7; ++n) {
+            const float cf = s.cg[c * 7 + n][tid];
+#pragma unroll
+            for (int tt = 0; tt < TG; ++tt)
+              g[tt][c] = (n == 0) ? cf * s.q[tt][st7[0]] : g[tt][c] + cf * s.q[tt][st7[n]];
+          }
+        }
+#pragma unroll
+        for (int tt = 0; tt < TG; ++tt) {
+          const float c0 = s.q[tt][st7[0]], n1 = s.q[tt][st7[1]], n2 = s.q[tt][st7[2]], n3 = s.q[tt][st7[3]],
+                      n4 = s.q[tt][st7[4]], n5 = s.q[tt][st7[5]], n6 = s.q[tt][st7[6]];
+          // 4-point bounds of the 6 faces (owner q first, as mod_src_tracer.f90:152-214)
+          float lo[7], hi[7];
+          lo[1] = mn32(mn32(mn32(c0, n6), n1), n2), hi[1] = mx32(mx32(mx32(c0, n6), n1), n2);
+          lo[2] = mn32(mn32(mn32(c0, n1), n2), n3), hi[2] = mx32(mx32(mx32(c0, n1), n2), n3);
+          lo[3] = mn32(mn32(mn32(c0, n2), n3), n4), hi[3] = mx32(mx32(mx32(c0, n2), n3), n4);
+          lo[4] = mn32(mn32(mn32(n4, n5), c0), n3), hi[4] = mx32(mx32(mx32(n4, n5), c0), n3);
+          lo[5] = mn32(mn32(mn32(n5, n6), c0), n4), hi[5] = mx32(mx32(mx32(n5, n6), c0), n4);
+          lo[6] = mn32(mn32(mn32(n6, n1), c0), n5), hi[6] = mx32(mx32(mx32(n6, n1), c0), n5);
+          float qnmin = c0, qnmax = c0, CQmin = 0.0f, CQmax = 0.0f;
+#pragma unroll
+          for (int m = 1; m <= 6; ++m) {
+            const bool in = (inmask >> m) & 1u;
+            const float qmn = in ? lo[m] : BIGf, qmx = in ? hi[m] : -BIGf;
+            qnmin = mn32(qnmin, qmn);
+            qnmax = mx32(qnmax, qmx);
+            CQmin = (m == 1) ? chm[1] * qmn : CQmin + chm[m] * qmn;
+            CQmax = (m == 1) ? chm[1] * qmx : CQmax + chm[m] * qmx;
+          }
+          s.u.t.gq[tt][0][tid] = g[tt][0];
+          s.u.t.gq[tt][1][tid] = g[tt][1];
+          s.u.t.gq[tt][2][tid] = g[tt][2];
+          s.u.t.gq[tt][3][tid] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
+          s.u.t.gq[tt][4][tid] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
+        }
       }
-      __syncthreads();
-      // ---- (b) gradient and Qout of cells in [-1, T]^2
-      for (int e = tid; e < N; e += NT) {
-        const int lx = e % W, ly = e / W;
-        if (lx < 2 || ly < 2 || lx > TX + 3 || ly > TY + 3) continue;
-        const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-        if (!inreg(i, j)) continue;
-        const int bs = I.bsrc[(size_t)l * I.gall + (j - 1) * G + (i - 1)];
-        if (bs >= 0) {
-          const double *bv = bval(I, t, k, bs);
-          for (int x = 0; x < 5; ++x) s.gq[x][e] = (float)bv[x];
+    }
+    __syncthreads();
+    // ---- (C) limited values of the faces owned by ring cells x, y in [-1, T-1]
+    if (owner) {
+      const int nbt[3] = {tid + 1, tid + RW + 1, tid + RW};  // ring thread of the neighbour
+      const int nbs[3] = {ec + 1, ec + WW + 1, ec + WW};       // window slot of the neighbour
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int ni = (a < 2) ? ci + 1 : ci, nj = (a > 0) ? cj + 1 : cj;
+        // needed by a tile cell (the owner or the neighbour)?
+        const bool need = (x >= 0 && y >= 0) || (ni - i0 >= 0 && nj - j0 >= 0 && ni - i0 < TX && nj - j0 < TY);
+        if (!need || !face_exists(I, ci, cj, a + 1)) {
+#pragma unroll
+          for (int tt = 0; tt < TG; ++tt) s.u.t.qa[tt][a][tid] = 0.0f;
           continue;
         }
-        if (bs == -2) {
-          s.gq[0][e] = s.gq[1][e] = s.gq[2][e] = 0.0f;
-          s.gq[3][e] = s.gq[4][e] = s.q[e];
+        if (!c_int || !interior(ni, nj)) {  // seam face, FP64
+          double xc[3];
+          const GFields gf{&I, l, k};
+          const double fl = face_geo(I, l, ci, cj, a + 1, sgp, gf, xc);
+#pragma unroll
+          for (int tt = 0; tt < TG; ++tt) {
+            if (tt >= ntg) break;
+            s.u.t.qa[tt][a][tid] = (float)seam_face(I, l, k, t0 + tt, ci, cj, a + 1, fl, xc);
+          }
           continue;
         }
-        // interior cell one or more cells away from the region edge: FP32
-        const int c = (j - 1) * G + (i - 1);
-        const int nbe[7] = {e, e + 1, e + W + 1, e + W, e - 1, e - W - 1, e - W};
-        for (int x = 0; x < 3; ++x) {
-          const float *cx = I.cg32 + ((size_t)l * 3 + x) * 7 * I.gall + c;
-          float g = __ldg(cx) * s.q[nbe[0]];
-          for (int n = 1; n <= 6; ++n) g = g + __ldg(cx + (size_t)n * I.gall) * s.q[nbe[n]];
-          s.gq[x][e] = g;
-        }
-        const float q0 = s.q[e];
-        const float rhoc = (float)s.rho[e];
-        const float rac = (float)rarea(I, l, i, j);
-        // the 6 faces: owner slot and face type
-        const int oe[7] = {0, e, e, e, e - 1, e - W - 1, e - W};
-        const int fa[7] = {0, 0, 1, 2, 0, 1, 2};
-        float qmn[7], qmx[7], ch[7], chm[7];
+        const bool cmu = (cmown >> a) & 1u;  // 1: the neighbour is upwind
+        const int ut = cmu ? nbt[a] : tid, us = cmu ? nbs[a] : ec;
 #pragma unroll
-        for (int m = 1; m <= 6; ++m) {
-          const int o = oe[m];
-          const float fl = (float)s.flux[fa[m]][o];
-          const float flxm = (m <= 3 ? fl : -fl) * rac * (float)dt;
-          ch[m] = flxm / rhoc;
-          chm[m] = mn32(ch[m], 0.0f);
-          const float cm = s.cm[fa[m]][o];
-          // 4-point bounds of the face around its owner o
+        for (int tt = 0; tt < TG; ++tt) {
+          float v = s.q[tt][us];
+          v = v + s.u.t.gq[tt][0][ut] * dup[a][0];
+          v = v + s.u.t.gq[tt][1][ut] * dup[a][1];
+          v = v + s.u.t.gq[tt][2][ut] * dup[a][2];
+          const float c0 = s.q[tt][ec];
           float b1, b2, b3;
-          const float qo = s.q[o];
-          if (fa[m] == 0) b1 = s.q[o - W], b2 = s.q[o + 1], b3 = s.q[o + W + 1];
-          else if (fa[m] == 1) b1 = s.q[o + 1], b2 = s.q[o + W + 1], b3 = s.q[o + W];
-          else b1 = s.q[o + W + 1], b2 = s.q[o + W], b3 = s.q[o - 1];
-          const float lo = mn32(mn32(mn32(qo, b1), b2), b3), hi = mx32(mx32(mx32(qo, b1), b2), b3);
-          if (m <= 3) qmn[m] = cm * lo + (1.0f - cm) * BIGf, qmx[m] = cm * hi + (1.0f - cm) * (-BIGf);
-          else qmn[m] = cm * BIGf + (1.0f - cm) * lo, qmx[m] = cm * (-BIGf) + (1.0f - cm) * hi;
-        }
-        float qnmin = q0, qnmax = q0;
-#pragma unroll
-        for (int m = 1; m <= 6; ++m) qnmin = mn32(qnmin, qmn[m]), qnmax = mx32(qnmax, qmx[m]);
-        const float Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
-        const float Cout =
-            ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
-        const float CQmin = chm[1] * qmn[1] + chm[2] * qmn[2] + chm[3] * qmn[3] + chm[4] * qmn[4] +
-                            chm[5] * qmn[5] + chm[6] * qmn[6];
-        const float CQmax = chm[1] * qmx[1] + chm[2] * qmx[2] + chm[3] * qmx[3] + chm[4] * qmx[4] +
-                            chm[5] * qmx[5] + chm[6] * qmx[6];
-        const float zerosw = 0.5f - copysignf(0.5f, fabsf(Cout) - EPSf);
-        s.gq[3][e] = (q0 - CQmax - qnmax * (1.0f - Cin - Cout)) / (Cout + zerosw) * (1.0f - zerosw) + q0 * zerosw;
-        s.gq[4][e] = (q0 - CQmin - qnmin * (1.0f - Cin - Cout)) / (Cout + zerosw) * (1.0f - zerosw) + q0 * zerosw;
-      }
-      __syncthreads();
-      // ---- (c) limited face values of owners in [-1, T-1]^2
-      for (int e = tid; e < N; e += NT) {
-        const int lx = e % W, ly = e / W;
-        if (lx < 2 || ly < 2 || lx > TX + 2 || ly > TY + 2) continue;
-        const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-        if (!inreg(i, j)) continue;
-        const int nbe[3] = {e + 1, e + W + 1, e + W};
-        const int nbi[3] = {i + 1, i + 1, i}, nbj[3] = {j, j + 1, j + 1};
-        const bool own_in = interior(i, j);
-        for (int a = 0; a < 3; ++a) {
-          if (!face_exists(I, i, j, a + 1)) {
-            s.qa[a][e] = 0.0;
-            continue;
-          }
-          const int n = nbe[a];
-          if (!own_in || !interior(nbi[a], nbj[a])) {  // seam face: FP64 from global memory
-            double xc[3];
-            const GFields f{&I, l, k};
-            const double fl = face_geo(I, l, i, j, a + 1, sgp, f, xc);
-            s.qa[a][e] = seam_face(I, l, k, t, i, j, a + 1, fl, xc);
-            continue;
-          }
-          const float cm = s.cm[a][e];
-          float vu = s.q[n], vs = s.q[e];
-          for (int x = 0; x < 3; ++x) {
-            const float xcv = s.xc[x][a][e];
-            vu = vu + s.gq[x][n] * (xcv - (float)gx(I, l, nbi[a], nbj[a], x));
-          }
-          for (int x = 0; x < 3; ++x) {
-            const float xcv = s.xc[x][a][e];
-            vs = vs + s.gq[x][e] * (xcv - (float)gx(I, l, i, j, x));
-          }
-          float v = cm * vu + (1.0f - cm) * vs;
-          float b1, b2, b3;
-          const float qo = s.q[e];
-          if (a == 0) b1 = s.q[e - W], b2 = s.q[e + 1], b3 = s.q[e + W + 1];
-          else if (a == 1) b1 = s.q[e + 1], b2 = s.q[e + W + 1], b3 = s.q[e + W];
-          else b1 = s.q[e + W + 1], b2 = s.q[e + W], b3 = s.q[e - 1];
-          const float lo = mn32(mn32(mn32(qo, b1), b2), b3), hi = mx32(mx32(mx32(qo, b1), b2), b3);
-          const float own_min = cm * lo + (1.0f - cm) * BIGf, own_max = cm * hi + (1.0f - cm) * (-BIGf);
-          const float nb_min = cm * BIGf + (1.0f - cm) * lo, nb_max = cm * (-BIGf) + (1.0f - cm) * hi;
-          v = cm * mn32(mx32(v, own_min), own_max) + (1.0f - cm) * mn32(mx32(v, nb_min), nb_max);
-          v = cm * mx32(mn32(v, s.gq[4][n]), s.gq[3][n]) + (1.0f - cm) * mx32(mn32(v, s.gq[4][e]), s.gq[3][e]);
-          s.qa[a][e] = (double)v;
+          if (a == 0) b1 = s.q[tt][ec - WW], b2 = s.q[tt][ec + 1], b3 = s.q[tt][ec + WW + 1];
+          else if (a == 1) b1 = s.q[tt][ec + 1], b2 = s.q[tt][ec + WW + 1], b3 = s.q[tt][ec + WW];
+          else b1 = s.q[tt][ec + WW + 1], b2 = s.q[tt][ec + WW], b3 = s.q[tt][ec - 1];
+          const float lo = mn32(mn32(mn32(c0, b1), b2), b3), hi = mx32(mx32(mx32(c0, b1), b2), b3);
+          v = mn32(mx32(v, lo), hi);
+          v = mx32(mn32(v, s.u.t.gq[tt][4][ut]), s.u.t.gq[tt][3][ut]);
+          s.u.t.qa[tt][a][tid] = v;
         }
       }
-      __syncthreads();
-      // ---- (d) horizontal update of this thread's cell (FP64) and (e) the vertical stream
-      if (active) {
-        const int e = LI(ci, cj);
-        const double qa[7] = {0, s.qa[0][e], s.qa[1][e], s.qa[2][e], s.qa[0][e - 1], s.qa[1][e - W - 1],
-                              s.qa[2][e - W]};
-        double sum = flx[1] * qa[1];
-        for (int m = 2; m <= 6; ++m) sum = sum + flx[m] * qa[m];
+    }
+    __syncthreads();
+    // ---- (D) horizontal update of the tile cells (FP64) and the vertical stream
+    if (active) {
+#pragma unroll
+      for (int tt = 0; tt < TG; ++tt) {
+        if (tt >= ntg) break;
+        const double *Qt = I.Q_in + (size_t)(t0 + tt) * tstride + base;
+        const float qa[7] = {0.0f, s.u.t.qa[tt][0][tid], s.u.t.qa[tt][1][tid], s.u.t.qa[tt][2][tid],
+                             s.u.t.qa[tt][0][tid - 1], s.u.t.qa[tt][1][tid - RW - 1], s.u.t.qa[tt][2][tid - RW]};
+        double sum = s.flx[0][tid] * (double)qa[1];
+#pragma unroll
+        for (int m = 2; m <= 6; ++m) sum = sum + s.flx[m - 1][tid] * (double)qa[m];
         const double Qhk = Qt[ccell] - sum;
         Qh[tt][0] = Qh[tt][1];
         Qh[tt][1] = Qh[tt][2];
@@ -557,21 +710,18 @@ __global__ void __launch_bounds__(TX *TY) k_fast_tile(FastInst I) {
           qmx_km1[tt] = Qmax;
         }
       }
-      __syncthreads();
-    }
-    // density: level k-2 final (one group writes it)
-    if (active && grp == 0 && k >= 3) {
-      const int L = k - 2;
-      const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dt * I.rdgz[L];
-      I.rho_out[(size_t)l * lk + (size_t)L * slab + ccell] = rn;
-      if (L == 1) I.rho_out[(size_t)l * lk + ccell] = rn;
+      // density: level k-2 final (one group writes it)
+      if (grp == 0 && k >= 3) {
+        const int L = k - 2;
+        const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dt * I.rdgz[L];
+        I.rho_out[(size_t)l * lk + (size_t)L * slab + ccell] = rn;
+        if (L == 1) I.rho_out[(size_t)l * lk + ccell] = rn;
+      }
     }
   }
   // ---- drain: levels K-3 and K-2 (faces K-2 and K-1)
   if (active) {
     const int kk = K - 1;  // ghost level above: q(kmax+1) = q(kmax)
-    const float wtop = 0.0f;
-    (void)wtop;
 #pragma unroll
     for (int tt = 0; tt < TG; ++tt) {
       if (tt >= ntg) break;
@@ -590,7 +740,7 @@ __global__ void __launch_bounds__(TX *TY) k_fast_tile(FastInst I) {
         store(tt, L, Qn);
         if (L == 1) store(tt, 0, Qn);
       }
-      // top face K-1: unlimited, rhogw = 0 there
+      // top face K-1: unlimited
       const float qtop = (float)I.afact[kk] * qv[tt][2] + (float)I.bfact[kk] * qv[tt][2];
       const float wk1 = I.w[(size_t)l * lk + (size_t)kk * slab + ccell];
       const double fu = (double)wk1 * (double)qtop, fl = (double)wf[2] * (double)qh;
@@ -662,7 +812,7 @@ __global__ void k_fast_pole(FastInst I) {
     Qh[k] = I.Q_in_pl[toff + off] - sum;
     rh[k] = I.rho_in_pl[off] - rsum;
   }
-  // vertical sub-step of the pole column (FP64, as the plain path)
+  // vertical sub-step of the pole column (FP64, region form, as the plain path)
   const int kmin = 1, kmax = K - 2;
   double ck1[KMAX], ck2[KMAX], q[KMAX], qh[KMAX];
   auto W = [&](int k) { return (double)I.w_pl[((size_t)p * K + k) * kGallPl]; };
@@ -685,7 +835,7 @@ __global__ void k_fast_pole(FastInst I) {
     const double maxL = mx64(qk, qm) - (1.0 - infl) * BIG, maxU = mx64(qk, qp) - (1.0 - infu) * BIG;
     const double qnmin = mn64(mn64(minL, minU), qk), qnmax = mx64(mx64(maxL, maxU), qk);
     const double Cin = infl * ck1[k] + infu * ck2[k], Cout = (1.0 - infl) * ck1[k] + (1.0 - infu) * ck2[k];
-    const double CQmax = infl * ck1[k] * maxL + infu * ck2[k] * maxU;  // region form, as the composed step
+    const double CQmax = infl * ck1[k] * maxL + infu * ck2[k] * maxU;
     const double CQmin = infl * ck1[k] * minL + infu * ck2[k] * minU;
     const double zerosw = 0.5 - fsg(0.5, fabs(Cout) - EPS);
     Qmin = ((qk - qnmax) + qnmax * (Cin + Cout) - CQmax) / (Cout + zerosw) * (1.0 - zerosw) + qk * zerosw;
@@ -729,18 +879,18 @@ __global__ void k_fast_carry(FastInst I) {
 // ---------------------------------------------------------------------------------------
 template <int TX, int TY, int TG>
 static cudaError_t launch_tile(const FastInst &I, cudaStream_t st) {
-  const size_t smem = sizeof(TileSmem<TX, TY>);
+  const size_t smem = sizeof(TileSmem<TX, TY, TG>);
   cudaError_t e = cudaFuncSetAttribute(k_fast_tile<TX, TY, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
   const int ngroups = (I.ntr + TG - 1) / TG;
   const long long blocks = (long long)I.lall * I.ntx * I.nty * ngroups;
-  k_fast_tile<TX, TY, TG><<<(unsigned)blocks, TX * TY, smem, st>>>(I);
+  k_fast_tile<TX, TY, TG><<<(unsigned)blocks, TileGeo<TX, TY>::NT, smem, st>>>(I);
   return cudaGetLastError();
 }
 
 int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax) {
-  static const int shapes[][3] = {{16, 16, 4}, {16, 16, 2}, {16, 8, 4}, {32, 8, 4}, {16, 16, 8}, {8, 8, 4}};
+  static const int shapes[][3] = {{14, 14, 4}, {30, 6, 4}, {14, 14, 2}, {14, 14, 8}, {6, 30, 4}};
   const int n = sizeof(shapes) / sizeof(shapes[0]);
   if (tx)
     for (int i = 0; i < n; ++i) tx[i] = shapes[i][0], ty[i] = shapes[i][1], tg[i] = shapes[i][2];
@@ -748,22 +898,27 @@ int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax) {
   return n;
 }
 
+cudaError_t fast_build_offsets(const FastInst &I, float *off, cudaStream_t st) {
+  const long long n = (long long)I.lall * I.gall;
+  k_fast_offsets<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(I, off);
+  return cudaGetLastError();
+}
+
 cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
                       long long &launches) {
-  const long long nbt = (long long)I.nb * (I.K - 2) * I.ntr;
-  k_fast_boundary<<<(unsigned)((nbt + 127) / 128), 128, 0, st>>>(I);
+  const long long nbk = (long long)I.nb * (I.K - 2);
+  k_fast_boundary<<<(unsigned)((nbk + 127) / 128), 128, 0, st>>>(I);
   if (I.K <= 48) k_fast_pole<48><<<1, 64, 0, st>>>(I);
   else if (I.K <= 128) k_fast_pole<128><<<1, 64, 0, st>>>(I);
   else return cudaErrorInvalidValue;
   if (ev0) cudaEventRecord(ev0, st);
   cudaError_t e;
   switch (shape) {
-    case 0: e = launch_tile<16, 16, 4>(I, st); break;
-    case 1: e = launch_tile<16, 16, 2>(I, st); break;
-    case 2: e = launch_tile<16, 8, 4>(I, st); break;
-    case 3: e = launch_tile<32, 8, 4>(I, st); break;
-    case 4: e = launch_tile<16, 16, 8>(I, st); break;
-    case 5: e = launch_tile<8, 8, 4>(I, st); break;
+    case 0: e = launch_tile<14, 14, 4>(I, st); break;
+    case 1: e = launch_tile<30, 6, 4>(I, st); break;
+    case 2: e = launch_tile<14, 14, 2>(I, st); break;
+    case 3: e = launch_tile<14, 14, 8>(I, st); break;
+    case 4: e = launch_tile<6, 30, 4>(I, st); break;
     default: return cudaErrorInvalidValue;
   }
   if (ev1) cudaEventRecord(ev1, st);

@@ -9,6 +9,9 @@ namespace icoadv {
 
 // Tile shapes available to the autotuner: fills tx/ty/tg (arrays of the returned length) when non-NULL.
 int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax);
+// Per-face remap offsets (GRD_xr - GRD_x of the owner and of the neighbour, FP32) into
+// off (lall, 18, gall); needs I's geometry pointers only.
+cudaError_t fast_build_offsets(const FastInst &I, float *off, cudaStream_t st);
 // One fused step of instance I on stream st with tile shape `shape`; ev0/ev1 (optional)
 // are recorded around the tile kernel, the dominant launch.
 cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
