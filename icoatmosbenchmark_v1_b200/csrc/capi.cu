@@ -172,7 +172,7 @@ Ctx::~Ctx() {
   for (void *p : stepgeo)
     if (p) cudaFree(p);
   for (void *p : {(void *)fast.bsrc, (void *)fast.blist, (void *)fast.ring, (void *)fast.carry, (void *)fast.cg32,
-                  (void *)fast.off32})
+                  (void *)fast.off32, (void *)fast.seam_list, (void *)fast.seam_id})
     if (p) cudaFree(p);
   for (auto &ev : fast.events) cudaEventDestroy(ev.first), cudaEventDestroy(ev.second);
   if (stream) cudaStreamDestroy(stream);
@@ -655,17 +655,38 @@ int Ctx::build_fast_tables() {
   for (int c = 0; c < npt; ++c)
     if (bsrc[c] == -2) carry.push_back(c);
   if (carry.empty()) carry.push_back(-1);  // keeps the device table non-empty; the kernel skips it
+  // seam faces: every face of horizontal_flux's loops (mod_src_tracer.f90:235-309) with a halo cell
+  std::vector<int> seam_list, seam_id((size_t)L * gall * 3, -1);
+  auto inner = [&](int i, int j) { return i >= g0 && i <= g1 && j >= g0 && j <= g1; };
+  for (int l = 0; l < L; ++l)
+    for (int j = 1; j <= G; ++j)
+      for (int i = 1; i <= G; ++i)
+        for (int a = 0; a < 3; ++a) {
+          const bool ex = (a == 0) ? (j >= g0 && j <= g1 && i >= g0 - 1 && i <= g1)
+                        : (a == 1) ? (i >= g0 - 1 && i <= g1 && j >= g0 - 1 && j <= g1)
+                                   : (i >= g0 && i <= g1 && j >= g0 - 1 && j <= g1);
+          const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
+          if (!ex || (inner(i, j) && inner(ni, nj))) continue;
+          const int code = (l * gall + (j - 1) * G + (i - 1)) * 3 + a;
+          seam_id[code] = (int)seam_list.size();
+          seam_list.push_back(code);
+        }
   fast.nb = (int)blist.size();
   fast.ncarry = (int)carry.size();
+  fast.ns = (int)seam_list.size();
   if (cudaMalloc(&fast.bsrc, bsrc.size() * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&fast.blist, blist.size() * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&fast.ring, ring.size() * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&fast.carry, carry.size() * sizeof(int)) != cudaSuccess)
+      cudaMalloc(&fast.carry, carry.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&fast.seam_list, seam_list.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&fast.seam_id, seam_id.size() * sizeof(int)) != cudaSuccess)
     return set_error("cudaMalloc(fast tables)"), ICA_ERR_NOMEM;
   cudaMemcpy(fast.bsrc, bsrc.data(), bsrc.size() * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(fast.blist, blist.data(), blist.size() * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(fast.ring, ring.data(), ring.size() * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(fast.carry, carry.data(), carry.size() * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(fast.seam_list, seam_list.data(), seam_list.size() * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(fast.seam_id, seam_id.data(), seam_id.size() * sizeof(int), cudaMemcpyHostToDevice);
   fast.built = true;
   return ICA_OK;
 }
@@ -705,6 +726,10 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
   const size_t nbb = (size_t)ntr * sz.kall * fast.nb * 5;
   I.bbuf = (double *)buf("fast_bbuf", nbb * sizeof(double));
   if (!I.bbuf) return set_error("cudaMalloc(fast boundary buffer)"), ICA_ERR_NOMEM;
+  I.seam_list = fast.seam_list, I.seam_id = fast.seam_id, I.ns = fast.ns;
+  I.sflux = (double *)buf("fast_sflux", (size_t)sz.kall * fast.ns * sizeof(double));
+  I.sval = (float *)buf("fast_sval", (size_t)ntr * sz.kall * fast.ns * sizeof(float));
+  if (!I.sflux || !I.sval) return set_error("cudaMalloc(fast seam buffers)"), ICA_ERR_NOMEM;
   return ICA_OK;
 }
 

@@ -28,7 +28,8 @@ struct FastState {  // fused path: boundary tables, tile shape, kernel timing
   bool built = false;
   int nb = 0, shape = 0;
   int *bsrc = nullptr, *blist = nullptr, *ring = nullptr, *carry = nullptr;
-  int ncarry = 0;
+  int *seam_list = nullptr, *seam_id = nullptr;
+  int ncarry = 0, ns = 0;
   float *cg32 = nullptr;
   float *off32 = nullptr;  // per-face remap offsets, rebuilt when the geometry changes
   bool off_ready = false;

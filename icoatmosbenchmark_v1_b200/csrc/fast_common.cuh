@@ -32,6 +32,12 @@ struct FastInst {
   int nb;
   const int *carry;  // (ncarry): region points no halo list writes; they keep their input values
   int ncarry;
+  // faces with a halo cell on one side ("seam" faces), precomputed in FP64 each step
+  const int *seam_list;  // (ns): (l*gall + owner cell)*3 + face (0..2)
+  const int *seam_id;    // (lall, gall, 3): index into seam_list, -1 for faces between interior cells
+  int ns;
+  double *sflux;  // (K, ns): 0.5 (rhov . HN) of the seam faces
+  float *sval;    // (ntr, K, ns): limited face values of the seam faces
   double *bbuf;  // (ntr, K, nb, 5): grad x, y, z, Qout min, Qout max
 };
 

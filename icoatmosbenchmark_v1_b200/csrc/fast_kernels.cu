@@ -8,6 +8,7 @@
 //                    exchanges (grad q and Qout, mod_src_tracer.f90:371) would move
 //                    into other regions' halos, so no exchange is needed.  One
 //                    thread per (cell, level): the face geometry once, then the tracers.
+//   k_fast_seam      FP64 flux and limited value of every seam face (below), all tracers.
 //   k_fast_pole      the two pole centres (horizontal + vertical), FP64.
 //   k_fast_tile      one CTA per (region tile, group of TG tracers), one thread per
 //                    cell of the tile and its 1-wide ring, looping over the levels:
@@ -21,7 +22,7 @@
 //
 // Faces are "seam" faces when one of their two cells is a halo cell; the
 // neighbouring region computes the same face from its own halo copy, so those
-// faces are done in FP64 (seam_face) from the FP64 boundary values.  An interior
+// faces are done in FP64 (seam_face, in k_fast_seam) from the FP64 boundary values.  An interior
 // face is computed by every tile that needs it from the same inputs by the same
 // instructions (cell positions enter only through the per-face offsets
 // GRD_xr - GRD_x, fixed per face), so both of its cells see the same value and
@@ -258,6 +259,23 @@ __device__ double seam_face(const FastInst &I, int l, int k, int t, int i, int j
   return v;
 }
 
+// ---- seam faces: FP64 flux once per (face, level), then the limited value of every tracer
+__global__ void k_fast_seam(FastInst I) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)I.ns * (I.K - 2)) return;
+  const int sidx = (int)(tid % I.ns), k = 1 + (int)(tid / I.ns);
+  const int code = I.seam_list[sidx];
+  const int a = code % 3 + 1, p = code / 3;
+  const int l = p / I.gall, c = p % I.gall;
+  const int i = c % I.G + 1, j = c / I.G + 1;
+  const GFields gf{&I, l, k};
+  double xc[3];
+  const double fl = face_geo(I, l, i, j, a, I.have_sgp[l] != 0, gf, xc);
+  I.sflux[(size_t)k * I.ns + sidx] = fl;
+  for (int t = 0; t < I.ntr; ++t)
+    I.sval[((size_t)t * I.K + k) * I.ns + sidx] = (float)seam_face(I, l, k, t, i, j, a, fl, xc);
+}
+
 // ---- per-face remap offsets GRD_xr - GRD_x of the owner and of the neighbour (FP32),
 // fixed per face, so an interior face value does not depend on the tile that computes it.
 // off32 (lall, 18, gall): [a*6 + x] owner side, [a*6 + 3 + x] neighbour side, a = face 0..2
@@ -275,6 +293,35 @@ __global__ void k_fast_offsets(FastInst I, float *off) {
       off[((size_t)l * 18 + (a - 1) * 6 + 3 + x) * I.gall + c] = nok ? (float)(xr - gx(I, l, ni, nj, x)) : 0.0f;
     }
   }
+}
+
+// ---- vertical Thuburn limiter (dyn_vert_adv_limiter/src/mod_src_tracer.f90:107-186), d = 0, FP32:
+// the tracer-independent part of a level (upwind flags, Courant sums) and the per-tracer bounds
+struct VLim {
+  float infl, a1, a2, bl, bu, icm, rden, zsw;
+};
+__device__ __forceinline__ VLim vlim_params(float c1, float c2, float c1p) {
+  VLim v;
+  v.infl = 0.5f - copysignf(0.5f, c1);
+  const float infu = 0.5f + copysignf(0.5f, c1p);
+  v.bl = (1.0f - v.infl) * FLT_MAX;
+  v.bu = (1.0f - infu) * FLT_MAX;
+  v.a1 = v.infl * c1;
+  v.a2 = infu * c2;
+  const float Cin = v.a1 + v.a2;
+  const float Cout = (1.0f - v.infl) * c1 + (1.0f - infu) * c2;
+  v.icm = Cin + Cout;
+  v.zsw = 0.5f - copysignf(0.5f, fabsf(Cout) - FLT_EPSILON);
+  v.rden = (1.0f - v.zsw) / (Cout + v.zsw);
+  return v;
+}
+__device__ __forceinline__ void vlim_qout(const VLim &v, float qm, float qk, float qp, float &Qmin, float &Qmax) {
+  const float minL = mn32(qk, qm) + v.bl, minU = mn32(qk, qp) + v.bu;
+  const float maxL = mx32(qk, qm) - v.bl, maxU = mx32(qk, qp) - v.bu;
+  const float qnmin = mn32(mn32(minL, minU), qk), qnmax = mx32(mx32(maxL, maxU), qk);
+  const float CQmin = v.a1 * minL + v.a2 * minU, CQmax = v.a1 * maxL + v.a2 * maxU;
+  Qmin = ((qk - qnmax) + qnmax * v.icm - CQmax) * v.rden + qk * v.zsw;
+  Qmax = ((qk - qnmin) + qnmin * v.icm - CQmin) * v.rden + qk * v.zsw;
 }
 
 // ---- the fused tile kernel ----------------------------------------------------------
@@ -373,25 +420,6 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
   ck1w[0] = ck1w[1] = ck1w[2] = ck2w[0] = ck2w[1] = ck2w[2] = 0.0f;
   wf[0] = wf[1] = wf[2] = 0.0f;
 
-  // vertical Qout of the middle level using q at the level below, itself and above (FP32)
-  auto vqout32 = [&](float qm, float qk, float qp, float c1, float c2, float c1p, float &infl, float &Qmin,
-                     float &Qmax) {
-    infl = 0.5f - copysignf(0.5f, c1);
-    const float infu = 0.5f + copysignf(0.5f, c1p);
-    const float minL = mn32(qk, qm) + (1.0f - infl) * BIGf;
-    const float minU = mn32(qk, qp) + (1.0f - infu) * BIGf;
-    const float maxL = mx32(qk, qm) - (1.0f - infl) * BIGf;
-    const float maxU = mx32(qk, qp) - (1.0f - infu) * BIGf;
-    const float qnmin = mn32(mn32(minL, minU), qk);
-    const float qnmax = mx32(mx32(maxL, maxU), qk);
-    const float Cin = infl * c1 + infu * c2;
-    const float Cout = (1.0f - infl) * c1 + (1.0f - infu) * c2;
-    const float CQmin = infl * c1 * minL + infu * c2 * minU;
-    const float CQmax = infl * c1 * maxL + infu * c2 * maxU;
-    const float zerosw = 0.5f - copysignf(0.5f, fabsf(Cout) - EPSf);
-    Qmin = ((qk - qnmax) + qnmax * (Cin + Cout) - CQmax) / (Cout + zerosw) * (1.0f - zerosw) + qk * zerosw;
-    Qmax = ((qk - qnmin) + qnmin * (Cin + Cout) - CQmin) / (Cout + zerosw) * (1.0f - zerosw) + qk * zerosw;
-  };
   auto store = [&](int tt, int L, double val) {
     if (!active) return;
     I.Q_out[(size_t)(t0 + tt) * tstride + (size_t)l * lk + (size_t)L * slab + ccell] = val;
@@ -451,10 +479,9 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
         float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
         if (own && face_exists(I, i, j, a + 1)) {
           const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
-          if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64, as the neighbouring region
-            double xc[3];
-            const GFields gf{&I, l, k};
-            F = face_geo(I, l, i, j, a + 1, sgp, gf, xc);
+          if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64 flux of k_fast_seam
+            const int sid = I.seam_id[((size_t)l * I.gall + (size_t)(j - 1) * G + (i - 1)) * 3 + a];
+            F = I.sflux[(size_t)k * I.ns + sid];
           } else {
             const int ep = (a == 0) ? e - WW : e, eq = (a == 2) ? e - 1 : e;  // TJ slot, TI slot
             const int sp = (a == 0) ? 1 : (a == 1 ? 0 : 1), sq = (a == 0) ? 0 : (a == 1 ? 1 : 0);
@@ -633,14 +660,12 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
           for (int tt = 0; tt < TG; ++tt) s.u.t.qa[tt][a][tid] = 0.0f;
           continue;
         }
-        if (!c_int || !interior(ni, nj)) {  // seam face, FP64
-          double xc[3];
-          const GFields gf{&I, l, k};
-          const double fl = face_geo(I, l, ci, cj, a + 1, sgp, gf, xc);
+        if (!c_int || !interior(ni, nj)) {  // seam face: value of k_fast_seam
+          const int sid = I.seam_id[((size_t)l * I.gall + ccell) * 3 + a];
 #pragma unroll
           for (int tt = 0; tt < TG; ++tt) {
             if (tt >= ntg) break;
-            s.u.t.qa[tt][a][tid] = (float)seam_face(I, l, k, t0 + tt, ci, cj, a + 1, fl, xc);
+            s.u.t.qa[tt][a][tid] = I.sval[((size_t)(t0 + tt) * K + k) * I.ns + sid];
           }
           continue;
         }
@@ -667,6 +692,8 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
     __syncthreads();
     // ---- (D) horizontal update of the tile cells (FP64) and the vertical stream
     if (active) {
+      const double rinvh = 1.0 / rho_h;
+      const VLim vp = vlim_params(ck1w[1], ck2w[1], ck1w[2]);  // level k-1 (used from k = 2)
 #pragma unroll
       for (int tt = 0; tt < TG; ++tt) {
         if (tt >= ntg) break;
@@ -682,15 +709,16 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
         Qh[tt][2] = Qhk;
         qv[tt][0] = qv[tt][1];
         qv[tt][1] = qv[tt][2];
-        qv[tt][2] = (float)(Qhk / rho_h);
+        qv[tt][2] = (float)(Qhk * rinvh);
         if (k == 1) {  // ghost level below: q(kmin-1) = q(kmin)
           qv[tt][1] = qv[tt][2];
           qh_last[tt] = 0.0f;
         }
         if (k >= 2) {
           // Qout of level k-1 (window slot 1) from q at k-2, k-1, k
-          float infl, Qmin, Qmax;
-          vqout32(qv[tt][0], qv[tt][1], qv[tt][2], ck1w[1], ck2w[1], ck1w[2], infl, Qmin, Qmax);
+          float Qmin, Qmax;
+          const float infl = vp.infl;
+          vlim_qout(vp, qv[tt][0], qv[tt][1], qv[tt][2], Qmin, Qmax);
           // face k-1 (between levels k-2 and k-1)
           const int f = k - 1;
           float qh = (float)I.afact[f] * qv[tt][1] + (float)I.bfact[f] * qv[tt][0];
@@ -722,14 +750,15 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
   // ---- drain: levels K-3 and K-2 (faces K-2 and K-1)
   if (active) {
     const int kk = K - 1;  // ghost level above: q(kmax+1) = q(kmax)
+    const float c1top = (float)(-(double)I.w[(size_t)l * lk + (size_t)kk * slab + ccell] * dt * I.rdgz[kk] /
+                                I.rho_in[(size_t)l * lk + (size_t)kk * slab + ccell]);
+    const VLim vd = vlim_params(ck1w[2], ck2w[2], c1top);  // level K-2 with q(K-1) := q(K-2)
 #pragma unroll
     for (int tt = 0; tt < TG; ++tt) {
       if (tt >= ntg) break;
-      // Qout of level K-2 with q(K-1) := q(K-2)
-      float infl, Qmin, Qmax;
-      const float c1top = (float)(-(double)I.w[(size_t)l * lk + (size_t)kk * slab + ccell] * dt * I.rdgz[kk] /
-                                  I.rho_in[(size_t)l * lk + (size_t)kk * slab + ccell]);
-      vqout32(qv[tt][1], qv[tt][2], qv[tt][2], ck1w[2], ck2w[2], c1top, infl, Qmin, Qmax);
+      float Qmin, Qmax;
+      const float infl = vd.infl;
+      vlim_qout(vd, qv[tt][1], qv[tt][2], qv[tt][2], Qmin, Qmax);
       const int f = K - 2;
       float qh = (float)I.afact[f] * qv[tt][2] + (float)I.bfact[f] * qv[tt][1];
       if (f >= 2) qh = infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - infl) * mx32(mn32(qh, Qmax), Qmin);
@@ -908,6 +937,8 @@ cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t
                       long long &launches) {
   const long long nbk = (long long)I.nb * (I.K - 2);
   k_fast_boundary<<<(unsigned)((nbk + 127) / 128), 128, 0, st>>>(I);
+  const long long nsk = (long long)I.ns * (I.K - 2);
+  k_fast_seam<<<(unsigned)((nsk + 127) / 128), 128, 0, st>>>(I);
   if (I.K <= 48) k_fast_pole<48><<<1, 64, 0, st>>>(I);
   else if (I.K <= 128) k_fast_pole<128><<<1, 64, 0, st>>>(I);
   else return cudaErrorInvalidValue;
@@ -924,7 +955,7 @@ cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t
   if (ev1) cudaEventRecord(ev1, st);
   const long long nc = (long long)I.ncarry * I.K;
   k_fast_carry<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(I);
-  launches += 4;
+  launches += 5;
   return e;
 }
 
