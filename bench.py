@@ -200,7 +200,7 @@ def run_ours(args, world, rank, local):
         step = runner.step
         st = runner.state
         dtype = "f32"
-        s_bytes = 32
+        s_bytes = 48
 
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -273,7 +273,7 @@ def measure_e2e(args, ctx, g, st, f, dt, upd, world):
     n = max(1, min(args.steps, args.e2e_steps))
     host = {k: v.cpu().pin_memory() for k, v in st.items()}
     hf = {k: v.cpu().pin_memory() for k, v in f.items()}
-    if args.mode != "plain":  # the fused path takes FP32 fields
+    if args.mode != "plain":  # the batched path takes FP32 fields
         hf = {k: v.to(torch.float32).pin_memory() for k, v in hf.items()}
     hn = {k: v.numpy() for k, v in host.items()}
     hfn = {k: v.numpy() for k, v in hf.items()}
@@ -313,7 +313,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--tile-shape", type=int, default=-1, help="fused tile shape index (default: autotune)")
+    ap.add_argument("--tile-shape", type=int, default=-1, help="tile shape index of the horizontal kernel (default: autotune)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")
     args = ap.parse_args()

@@ -265,9 +265,9 @@ class IcoAdv:
         with self._ordered(bool(kinds[0])):
             _check(name, getattr(lib(), name)(self.h, int(ntr), C.c_double(dt), *ptrs))
 
-    # ---- fused batched path ------------------------------------------------------
+    # ---- batched path (all tracers per launch) -------------------------------------
     def advect_fast_dev(self, dt, state_in, state_out, fields32):
-        """One fused step on device tensors: state dicts (rhog, rhog_pl, rhogq, rhogq_pl) FP64,
+        """One batched step on device tensors: state dicts (rhog, rhog_pl, rhogq, rhogq_pl) FP64,
         fields32 dict (rhogvx..rhogw_pl) FP32; writes state_out."""
         ntr = state_in["rhogq"].shape[0]
         sp = [_ptr(state_in[k], np.float64)[0] for k in STATE_KEYS]
@@ -279,7 +279,7 @@ class IcoAdv:
 
     def advect_fast_host(self, dt, rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz,
                          rhogvz_pl, rhogw, rhogw_pl):
-        """One fused step on host arrays, in place on the FP64 state (FP32 fields)."""
+        """One batched step on host arrays, in place on the FP64 state (FP32 fields)."""
         ntr = rhogq.shape[0]
         sp = [_ptr(a, np.float64)[0] for a in (rhog, rhog_pl, rhogq, rhogq_pl)]
         fp = [_ptr(a, np.float32)[0] for a in (rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz, rhogvz_pl, rhogw,
@@ -313,7 +313,7 @@ FIELD_KEYS = ("rhogvx", "rhogvx_pl", "rhogvy", "rhogvy_pl", "rhogvz", "rhogvz_pl
 
 
 class FastRunner:
-    """Device-resident loop of the fused step: double-buffered FP64 state, FP32 fields, tile
+    """Device-resident loop of the batched step: double-buffered FP64 state, FP32 fields, tile
     shape chosen by timing every available shape on the real inputs (the autotuner)."""
 
     def __init__(self, ctx, grid, state, fields, dt, autotune=True):
@@ -323,7 +323,9 @@ class FastRunner:
         self.b = {k: torch.empty_like(v) for k, v in state.items()}
         self.f32 = {k: fields[k].to(torch.float32).contiguous() for k in FIELD_KEYS}
         self.updates = (10 * 4 ** grid.glevel + 2) * grid.kall * state["rhogq"].shape[0]
-        self.alg_bytes = 16.0 + 32.0 / state["rhogq"].shape[0]
+        # k_fast_horiz per tracer cell-level: rhogq read + write (FP64); per cell-level, shared by
+        # the tracers: rhog read + write (FP64), rhogv x/y/z + rhogw (FP32), vertical inputs (16 B)
+        self.alg_bytes = 16.0 + 48.0 / state["rhogq"].shape[0]
         self.shape = 0
         self.tuning = []
         if autotune:
@@ -363,9 +365,9 @@ class FastRunner:
         self.ctx.fast_timing(1)
 
     def kernel_stats(self):
-        """Average CUDA-event duration of the tile kernel over the steps since start_timing()."""
+        """Average CUDA-event duration of the horizontal kernel over the steps since start_timing()."""
         ms, n = self.ctx.fast_timing(0)
         if n == 0:
             return None
-        return {"name": "k_fast_tile", "ms_per_launch": ms / n, "launches": n,
+        return {"name": "k_fast_horiz", "ms_per_launch": ms / n, "launches": n,
                 "bytes_per_launch": self.updates * self.alg_bytes}

@@ -542,7 +542,7 @@ int ica_set_step_geometry(ica_ctx *c, const double *GRD_x, const double *GRD_x_p
     cudaError_t e = cudaMemcpy(c->stepgeo[i], h[i], n[i] * sizeof(double), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(step geometry)");
   }
-  // FP32 copy of the gradient coefficients for the fused path
+  // FP32 copy of the gradient coefficients for the batched path
   std::vector<float> cg32(n[2]);
   for (size_t j = 0; j < n[2]; ++j) cg32[j] = (float)coef_grad[j];
   if (!c->fast.cg32 && cudaMalloc(&c->fast.cg32, n[2] * sizeof(float)) != cudaSuccess)
@@ -601,12 +601,12 @@ int ica_advect_step(ica_ctx *c, int ntr, double dt, double *rhog, double *rhog_p
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// fused batched path
+// batched path
 #include "fast_kernels.cuh"
 
 namespace icoadv {
 
-// Boundary tables of the fused path: which cells' gradient / Qout come from the
+// Boundary tables of the batched path: which cells' gradient / Qout come from the
 // boundary pass (region-boundary cells, halo cells through the COMM plan, pole centres).
 int Ctx::build_fast_tables() {
   if (fast.built) return ICA_OK;
@@ -730,6 +730,8 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
   I.sflux = (double *)buf("fast_sflux", (size_t)sz.kall * fast.ns * sizeof(double));
   I.sval = (float *)buf("fast_sval", (size_t)ntr * sz.kall * fast.ns * sizeof(float));
   if (!I.sflux || !I.sval) return set_error("cudaMalloc(fast seam buffers)"), ICA_ERR_NOMEM;
+  I.vco = (float4 *)buf("fast_vco", (size_t)sz.lall * sz.kall * sz.gall * sizeof(float4));
+  if (!I.vco) return set_error("cudaMalloc(fast vertical coefficients)"), ICA_ERR_NOMEM;
   return ICA_OK;
 }
 

@@ -1,4 +1,4 @@
-// Shared device code of the fused path: one instance of the grid, the FP64
+// Shared device code of the batched path: one instance of the grid, the FP64
 // face geometry and face bounds with every special case of the reference
 // (singular point, index clamps, unused faces), usable on global or shared data.
 #pragma once
@@ -11,7 +11,7 @@
 
 namespace icoadv {
 
-// One grid instance of the fused path (device pointers; region arrays in the
+// One grid instance of the batched path (device pointers; region arrays in the
 // reference layout (m, lall, kall, gall), pole arrays (m, 2, kall, 6)).
 struct FastInst {
   int G, gall, gmin, gmax, K, kmin, kmax, lall, ntr, ntx, nty;  // ntx/nty: tiles per region side
@@ -39,6 +39,7 @@ struct FastInst {
   double *sflux;  // (K, ns): 0.5 (rhov . HN) of the seam faces
   float *sval;    // (ntr, K, ns): limited face values of the seam faces
   double *bbuf;  // (ntr, K, nb, 5): grad x, y, z, Qout min, Qout max
+  float4 *vco;   // (lall, K, gall): ck(k,1), ck(k,2), 1/rhog, rhogw(k) after the horizontal sub-step
 };
 
 __device__ __forceinline__ double fsg(double a, double b) { return copysign(fabs(a), b); }

@@ -1,5 +1,5 @@
-// Fused batched tracer step: FP32 flux-form remap / limiter arithmetic on
-// interior faces, FP64 on region-seam faces, FP64 rhog / rhogq mass update.
+// Batched tracer step: FP32 flux-form remap / limiter arithmetic on interior
+// faces, FP64 on region-seam faces, FP64 rhog / rhogq mass update.
 //
 // Per step, on the context stream:
 //   k_fast_boundary  gradient and Thuburn outflow bounds Qout (FP64) of every
@@ -10,23 +10,23 @@
 //                    thread per (cell, level): the face geometry once, then the tracers.
 //   k_fast_seam      FP64 flux and limited value of every seam face (below), all tracers.
 //   k_fast_pole      the two pole centres (horizontal + vertical), FP64.
-//   k_fast_tile      one CTA per (region tile, group of TG tracers), one thread per
-//                    cell of the tile and its 1-wide ring, looping over the levels:
-//                    per level the tracer-independent part (triangle values, face
-//                    fluxes, Courant numbers, upwind masks and remap offsets) once,
-//                    then three phases over the TG tracers (q; gradient + Qout;
-//                    limited face values), the FP64 update and the vertical sub-step
-//                    streamed two levels behind in registers.
+//   k_fast_horiz     horizontal sub-step: one CTA per (region tile, level), one thread per
+//                    cell of the tile and its 1-wide ring; the tracer-independent part
+//                    (triangle values, face fluxes, Courant numbers, upwind masks, remap
+//                    offsets) once, then per batch of TB tracers three phases (q;
+//                    gradient + Qout; limited face values) and the FP64 update.
+//   k_fast_vert      vertical sub-step: one thread per (column, tracer) streaming the
+//                    levels, limiter two levels behind, FP64 update in place.
 //   k_fast_carry     halo points that no halo list writes keep their input values.
 //   gather           halo/pole fill of the new state (the COMM plan).
 //
 // Faces are "seam" faces when one of their two cells is a halo cell; the
 // neighbouring region computes the same face from its own halo copy, so those
-// faces are done in FP64 (seam_face, in k_fast_seam) from the FP64 boundary values.  An interior
-// face is computed by every tile that needs it from the same inputs by the same
-// instructions (cell positions enter only through the per-face offsets
-// GRD_xr - GRD_x, fixed per face), so both of its cells see the same value and
-// the flux form conserves mass to FP64 rounding.
+// faces are done in FP64 (seam_face, in k_fast_seam) from the FP64 boundary values.  An
+// interior face is computed by every tile that needs it from the same inputs by the same
+// instructions (cell positions enter only through the per-face offsets GRD_xr - GRD_x,
+// fixed per face), so both of its cells see the same value and the flux form conserves
+// mass to FP64 rounding.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -324,31 +324,30 @@ __device__ __forceinline__ void vlim_qout(const VLim &v, float qm, float qk, flo
   Qmax = ((qk - qnmin) + qnmin * v.icm - CQmin) * v.rden + qk * v.zsw;
 }
 
-// ---- the fused tile kernel ----------------------------------------------------------
-// Local frame: cell (i,j) of the region -> (x,y) = (i - i0, j - j0); the tile is
-// x in [0,TX), y in [0,TY); the ring (one thread per cell) x in [-1,TX], y in [-1,TY];
-// the window of shared per-cell data x in [-3,TX+1], y in [-3,TY+1].
+// ---- horizontal sub-step -----------------------------------------------------------
+// One CTA per (region tile, level), all tracers in batches of TB.  Local frame: cell (i,j)
+// of the region -> (x,y) = (i - i0, j - j0); the tile is x in [0,TX), y in [0,TY); the ring
+// (one thread per cell) x in [-1,TX], y in [-1,TY]; the window of shared per-cell data
+// x in [-3,TX+1], y in [-3,TY+1].
 template <int TX, int TY>
 struct TileGeo {
-  static constexpr int RW = TX + 2, RH = TY + 2, NT = RW * RH;
+  static constexpr int RW = TX + 2, RH = TY + 2, NR = RW * RH;  // ring cells
+  static constexpr int NT = (NR + 31) / 32 * 32;                // threads (whole warps)
   static constexpr int WW = TX + 5, WH = TY + 5, NW = WW * WH;
 };
 
-template <int TX, int TY, int TG>
+template <int TX, int TY, int TB>
 struct TileSmem {
   static constexpr int NT = TileGeo<TX, TY>::NT, NW = TileGeo<TX, TY>::NW;
-  float cg[21][NT];   // gradient coefficients of ring cells, [x*7 + n] (level-invariant)
-  float off[18][NT];  // remap offsets of the faces of ring cells (level-invariant)
-  double rinv[NW];    // 1 / rho
-  double F[3][NW];    // face flux 0.5 (rhov . HN) by owner (FP32 arithmetic on interior faces)
-  double flx[6][NT];  // flx_h of the tile cells (FP64)
+  double rinv[NW];  // 1 / rho
+  double F[3][NW];  // face flux 0.5 (rhov . HN) by owner (FP32 arithmetic on interior faces)
   float rho[NW];
   float v[3][NW];
-  float q[TG][NW];
+  float q[TB][NW];
   union {
     struct {
-      float gq[TG][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
-      float qa[TG][3][NT];  // limited face values of the faces owned by ring cells
+      float gq[TB][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
+      float qa[TB][3][NT];  // limited face values of the faces owned by ring cells
     } t;
     struct {
       float tri[2][4][NW];   // rho, rhovx, rhovy, rhovz at TI / TJ
@@ -357,224 +356,191 @@ struct TileSmem {
   } u;
 };
 
-template <int TX, int TY, int TG>
-__global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I) {
+template <int TX, int TY, int TB>
+__global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst I) {
   using Gm = TileGeo<TX, TY>;
-  using S = TileSmem<TX, TY, TG>;
-  constexpr int RW = Gm::RW, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW;
+  using S = TileSmem<TX, TY, TB>;
+  constexpr int RW = Gm::RW, NR = Gm::NR, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S &s = *reinterpret_cast<S *>(smem_raw);
 
-  const int ngroups = (I.ntr + TG - 1) / TG;
-  const int grp = blockIdx.x % ngroups;
-  const int tile = blockIdx.x / ngroups;
+  const int tile = blockIdx.x, k = 1 + blockIdx.y;
   const int tiles_per_rgn = I.ntx * I.nty;
   const int l = tile / tiles_per_rgn;
   const int tr = tile % tiles_per_rgn;
   const int i0 = I.gmin + (tr % I.ntx) * TX, j0 = I.gmin + (tr / I.ntx) * TY;
-  const int t0 = grp * TG;
-  const int ntg = min(TG, I.ntr - t0);
   const int tid = threadIdx.x;
-  const int G = I.G, K = I.K;
+  const int G = I.G, K = I.K, ntr = I.ntr;
   const bool sgp = I.have_sgp[l] != 0;
   const size_t slab = (size_t)I.gall, lk = (size_t)K * I.gall, tstride = (size_t)I.lall * K * I.gall;
+  const size_t base = (size_t)l * lk + (size_t)k * slab;
   const double dt = I.dt;
   const float dtf = (float)dt;
   const float BIGf = FLT_MAX, EPSf = FLT_EPSILON;
 
   // this thread's ring cell
-  const int x = tid % RW - 1, y = tid / RW - 1;
+  const bool ring = tid < NR;
+  const int x = ring ? tid % RW - 1 : TX + 8, y = ring ? tid / RW - 1 : TY + 8;
   const int ci = i0 + x, cj = j0 + y;
-  const int ec = (y + 3) * WW + (x + 3);
-  const bool in_arr = ci >= 1 && ci <= G && cj >= 1 && cj <= G;
+  const int ec = ring ? (y + 3) * WW + (x + 3) : 0;
+  const bool in_arr = ring && ci >= 1 && ci <= G && cj >= 1 && cj <= G;
   auto interior = [&](int i, int j) { return i >= I.gmin && i <= I.gmax && j >= I.gmin && j <= I.gmax; };
   const bool c_int = in_arr && interior(ci, cj);
   const int bs = in_arr ? I.bsrc[(size_t)l * I.gall + (cj - 1) * G + (ci - 1)] : -3;
-  const bool fp32_cell = c_int && bs == -1;                      // gradient / Qout in FP32 here
+  const bool fp32_cell = c_int && bs == -1;                          // gradient / Qout in FP32 here
   const bool active = x >= 0 && x < TX && y >= 0 && y < TY && c_int;  // updated by this thread
   const bool owner = x < TX && y < TY && in_arr;                     // face values of its 3 faces
-  const size_t ccell = (size_t)(cj - 1) * G + (ci - 1);
+  const size_t ccell = in_arr ? (size_t)(cj - 1) * G + (ci - 1) : 0;
   const double ra64 = c_int ? rarea(I, l, ci, cj) : 1.0;
   const float ra32 = (float)ra64;
 
-  // ---- level-invariant tables of the ring cells
-  for (int n = 0; n < 21; ++n)
-    s.cg[n][tid] = fp32_cell ? I.cg32[((size_t)l * 21 + n) * I.gall + ccell] : 0.0f;
-  for (int n = 0; n < 18; ++n)
-    s.off[n][tid] = (owner && ci <= G - 1 && cj <= G - 1) ? I.off32[((size_t)l * 18 + n) * I.gall + ccell] : 0.0f;
-
-  // vertical window, per tracer of the group (registers)
-  double Qh[TG][3];
-  float qv[TG][3], qmn_km1[TG], qmx_km1[TG], qh_last[TG];
-  double rh[3];   // rho after the horizontal sub-step at levels k-2, k-1, k
-  float ck1w[3];  // ck(k,1) at levels k-2..k
-  float ck2w[3];
-  float wf[3];    // rhogw at faces k-2..k (face k = below level k)
-#pragma unroll
-  for (int tt = 0; tt < TG; ++tt) {
-    qv[tt][0] = qv[tt][1] = qv[tt][2] = 0.0f;
-    qmn_km1[tt] = qmx_km1[tt] = qh_last[tt] = 0.0f;
-    Qh[tt][0] = Qh[tt][1] = Qh[tt][2] = 0.0;
+  // ---- (0a) fields of this level in the window
+  for (int e = tid; e < NW; e += NT) {
+    const int i = i0 - 3 + e % WW, j = j0 - 3 + e / WW;
+    if (i >= 1 && i <= G && j >= 1 && j <= G) {
+      const size_t o = base + (size_t)(j - 1) * G + (i - 1);
+      const double r = I.rho_in[o];
+      s.rinv[e] = 1.0 / r;
+      s.rho[e] = (float)r;
+      s.v[0][e] = I.vx[o];
+      s.v[1][e] = I.vy[o];
+      s.v[2][e] = I.vz[o];
+    } else {
+      s.rinv[e] = 1.0;
+      s.rho[e] = 1.0f;
+      s.v[0][e] = s.v[1][e] = s.v[2][e] = 0.0f;
+    }
   }
-  rh[0] = rh[1] = rh[2] = 0.0;
-  ck1w[0] = ck1w[1] = ck1w[2] = ck2w[0] = ck2w[1] = ck2w[2] = 0.0f;
-  wf[0] = wf[1] = wf[2] = 0.0f;
-
-  auto store = [&](int tt, int L, double val) {
-    if (!active) return;
-    I.Q_out[(size_t)(t0 + tt) * tstride + (size_t)l * lk + (size_t)L * slab + ccell] = val;
-  };
-
-  for (int k = 1; k <= K - 2; ++k) {
-    const size_t base = (size_t)l * lk + (size_t)k * slab;
-    // ---- (0a) fields of this level in the window
-    for (int e = tid; e < NW; e += NT) {
-      const int i = i0 - 3 + e % WW, j = j0 - 3 + e / WW;
-      if (i >= 1 && i <= G && j >= 1 && j <= G) {
-        const size_t o = base + (size_t)(j - 1) * G + (i - 1);
-        const double r = I.rho_in[o];
-        s.rinv[e] = 1.0 / r;
-        s.rho[e] = (float)r;
-        s.v[0][e] = I.vx[o];
-        s.v[1][e] = I.vy[o];
-        s.v[2][e] = I.vz[o];
-      } else {
-        s.rinv[e] = 1.0;
-        s.rho[e] = 1.0f;
-        s.v[0][e] = s.v[1][e] = s.v[2][e] = 0.0f;
+  __syncthreads();
+  // ---- (0b) triangle values TI, TJ (dyn_horiz_adv_flux/src/mod_src_tracer.f90:141-201), FP32
+  for (int e = tid; e < NW; e += NT) {
+    const int i = i0 - 3 + e % WW, j = j0 - 3 + e / WW;
+    const bool ok = i >= 1 && j >= 1 && i + 1 <= G && j + 1 <= G;
+    float ti[4] = {0, 0, 0, 0}, tj[4] = {0, 0, 0, 0};
+    if (ok && e % WW + 1 < WW && e / WW + 1 < Gm::WH) {
+      const float a1 = (float)gt(I, l, i, j, TI, W1), a2 = (float)gt(I, l, i, j, TI, W2),
+                  a3 = (float)gt(I, l, i, j, TI, W3);
+      const float b1 = (float)gt(I, l, i, j, TJ, W1), b2 = (float)gt(I, l, i, j, TJ, W2),
+                  b3 = (float)gt(I, l, i, j, TJ, W3);
+      const int e1 = e + 1, e2 = e + WW + 1, e3 = e + WW;
+      ti[0] = s.rho[e] * a1 + s.rho[e1] * a2 + s.rho[e2] * a3;
+      tj[0] = s.rho[e] * b1 + s.rho[e2] * b2 + s.rho[e3] * b3;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ti[c + 1] = s.v[c][e] * a1 + s.v[c][e1] * a2 + s.v[c][e2] * a3;
+        tj[c + 1] = s.v[c][e] * b1 + s.v[c][e2] * b2 + s.v[c][e3] * b3;
       }
     }
-    __syncthreads();
-    // ---- (0b) triangle values TI, TJ (dyn_horiz_adv_flux/src/mod_src_tracer.f90:141-201), FP32
-    for (int e = tid; e < NW; e += NT) {
-      const int i = i0 - 3 + e % WW, j = j0 - 3 + e / WW;
-      const bool ok = i >= 1 && j >= 1 && i + 1 <= G && j + 1 <= G;
-      float ti[4] = {0, 0, 0, 0}, tj[4] = {0, 0, 0, 0};
-      if (ok && e % WW + 1 < WW && e / WW + 1 < Gm::WH) {
-        const float a1 = (float)gt(I, l, i, j, TI, W1), a2 = (float)gt(I, l, i, j, TI, W2),
-                    a3 = (float)gt(I, l, i, j, TI, W3);
-        const float b1 = (float)gt(I, l, i, j, TJ, W1), b2 = (float)gt(I, l, i, j, TJ, W2),
-                    b3 = (float)gt(I, l, i, j, TJ, W3);
-        const int e1 = e + 1, e2 = e + WW + 1, e3 = e + WW;
-        ti[0] = s.rho[e] * a1 + s.rho[e1] * a2 + s.rho[e2] * a3;
-        tj[0] = s.rho[e] * b1 + s.rho[e2] * b2 + s.rho[e3] * b3;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          ti[c + 1] = s.v[c][e] * a1 + s.v[c][e1] * a2 + s.v[c][e2] * a3;
-          tj[c + 1] = s.v[c][e] * b1 + s.v[c][e2] * b2 + s.v[c][e3] * b3;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 4; ++c) s.u.f.tri[0][c][e] = ti[c], s.u.f.tri[1][c][e] = tj[c];
-    }
-    __syncthreads();
-    // ---- (0c) face fluxes and centroid displacements of owners x, y in [-2, T]
-    for (int e = tid; e < NW; e += NT) {
-      const int lx = e % WW, ly = e / WW;  // local slot: x = lx - 3
-      const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-      const bool own = lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3 && i >= 1 && j >= 1 && i < G && j < G;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        double F = 0.0;
-        float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
-        if (own && face_exists(I, i, j, a + 1)) {
-          const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
-          if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64 flux of k_fast_seam
-            const int sid = I.seam_id[((size_t)l * I.gall + (size_t)(j - 1) * G + (i - 1)) * 3 + a];
-            F = I.sflux[(size_t)k * I.ns + sid];
-          } else {
-            const int ep = (a == 0) ? e - WW : e, eq = (a == 2) ? e - 1 : e;  // TJ slot, TI slot
-            const int sp = (a == 0) ? 1 : (a == 1 ? 0 : 1), sq = (a == 0) ? 0 : (a == 1 ? 1 : 0);
-            const float pr = s.u.f.tri[sp][0][ep], qr = s.u.f.tri[sq][0][eq];
-            const float vx = s.u.f.tri[sp][1][ep] + s.u.f.tri[sq][1][eq];
-            const float vy = s.u.f.tri[sp][2][ep] + s.u.f.tri[sq][2][eq];
-            const float vz = s.u.f.tri[sp][3][ep] + s.u.f.tri[sq][3][eq];
-            const float rr = 1.0f / mx32(pr + qr, FLT_EPSILON);
-            const float Ff = 0.5f * (vx * (float)ga(I, l, i, j, a + 1, HNX) + vy * (float)ga(I, l, i, j, a + 1, HNY) +
-                                     vz * (float)ga(I, l, i, j, a + 1, HNZ));
-            F = (double)Ff;
-            d0 = -(vx * rr * dtf * 0.5f);
-            d1 = -(vy * rr * dtf * 0.5f);
-            d2 = -(vz * rr * dtf * 0.5f);
-          }
-        }
-        s.F[a][e] = F;
-        s.u.f.disp[a][0][e] = d0;
-        s.u.f.disp[a][1][e] = d1;
-        s.u.f.disp[a][2][e] = d2;
-      }
-    }
-    __syncthreads();
-    // ---- (0d) per ring cell: Courant numbers, masks, outflow sums; per owner: upwind
-    // offsets; per tile cell: flx_h (FP64) and rho after the horizontal sub-step
-    float chm[7], omc = 0.0f, rden = 0.0f, zsw = 1.0f;
-    unsigned inmask = 0, cmown = 0;
-    float dup[3][3];
-    const int nbe[7] = {0, ec, ec, ec, ec - 1, ec - WW - 1, ec - WW};  // owner slot of face m
-    if (fp32_cell) {
-      const float rc = s.rho[ec];
-      float ch[7];
-#pragma unroll
-      for (int m = 1; m <= 6; ++m) {
-        const float Fm = (float)s.F[(m - 1) % 3][nbe[m]];
-        ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) / rc;
-        chm[m] = mn32(ch[m], 0.0f);
-        float chown = ch[m];
-        if (m >= 4) {  // the owner's own Courant number of this face
-          const int oi = (m == 6) ? ci : ci - 1, oj = (m == 4) ? cj : cj - 1;
-          chown = (Fm * (float)rarea(I, l, oi, oj) * dtf) / s.rho[nbe[m]];
-        }
-        const float cm = 0.5f - copysignf(0.5f, chown - EPSf);
-        const bool in = (m <= 3) ? (cm != 0.0f) : (cm == 0.0f);
-        inmask |= in ? (1u << m) : 0u;
-      }
-      const float Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
-      const float Cout =
-          ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
-      zsw = 0.5f - copysignf(0.5f, fabsf(Cout) - EPSf);
-      omc = 1.0f - Cin - Cout;
-      rden = (1.0f - zsw) / (Cout + zsw);
-    }
+    for (int c = 0; c < 4; ++c) s.u.f.tri[0][c][e] = ti[c], s.u.f.tri[1][c][e] = tj[c];
+  }
+  __syncthreads();
+  // ---- (0c) face fluxes and centroid displacements of owners x, y in [-2, T]
+  for (int e = tid; e < NW; e += NT) {
+    const int lx = e % WW, ly = e / WW;  // local slot: x = lx - 3
+    const int i = i0 - 3 + lx, j = j0 - 3 + ly;
+    const bool own = lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3 && i >= 1 && j >= 1 && i < G && j < G;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      dup[a][0] = dup[a][1] = dup[a][2] = 0.0f;
-      if (owner && c_int) {
-        const float Fa = (float)s.F[a][ec];
-        const float chown = (Fa * ra32 * dtf) / s.rho[ec];
-        const bool cm = (0.5f - copysignf(0.5f, chown - EPSf)) != 0.0f;
-        cmown |= cm ? (1u << a) : 0u;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) dup[a][c] = s.off[a * 6 + (cm ? 3 : 0) + c][tid] + s.u.f.disp[a][c][ec];
+      double F = 0.0;
+      float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
+      if (own && face_exists(I, i, j, a + 1)) {
+        const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
+        if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64 flux of k_fast_seam
+          const int sid = I.seam_id[((size_t)l * I.gall + (size_t)(j - 1) * G + (i - 1)) * 3 + a];
+          F = I.sflux[(size_t)k * I.ns + sid];
+        } else {
+          const int ep = (a == 0) ? e - WW : e, eq = (a == 2) ? e - 1 : e;  // TJ slot, TI slot
+          const int sp = (a == 0) ? 1 : (a == 1 ? 0 : 1), sq = (a == 0) ? 0 : (a == 1 ? 1 : 0);
+          const float pr = s.u.f.tri[sp][0][ep], qr = s.u.f.tri[sq][0][eq];
+          const float vx = s.u.f.tri[sp][1][ep] + s.u.f.tri[sq][1][eq];
+          const float vy = s.u.f.tri[sp][2][ep] + s.u.f.tri[sq][2][eq];
+          const float vz = s.u.f.tri[sp][3][ep] + s.u.f.tri[sq][3][eq];
+          const float rr = 1.0f / mx32(pr + qr, FLT_EPSILON);
+          const float Ff = 0.5f * (vx * (float)ga(I, l, i, j, a + 1, HNX) + vy * (float)ga(I, l, i, j, a + 1, HNY) +
+                                   vz * (float)ga(I, l, i, j, a + 1, HNZ));
+          F = (double)Ff;
+          d0 = -(vx * rr * dtf * 0.5f);
+          d1 = -(vy * rr * dtf * 0.5f);
+          d2 = -(vz * rr * dtf * 0.5f);
+        }
       }
+      s.F[a][e] = F;
+      s.u.f.disp[a][0][e] = d0;
+      s.u.f.disp[a][1][e] = d1;
+      s.u.f.disp[a][2][e] = d2;
     }
-    double rho_h = 0.0;
-    if (active) {
-      double sum = 0.0;
+  }
+  __syncthreads();
+  // ---- (0d) per ring cell: Courant numbers, masks, outflow sums, gradient coefficients;
+  // per owner: upwind offsets; per tile cell: flx_h (FP64), rho after the horizontal
+  // sub-step and the tracer-independent inputs of the vertical sub-step
+  float chm[7], omc = 0.0f, rden = 0.0f, zsw = 1.0f, cgr[21];
+  unsigned inmask = 0, cmown = 0;
+  float dup[3][3];
+  const int nbe[7] = {0, ec, ec, ec, ec - 1, ec - WW - 1, ec - WW};  // owner slot of face m
 #pragma unroll
-      for (int m = 1; m <= 6; ++m) {
-        const double fl = cell_flx(I, l, ci, cj, m, sgp, s.F[(m - 1) % 3][nbe[m]], ra64);
-        s.flx[m - 1][tid] = fl;
-        sum = (m == 1) ? fl : sum + fl;
+  for (int m = 0; m < 7; ++m) chm[m] = 0.0f;
+#pragma unroll
+  for (int n = 0; n < 21; ++n) cgr[n] = fp32_cell ? I.cg32[((size_t)l * 21 + n) * I.gall + ccell] : 0.0f;
+  if (fp32_cell) {
+    const float rc = s.rho[ec];
+    float ch[7];
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) {
+      const float Fm = (float)s.F[(m - 1) % 3][nbe[m]];
+      ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) / rc;
+      chm[m] = mn32(ch[m], 0.0f);
+      float chown = ch[m];
+      if (m >= 4) {  // the owner's own Courant number of this face
+        const int oi = (m == 6) ? ci : ci - 1, oj = (m == 4) ? cj : cj - 1;
+        chown = (Fm * (float)rarea(I, l, oi, oj) * dtf) / s.rho[nbe[m]];
       }
-      rho_h = I.rho_in[base + ccell] - sum;
+      const float cm = 0.5f - copysignf(0.5f, chown - EPSf);
+      const bool in = (m <= 3) ? (cm != 0.0f) : (cm == 0.0f);
+      inmask |= in ? (1u << m) : 0u;
     }
-    // vertical window of shared quantities (slot 2 = level k)
-    rh[0] = rh[1];
-    rh[1] = rh[2];
-    rh[2] = rho_h;
-    wf[0] = wf[1];
-    wf[1] = wf[2];
-    wf[2] = active ? I.w[base + ccell] : 0.0f;
-    const float wtop = active ? I.w[base + slab + ccell] : 0.0f;  // face k+1
-    ck1w[0] = ck1w[1];
-    ck1w[1] = ck1w[2];
-    ck2w[0] = ck2w[1];
-    ck2w[1] = ck2w[2];
-    ck1w[2] = active ? (float)(-(double)wf[2] * dt * I.rdgz[k] / rho_h) : 0.0f;
-    ck2w[2] = active ? (float)((double)wtop * dt * I.rdgz[k] / rho_h) : 0.0f;
+    const float Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
+    const float Cout =
+        ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
+    zsw = 0.5f - copysignf(0.5f, fabsf(Cout) - EPSf);
+    omc = 1.0f - Cin - Cout;
+    rden = (1.0f - zsw) / (Cout + zsw);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    dup[a][0] = dup[a][1] = dup[a][2] = 0.0f;
+    if (owner && c_int) {
+      const float Fa = (float)s.F[a][ec];
+      const float chown = (Fa * ra32 * dtf) / s.rho[ec];
+      const bool cm = (0.5f - copysignf(0.5f, chown - EPSf)) != 0.0f;
+      cmown |= cm ? (1u << a) : 0u;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        dup[a][c] = I.off32[((size_t)l * 18 + a * 6 + (cm ? 3 : 0) + c) * I.gall + ccell] + s.u.f.disp[a][c][ec];
+    }
+  }
+  double flx[7];
+#pragma unroll
+  for (int m = 0; m < 7; ++m) flx[m] = 0.0;
+  if (active) {
+    double sum = 0.0;
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) {
+      flx[m] = cell_flx(I, l, ci, cj, m, sgp, s.F[(m - 1) % 3][nbe[m]], ra64);
+      sum = (m == 1) ? flx[m] : sum + flx[m];
+    }
+    const double rho_h = I.rho_in[base + ccell] - sum;
+    I.rho_out[base + ccell] = rho_h;
+    const float wk = I.w[base + ccell], wk1 = I.w[base + slab + ccell];
+    I.vco[base + ccell] = make_float4((float)(-(double)wk * dt * I.rdgz[k] / rho_h),
+                                      (float)((double)wk1 * dt * I.rdgz[k] / rho_h), (float)(1.0 / rho_h), wk);
+  }
 
-    // ---- (A) q of the group's tracers in the window x, y in [-2, T+1]
-    for (int idx = tid; idx < TG * NW; idx += NT) {
+  for (int t0 = 0; t0 < ntr; t0 += TB) {
+    const int ntg = min(TB, ntr - t0);
+    // ---- (A) q of the batch's tracers in the window x, y in [-2, T+1]
+    for (int idx = tid; idx < TB * NW; idx += NT) {
       const int tt = idx / NW, e = idx % NW;
       const int lx = e % WW, ly = e / WW;
       const int i = i0 - 3 + lx, j = j0 - 3 + ly;
@@ -588,7 +554,7 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
     if (in_arr) {
       if (bs >= 0) {  // region-boundary cell or halo cell: the FP64 boundary values
 #pragma unroll
-        for (int tt = 0; tt < TG; ++tt) {
+        for (int tt = 0; tt < TB; ++tt) {
           if (tt >= ntg) break;
           const double *bv = bval(I, t0 + tt, k, bs);
 #pragma unroll
@@ -596,30 +562,27 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
         }
       } else if (!fp32_cell) {  // halo point no list reaches: grad 0, Qout = q
 #pragma unroll
-        for (int tt = 0; tt < TG; ++tt) {
+        for (int tt = 0; tt < TB; ++tt) {
           s.u.t.gq[tt][0][tid] = s.u.t.gq[tt][1][tid] = s.u.t.gq[tt][2][tid] = 0.0f;
           s.u.t.gq[tt][3][tid] = s.u.t.gq[tt][4][tid] = s.q[tt][ec];
         }
       } else {
-        float g[TG][3];
-#pragma unroll
-        for (int tt = 0; tt < TG; ++tt) g[tt][0] = g[tt][1] = g[tt][2] = 0.0f;
         const int st7[7] = {ec, ec + 1, ec + WW + 1, ec + WW, ec - 1, ec - WW - 1, ec - WW};
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
+        for (int tt = 0; tt < TB; ++tt) {
+          float qs[7];
 #pragma unroll
-          for (int n = 0; n < 7; ++n) {
-            const float cf = s.cg[c * 7 + n][tid];
+          for (int n = 0; n < 7; ++n) qs[n] = s.q[tt][st7[n]];
+          float g[3];
 #pragma unroll
-            for (int tt = 0; tt < TG; ++tt)
-              g[tt][c] = (n == 0) ? cf * s.q[tt][st7[0]] : g[tt][c] + cf * s.q[tt][st7[n]];
+          for (int c = 0; c < 3; ++c) {
+            g[c] = cgr[c * 7] * qs[0];
+#pragma unroll
+            for (int n = 1; n < 7; ++n) g[c] = g[c] + cgr[c * 7 + n] * qs[n];
           }
-        }
-#pragma unroll
-        for (int tt = 0; tt < TG; ++tt) {
-          const float c0 = s.q[tt][st7[0]], n1 = s.q[tt][st7[1]], n2 = s.q[tt][st7[2]], n3 = s.q[tt][st7[3]],
-                      n4 = s.q[tt][st7[4]], n5 = s.q[tt][st7[5]], n6 = s.q[tt][st7[6]];
-          // 4-point bounds of the 6 faces (owner q first, as mod_src_tracer.f90:152-214)
+          // 4-point bounds of the 6 faces: the cell and three consecutive neighbours
+          // (owner q first, as mod_src_tracer.f90:152-214)
+          const float c0 = qs[0], n1 = qs[1], n2 = qs[2], n3 = qs[3], n4 = qs[4], n5 = qs[5], n6 = qs[6];
           float lo[7], hi[7];
           lo[1] = mn32(mn32(mn32(c0, n6), n1), n2), hi[1] = mx32(mx32(mx32(c0, n6), n1), n2);
           lo[2] = mn32(mn32(mn32(c0, n1), n2), n3), hi[2] = mx32(mx32(mx32(c0, n1), n2), n3);
@@ -637,9 +600,9 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
             CQmin = (m == 1) ? chm[1] * qmn : CQmin + chm[m] * qmn;
             CQmax = (m == 1) ? chm[1] * qmx : CQmax + chm[m] * qmx;
           }
-          s.u.t.gq[tt][0][tid] = g[tt][0];
-          s.u.t.gq[tt][1][tid] = g[tt][1];
-          s.u.t.gq[tt][2][tid] = g[tt][2];
+          s.u.t.gq[tt][0][tid] = g[0];
+          s.u.t.gq[tt][1][tid] = g[1];
+          s.u.t.gq[tt][2][tid] = g[2];
           s.u.t.gq[tt][3][tid] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
           s.u.t.gq[tt][4][tid] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
         }
@@ -657,13 +620,13 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
         const bool need = (x >= 0 && y >= 0) || (ni - i0 >= 0 && nj - j0 >= 0 && ni - i0 < TX && nj - j0 < TY);
         if (!need || !face_exists(I, ci, cj, a + 1)) {
 #pragma unroll
-          for (int tt = 0; tt < TG; ++tt) s.u.t.qa[tt][a][tid] = 0.0f;
+          for (int tt = 0; tt < TB; ++tt) s.u.t.qa[tt][a][tid] = 0.0f;
           continue;
         }
         if (!c_int || !interior(ni, nj)) {  // seam face: value of k_fast_seam
           const int sid = I.seam_id[((size_t)l * I.gall + ccell) * 3 + a];
 #pragma unroll
-          for (int tt = 0; tt < TG; ++tt) {
+          for (int tt = 0; tt < TB; ++tt) {
             if (tt >= ntg) break;
             s.u.t.qa[tt][a][tid] = I.sval[((size_t)(t0 + tt) * K + k) * I.ns + sid];
           }
@@ -672,7 +635,7 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
         const bool cmu = (cmown >> a) & 1u;  // 1: the neighbour is upwind
         const int ut = cmu ? nbt[a] : tid, us = cmu ? nbs[a] : ec;
 #pragma unroll
-        for (int tt = 0; tt < TG; ++tt) {
+        for (int tt = 0; tt < TB; ++tt) {
           float v = s.q[tt][us];
           v = v + s.u.t.gq[tt][0][ut] * dup[a][0];
           v = v + s.u.t.gq[tt][1][ut] * dup[a][1];
@@ -690,107 +653,118 @@ __global__ void __launch_bounds__((TX + 2) * (TY + 2), 2) k_fast_tile(FastInst I
       }
     }
     __syncthreads();
-    // ---- (D) horizontal update of the tile cells (FP64) and the vertical stream
+    // ---- (D) horizontal update of the tile cells (FP64): rhogq after the horizontal sub-step
     if (active) {
-      const double rinvh = 1.0 / rho_h;
-      const VLim vp = vlim_params(ck1w[1], ck2w[1], ck1w[2]);  // level k-1 (used from k = 2)
 #pragma unroll
-      for (int tt = 0; tt < TG; ++tt) {
+      for (int tt = 0; tt < TB; ++tt) {
         if (tt >= ntg) break;
-        const double *Qt = I.Q_in + (size_t)(t0 + tt) * tstride + base;
+        const size_t o = (size_t)(t0 + tt) * tstride + base + ccell;
         const float qa[7] = {0.0f, s.u.t.qa[tt][0][tid], s.u.t.qa[tt][1][tid], s.u.t.qa[tt][2][tid],
                              s.u.t.qa[tt][0][tid - 1], s.u.t.qa[tt][1][tid - RW - 1], s.u.t.qa[tt][2][tid - RW]};
-        double sum = s.flx[0][tid] * (double)qa[1];
+        double sum = flx[1] * (double)qa[1];
 #pragma unroll
-        for (int m = 2; m <= 6; ++m) sum = sum + s.flx[m - 1][tid] * (double)qa[m];
-        const double Qhk = Qt[ccell] - sum;
-        Qh[tt][0] = Qh[tt][1];
-        Qh[tt][1] = Qh[tt][2];
-        Qh[tt][2] = Qhk;
-        qv[tt][0] = qv[tt][1];
-        qv[tt][1] = qv[tt][2];
-        qv[tt][2] = (float)(Qhk * rinvh);
-        if (k == 1) {  // ghost level below: q(kmin-1) = q(kmin)
-          qv[tt][1] = qv[tt][2];
-          qh_last[tt] = 0.0f;
-        }
-        if (k >= 2) {
-          // Qout of level k-1 (window slot 1) from q at k-2, k-1, k
-          float Qmin, Qmax;
-          const float infl = vp.infl;
-          vlim_qout(vp, qv[tt][0], qv[tt][1], qv[tt][2], Qmin, Qmax);
-          // face k-1 (between levels k-2 and k-1)
-          const int f = k - 1;
-          float qh = (float)I.afact[f] * qv[tt][1] + (float)I.bfact[f] * qv[tt][0];
-          if (f >= 2) {
-            qh = infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - infl) * mx32(mn32(qh, Qmax), Qmin);
-          }
-          // level k-2 is final once faces k-2 and k-1 are
-          if (k - 2 >= 1) {
-            const int L = k - 2;
-            const double fu = (double)wf[1] * (double)qh, fl = (double)wf[0] * (double)qh_last[tt];
-            const double Qn = Qh[tt][0] - (fu - fl) * dt * I.rdgz[L];
-            store(tt, L, Qn);
-            if (L == 1) store(tt, 0, Qn);
-          }
-          qh_last[tt] = qh;
-          qmn_km1[tt] = Qmin;
-          qmx_km1[tt] = Qmax;
-        }
-      }
-      // density: level k-2 final (one group writes it)
-      if (grp == 0 && k >= 3) {
-        const int L = k - 2;
-        const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dt * I.rdgz[L];
-        I.rho_out[(size_t)l * lk + (size_t)L * slab + ccell] = rn;
-        if (L == 1) I.rho_out[(size_t)l * lk + ccell] = rn;
+        for (int m = 2; m <= 6; ++m) sum = sum + flx[m] * (double)qa[m];
+        I.Q_out[o] = I.Q_in[o] - sum;
       }
     }
   }
-  // ---- drain: levels K-3 and K-2 (faces K-2 and K-1)
-  if (active) {
-    const int kk = K - 1;  // ghost level above: q(kmax+1) = q(kmax)
-    const float c1top = (float)(-(double)I.w[(size_t)l * lk + (size_t)kk * slab + ccell] * dt * I.rdgz[kk] /
-                                I.rho_in[(size_t)l * lk + (size_t)kk * slab + ccell]);
-    const VLim vd = vlim_params(ck1w[2], ck2w[2], c1top);  // level K-2 with q(K-1) := q(K-2)
-#pragma unroll
-    for (int tt = 0; tt < TG; ++tt) {
-      if (tt >= ntg) break;
-      float Qmin, Qmax;
-      const float infl = vd.infl;
-      vlim_qout(vd, qv[tt][1], qv[tt][2], qv[tt][2], Qmin, Qmax);
-      const int f = K - 2;
-      float qh = (float)I.afact[f] * qv[tt][2] + (float)I.bfact[f] * qv[tt][1];
-      if (f >= 2) qh = infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - infl) * mx32(mn32(qh, Qmax), Qmin);
-      if (K - 3 >= 1) {
-        const int L = K - 3;
-        const double fu = (double)wf[2] * (double)qh, fl = (double)wf[1] * (double)qh_last[tt];
-        const double Qn = Qh[tt][1] - (fu - fl) * dt * I.rdgz[L];
-        store(tt, L, Qn);
-        if (L == 1) store(tt, 0, Qn);
-      }
-      // top face K-1: unlimited
-      const float qtop = (float)I.afact[kk] * qv[tt][2] + (float)I.bfact[kk] * qv[tt][2];
-      const float wk1 = I.w[(size_t)l * lk + (size_t)kk * slab + ccell];
-      const double fu = (double)wk1 * (double)qtop, fl = (double)wf[2] * (double)qh;
-      const double Qn = Qh[tt][2] - (fu - fl) * dt * I.rdgz[K - 2];
-      store(tt, K - 2, Qn);
-      store(tt, K - 1, Qn);
-      if (K - 2 == 1) store(tt, 0, Qn);
+}
+
+// ---- vertical sub-step: one thread per (interior column, tracer), streaming the levels
+// with the limiter two levels behind; FP32 limiter, FP64 update.  rhogq after the
+// horizontal sub-step is read from (and the result written to) Q_out; tracer 0's threads
+// also finish rhog.  blockIdx.x = tracer, so the tracers of a column block run together
+// and share the per-level inputs (vco) in L2.
+__global__ void __launch_bounds__(256) k_fast_vert(FastInst I) {
+  const int t = blockIdx.x;
+  const int n = I.gmax - I.gmin + 1;
+  const long long col = (long long)blockIdx.y * blockDim.x + threadIdx.x;
+  if (col >= (long long)I.lall * n * n) return;
+  const int l = (int)(col / ((long long)n * n)), r = (int)(col % ((long long)n * n));
+  const int i = I.gmin + r % n, j = I.gmin + r / n;
+  const int K = I.K;
+  const size_t slab = (size_t)I.gall;
+  const size_t cbase = (size_t)l * K * slab + (size_t)(j - 1) * I.G + (i - 1);
+  double *Q = I.Q_out + (size_t)t * I.lall * K * slab + cbase;
+  double *R = I.rho_out + cbase;
+  const float4 *V = I.vco + cbase;
+  const bool dens = t == 0;
+  const double dt = I.dt;
+  float ck1w[3] = {0.0f, 0.0f, 0.0f}, ck2w[3] = {0.0f, 0.0f, 0.0f}, wf[3] = {0.0f, 0.0f, 0.0f};
+  double Qh[3] = {0.0, 0.0, 0.0}, rh[3] = {0.0, 0.0, 0.0};
+  float qv[3] = {0.0f, 0.0f, 0.0f};
+  float qmn_km1 = 0.0f, qmx_km1 = 0.0f, qh_last = 0.0f;
+  for (int k = 1; k <= K - 2; ++k) {
+    const float4 c = V[(size_t)k * slab];
+    ck1w[0] = ck1w[1], ck1w[1] = ck1w[2], ck1w[2] = c.x;
+    ck2w[0] = ck2w[1], ck2w[1] = ck2w[2], ck2w[2] = c.y;
+    wf[0] = wf[1], wf[1] = wf[2], wf[2] = c.w;
+    const double Qhk = Q[(size_t)k * slab];
+    Qh[0] = Qh[1], Qh[1] = Qh[2], Qh[2] = Qhk;
+    qv[0] = qv[1], qv[1] = qv[2], qv[2] = (float)(Qhk * (double)c.z);
+    if (dens) rh[0] = rh[1], rh[1] = rh[2], rh[2] = R[(size_t)k * slab];
+    if (k == 1) {  // ghost level below: q(kmin-1) = q(kmin)
+      qv[1] = qv[2];
+      qh_last = 0.0f;
+      continue;
     }
-    if (grp == 0) {
-      const float wk1 = I.w[(size_t)l * lk + (size_t)kk * slab + ccell];
-      if (K - 3 >= 1) {
-        const int L = K - 3;
-        const double rn = rh[1] - ((double)wf[2] - (double)wf[1]) * dt * I.rdgz[L];
-        I.rho_out[(size_t)l * lk + (size_t)L * slab + ccell] = rn;
-        if (L == 1) I.rho_out[(size_t)l * lk + ccell] = rn;
+    // Qout of level k-1 from q at k-2, k-1, k; the face k-1 between levels k-2 and k-1
+    const VLim vp = vlim_params(ck1w[1], ck2w[1], ck1w[2]);
+    float Qmin, Qmax;
+    vlim_qout(vp, qv[0], qv[1], qv[2], Qmin, Qmax);
+    const int f = k - 1;
+    float qh = (float)I.afact[f] * qv[1] + (float)I.bfact[f] * qv[0];
+    if (f >= 2) qh = vp.infl * mx32(mn32(qh, qmx_km1), qmn_km1) + (1.0f - vp.infl) * mx32(mn32(qh, Qmax), Qmin);
+    if (k - 2 >= 1) {  // level k-2 is final once faces k-2 and k-1 are
+      const int L = k - 2;
+      const double fu = (double)wf[1] * (double)qh, fl = (double)wf[0] * (double)qh_last;
+      const double Qn = Qh[0] - (fu - fl) * dt * I.rdgz[L];
+      Q[(size_t)L * slab] = Qn;
+      if (L == 1) Q[0] = Qn;
+      if (dens) {
+        const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dt * I.rdgz[L];
+        R[(size_t)L * slab] = rn;
+        if (L == 1) R[0] = rn;
       }
-      const double rn = rh[2] - ((double)wk1 - (double)wf[2]) * dt * I.rdgz[K - 2];
-      I.rho_out[(size_t)l * lk + (size_t)(K - 2) * slab + ccell] = rn;
-      I.rho_out[(size_t)l * lk + (size_t)(K - 1) * slab + ccell] = rn;
-      if (K - 2 == 1) I.rho_out[(size_t)l * lk + ccell] = rn;
     }
+    qh_last = qh;
+    qmn_km1 = Qmin;
+    qmx_km1 = Qmax;
+  }
+  // ---- drain: levels K-3 and K-2 (faces K-2 and K-1); ghost level above: q(kmax+1) = q(kmax)
+  const int kk = K - 1;
+  const float wk1 = I.w[cbase + (size_t)kk * slab];
+  const float c1top = (float)(-(double)wk1 * dt * I.rdgz[kk] / I.rho_in[cbase + (size_t)kk * slab]);
+  const VLim vd = vlim_params(ck1w[2], ck2w[2], c1top);  // level K-2 with q(K-1) := q(K-2)
+  float Qmin, Qmax;
+  vlim_qout(vd, qv[1], qv[2], qv[2], Qmin, Qmax);
+  const int f = K - 2;
+  float qh = (float)I.afact[f] * qv[2] + (float)I.bfact[f] * qv[1];
+  if (f >= 2) qh = vd.infl * mx32(mn32(qh, qmx_km1), qmn_km1) + (1.0f - vd.infl) * mx32(mn32(qh, Qmax), Qmin);
+  if (K - 3 >= 1) {
+    const int L = K - 3;
+    const double fu = (double)wf[2] * (double)qh, fl = (double)wf[1] * (double)qh_last;
+    const double Qn = Qh[1] - (fu - fl) * dt * I.rdgz[L];
+    Q[(size_t)L * slab] = Qn;
+    if (L == 1) Q[0] = Qn;
+    if (dens) {
+      const double rn = rh[1] - ((double)wf[2] - (double)wf[1]) * dt * I.rdgz[L];
+      R[(size_t)L * slab] = rn;
+      if (L == 1) R[0] = rn;
+    }
+  }
+  // top face K-1: unlimited
+  const float qtop = (float)I.afact[kk] * qv[2] + (float)I.bfact[kk] * qv[2];
+  const double fu = (double)wk1 * (double)qtop, fl = (double)wf[2] * (double)qh;
+  const double Qn = Qh[2] - (fu - fl) * dt * I.rdgz[K - 2];
+  Q[(size_t)(K - 2) * slab] = Qn;
+  Q[(size_t)(K - 1) * slab] = Qn;
+  if (K - 2 == 1) Q[0] = Qn;
+  if (dens) {
+    const double rn = rh[2] - ((double)wk1 - (double)wf[2]) * dt * I.rdgz[K - 2];
+    R[(size_t)(K - 2) * slab] = rn;
+    R[(size_t)(K - 1) * slab] = rn;
+    if (K - 2 == 1) R[0] = rn;
   }
 }
 
@@ -906,20 +880,19 @@ __global__ void k_fast_carry(FastInst I) {
 }
 
 // ---------------------------------------------------------------------------------------
-template <int TX, int TY, int TG>
+template <int TX, int TY, int TB>
 static cudaError_t launch_tile(const FastInst &I, cudaStream_t st) {
-  const size_t smem = sizeof(TileSmem<TX, TY, TG>);
-  cudaError_t e = cudaFuncSetAttribute(k_fast_tile<TX, TY, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const size_t smem = sizeof(TileSmem<TX, TY, TB>);
+  cudaError_t e = cudaFuncSetAttribute(k_fast_horiz<TX, TY, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  const int ngroups = (I.ntr + TG - 1) / TG;
-  const long long blocks = (long long)I.lall * I.ntx * I.nty * ngroups;
-  k_fast_tile<TX, TY, TG><<<(unsigned)blocks, TileGeo<TX, TY>::NT, smem, st>>>(I);
+  const dim3 grid((unsigned)(I.lall * I.ntx * I.nty), (unsigned)(I.K - 2));
+  k_fast_horiz<TX, TY, TB><<<grid, TileGeo<TX, TY>::NT, smem, st>>>(I);
   return cudaGetLastError();
 }
 
 int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax) {
-  static const int shapes[][3] = {{14, 14, 4}, {30, 6, 4}, {14, 14, 2}, {14, 14, 8}, {6, 30, 4}};
+  static const int shapes[][3] = {{16, 16, 4}, {16, 16, 8}, {16, 16, 2}, {14, 14, 4}, {32, 8, 4}};
   const int n = sizeof(shapes) / sizeof(shapes[0]);
   if (tx)
     for (int i = 0; i < n; ++i) tx[i] = shapes[i][0], ty[i] = shapes[i][1], tg[i] = shapes[i][2];
@@ -945,17 +918,21 @@ cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t
   if (ev0) cudaEventRecord(ev0, st);
   cudaError_t e;
   switch (shape) {
-    case 0: e = launch_tile<14, 14, 4>(I, st); break;
-    case 1: e = launch_tile<30, 6, 4>(I, st); break;
-    case 2: e = launch_tile<14, 14, 2>(I, st); break;
-    case 3: e = launch_tile<14, 14, 8>(I, st); break;
-    case 4: e = launch_tile<6, 30, 4>(I, st); break;
+    case 0: e = launch_tile<16, 16, 4>(I, st); break;
+    case 1: e = launch_tile<16, 16, 8>(I, st); break;
+    case 2: e = launch_tile<16, 16, 2>(I, st); break;
+    case 3: e = launch_tile<14, 14, 4>(I, st); break;
+    case 4: e = launch_tile<32, 8, 4>(I, st); break;
     default: return cudaErrorInvalidValue;
   }
   if (ev1) cudaEventRecord(ev1, st);
+  if (e != cudaSuccess) return e;
+  const int n = I.gmax - I.gmin + 1;
+  const long long ncol = (long long)I.lall * n * n;
+  k_fast_vert<<<dim3((unsigned)I.ntr, (unsigned)((ncol + 255) / 256)), 256, 0, st>>>(I);
   const long long nc = (long long)I.ncarry * I.K;
   k_fast_carry<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(I);
-  launches += 5;
+  launches += 6;
   return e;
 }
 

@@ -1,4 +1,4 @@
-// Launch interface of the fused batched path.
+// Launch interface of the batched path.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -12,8 +12,8 @@ int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax);
 // Per-face remap offsets (GRD_xr - GRD_x of the owner and of the neighbour, FP32) into
 // off (lall, 18, gall); needs I's geometry pointers only.
 cudaError_t fast_build_offsets(const FastInst &I, float *off, cudaStream_t st);
-// One fused step of instance I on stream st with tile shape `shape`; ev0/ev1 (optional)
-// are recorded around the tile kernel, the dominant launch.
+// One step of instance I on stream st with tile shape `shape` (of k_fast_horiz); ev0/ev1
+// (optional) are recorded around k_fast_horiz, the dominant launch.
 cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
                       long long &launches);
 

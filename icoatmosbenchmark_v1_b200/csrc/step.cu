@@ -1,7 +1,7 @@
 // The composed tracer step, plain FP64 path: the reference kernels chained with
 // the pieces the reference leaves out (Courant numbers, gradient, remap,
 // rhogq update, vertical flux), one kernel each, tracer by tracer.  This is
-// the "plain per-tracer" GPU path; the fused batched path is fast_kernels.cu.
+// the "plain per-tracer" GPU path; the batched path is fast_kernels.cu.
 //
 // The composition (horizontal sub-step, then vertical sub-step, then the halo
 // fill of the state) and every formula match the CPU oracle's definition of

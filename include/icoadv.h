@@ -237,10 +237,11 @@ int ica_advect_step_dev(ica_ctx *ctx, int ntr, double dt,
                         const double *rhogvz, const double *rhogvz_pl,
                         const double *rhogw, const double *rhogw_pl);
 
-/* Fused batched step: all tracers of the step in one tile kernel, FP32
- * flux-form remap / limiter arithmetic on interior faces, FP64 on the faces
- * between a region and its halo, FP64 rhog / rhogq update (conservative to
- * FP64 rounding).  Same composition and state layout as ica_advect_step; the
+/* Batched step: all tracers of the step together, a horizontal kernel (one
+ * CTA per region tile and level) and a vertical kernel (one thread per column
+ * and tracer); FP32 flux-form remap / limiter arithmetic on interior faces,
+ * FP64 on the faces between a region and its halo, FP64 rhog / rhogq update
+ * (conservative to FP64 rounding).  Same composition and state layout as ica_advect_step; the
  * fields are FP32.  Device pointers, asynchronous on the context stream; the
  * state goes from the *_in to the *_out buffers (which must differ) with the
  * halos of the output filled.  Needs 4 <= kall <= 128. */
@@ -260,12 +261,12 @@ int ica_advect_fast(ica_ctx *ctx, int ntr, double dt,
                     const float *rhogvy, const float *rhogvy_pl,
                     const float *rhogvz, const float *rhogvz_pl,
                     const float *rhogw, const float *rhogw_pl);
-/* Tile shapes of the fused kernel (TX x TY cells, TG tracers per CTA): *n shapes;
+/* Tile shapes of the horizontal kernel (TX x TY cells, TG tracers per batch): *n shapes;
  * tx/ty/tg (may be NULL) receive them.  ica_fast_set_shape selects one (the
  * autotuner in the Python layer times them and keeps the fastest). */
 int ica_fast_shapes(ica_ctx *ctx, int *n, int *tx, int *ty, int *tg);
 int ica_fast_set_shape(ica_ctx *ctx, int shape);
-/* CUDA-event timing of the fused tile kernel: returns the total milliseconds and
+/* CUDA-event timing of the horizontal kernel: returns the total milliseconds and
  * the number of launches recorded since the last call, then enables (1) or
  * disables (0) recording for the following calls.  Synchronises the stream. */
 int ica_fast_timing(ica_ctx *ctx, int enable, double *ms_total, long long *count);
