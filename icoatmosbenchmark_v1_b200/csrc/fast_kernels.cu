@@ -15,7 +15,7 @@
 //                    (triangle values, face fluxes, Courant numbers, upwind masks, remap
 //                    offsets) once, then per batch of TB tracers three phases (q;
 //                    gradient + Qout; limited face values) and the FP64 update.
-//   k_fast_vert      vertical sub-step: one thread per (column, tracer) streaming the
+//   k_fast_vert      vertical sub-step: one thread per (column, 4 tracers) streaming the
 //                    levels, limiter two levels behind, FP64 update in place.
 //   k_fast_carry     halo points that no halo list writes keep their input values.
 //   gather           halo/pole fill of the new state (the COMM plan).
@@ -334,6 +334,9 @@ struct TileGeo {
   static constexpr int RW = TX + 2, RH = TY + 2, NR = RW * RH;  // ring cells
   static constexpr int NT = (NR + 31) / 32 * 32;                // threads (whole warps)
   static constexpr int WW = TX + 5, WH = TY + 5, NW = WW * WH;
+  // row stride of the q window: congruent to RW mod 32, so that the cells of a warp (whole
+  // ring rows in thread order) fall on 32 different banks in every stencil access
+  static constexpr int QW = WW + ((RW - WW) % 32 + 32) % 32, NQ = QW * WH;
 };
 
 template <int TX, int TY, int TB>
@@ -343,7 +346,8 @@ struct TileSmem {
   double F[3][NW];  // face flux 0.5 (rhov . HN) by owner (FP32 arithmetic on interior faces)
   float rho[NW];
   float v[3][NW];
-  float q[TB][NW];
+  double stage[2][TB][NW];  // rhogq of the window, FP64, two batches in flight (cp.async)
+  float q[TB][TileGeo<TX, TY>::NQ];
   union {
     struct {
       float gq[TB][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
@@ -360,7 +364,7 @@ template <int TX, int TY, int TB>
 __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst I) {
   using Gm = TileGeo<TX, TY>;
   using S = TileSmem<TX, TY, TB>;
-  constexpr int RW = Gm::RW, NR = Gm::NR, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW;
+  constexpr int RW = Gm::RW, NR = Gm::NR, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW, QW = Gm::QW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S &s = *reinterpret_cast<S *>(smem_raw);
 
@@ -382,7 +386,8 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst 
   const bool ring = tid < NR;
   const int x = ring ? tid % RW - 1 : TX + 8, y = ring ? tid / RW - 1 : TY + 8;
   const int ci = i0 + x, cj = j0 + y;
-  const int ec = ring ? (y + 3) * WW + (x + 3) : 0;
+  const int ec = ring ? (y + 3) * WW + (x + 3) : 0;   // window slot of the cell
+  const int eq = ring ? (y + 3) * QW + (x + 3) : 0;   // its q slot
   const bool in_arr = ring && ci >= 1 && ci <= G && cj >= 1 && cj <= G;
   auto interior = [&](int i, int j) { return i >= I.gmin && i <= I.gmax && j >= I.gmin && j <= I.gmax; };
   const bool c_int = in_arr && interior(ci, cj);
@@ -537,19 +542,52 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst 
                                       (float)((double)wk1 * dt * I.rdgz[k] / rho_h), (float)(1.0 / rho_h), wk);
   }
 
-  for (int t0 = 0; t0 < ntr; t0 += TB) {
-    const int ntg = min(TB, ntr - t0);
-    // ---- (A) q of the batch's tracers in the window x, y in [-2, T+1]
-    for (int idx = tid; idx < TB * NW; idx += NT) {
-      const int tt = idx / NW, e = idx % NW;
-      const int lx = e % WW, ly = e / WW;
-      const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-      float qv0 = 0.0f;
-      if (tt < ntg && lx >= 1 && ly >= 1 && i >= 1 && i <= G && j >= 1 && j <= G)
-        qv0 = (float)(I.Q_in[(size_t)(t0 + tt) * tstride + base + (size_t)(j - 1) * G + (i - 1)] * s.rinv[e]);
-      s.q[tt][e] = qv0;
+  // the window slots of this thread (e = tid + r*NT): global offset in the level, q slot
+  constexpr int NSLOT = (NW + NT - 1) / NT;
+  int sofs[NSLOT], sq[NSLOT];
+  bool sok[NSLOT];
+#pragma unroll
+  for (int r = 0; r < NSLOT; ++r) {
+    const int e = tid + r * NT;
+    const int lx = e % WW, ly = e / WW;
+    const int i = i0 - 3 + lx, j = j0 - 3 + ly;
+    sok[r] = e < NW && lx >= 1 && ly >= 1 && i >= 1 && i <= G && j >= 1 && j <= G;
+    sofs[r] = sok[r] ? (j - 1) * G + (i - 1) : 0;
+    sq[r] = ly * QW + lx;
+  }
+  // rhogq window of the batch starting at tracer tb into stage[buf], asynchronously
+  auto issue = [&](int tb, int buf) {
+    const int nb = min(TB, ntr - tb);
+#pragma unroll
+    for (int tt = 0; tt < TB; ++tt) {
+      if (tt >= nb) break;
+      const double *src = I.Q_in + (size_t)(tb + tt) * tstride + base;
+#pragma unroll
+      for (int r = 0; r < NSLOT; ++r)
+        if (sok[r]) {
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(&s.stage[buf][tt][tid + r * NT]);
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src + sofs[r]));
+        }
     }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  issue(0, 0);
+  for (int t0 = 0, b = 0; t0 < ntr; t0 += TB, ++b) {
+    const int ntg = min(TB, ntr - t0);
+    asm volatile("cp.async.wait_group 0;\n" ::);  // this thread's copies of batch b have landed
     __syncthreads();
+    // ---- (A) q of the batch's tracers in the window x, y in [-2, T+1]
+#pragma unroll
+    for (int tt = 0; tt < TB; ++tt)
+#pragma unroll
+      for (int r = 0; r < NSLOT; ++r) {
+        const int e = tid + r * NT;
+        if (e < NW) s.q[tt][sq[r]] = (sok[r] && tt < ntg) ? (float)(s.stage[b & 1][tt][e] * s.rinv[e]) : 0.0f;
+      }
+    __syncthreads();
+    // the next batch's window streams in during this batch's work (its buffer was last
+    // read by the previous batch's update, which every thread has finished here)
+    if (t0 + TB < ntr) issue(t0 + TB, (b + 1) & 1);
     // ---- (B) gradient and Qout of the ring cells
     if (in_arr) {
       if (bs >= 0) {  // region-boundary cell or halo cell: the FP64 boundary values
@@ -564,10 +602,10 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst 
 #pragma unroll
         for (int tt = 0; tt < TB; ++tt) {
           s.u.t.gq[tt][0][tid] = s.u.t.gq[tt][1][tid] = s.u.t.gq[tt][2][tid] = 0.0f;
-          s.u.t.gq[tt][3][tid] = s.u.t.gq[tt][4][tid] = s.q[tt][ec];
+          s.u.t.gq[tt][3][tid] = s.u.t.gq[tt][4][tid] = s.q[tt][eq];
         }
       } else {
-        const int st7[7] = {ec, ec + 1, ec + WW + 1, ec + WW, ec - 1, ec - WW - 1, ec - WW};
+        const int st7[7] = {eq, eq + 1, eq + QW + 1, eq + QW, eq - 1, eq - QW - 1, eq - QW};
 #pragma unroll
         for (int tt = 0; tt < TB; ++tt) {
           float qs[7];
@@ -580,16 +618,18 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst 
 #pragma unroll
             for (int n = 1; n < 7; ++n) g[c] = g[c] + cgr[c * 7 + n] * qs[n];
           }
-          // 4-point bounds of the 6 faces: the cell and three consecutive neighbours
-          // (owner q first, as mod_src_tracer.f90:152-214)
+          // 4-point bounds of the 6 faces (mod_src_tracer.f90:152-214)
           const float c0 = qs[0], n1 = qs[1], n2 = qs[2], n3 = qs[3], n4 = qs[4], n5 = qs[5], n6 = qs[6];
+          // face m: the cell and the neighbours m-1, m, m+1 (cyclic, n0 = n6)
           float lo[7], hi[7];
-          lo[1] = mn32(mn32(mn32(c0, n6), n1), n2), hi[1] = mx32(mx32(mx32(c0, n6), n1), n2);
-          lo[2] = mn32(mn32(mn32(c0, n1), n2), n3), hi[2] = mx32(mx32(mx32(c0, n1), n2), n3);
-          lo[3] = mn32(mn32(mn32(c0, n2), n3), n4), hi[3] = mx32(mx32(mx32(c0, n2), n3), n4);
-          lo[4] = mn32(mn32(mn32(n4, n5), c0), n3), hi[4] = mx32(mx32(mx32(n4, n5), c0), n3);
-          lo[5] = mn32(mn32(mn32(n5, n6), c0), n4), hi[5] = mx32(mx32(mx32(n5, n6), c0), n4);
-          lo[6] = mn32(mn32(mn32(n6, n1), c0), n5), hi[6] = mx32(mx32(mx32(n6, n1), c0), n5);
+          const float l12 = mn32(n1, n2), l34 = mn32(n3, n4), l56 = mn32(n5, n6);
+          const float h12 = mx32(n1, n2), h34 = mx32(n3, n4), h56 = mx32(n5, n6);
+          lo[1] = mn32(c0, mn32(n6, l12)), hi[1] = mx32(c0, mx32(n6, h12));
+          lo[2] = mn32(c0, mn32(l12, n3)), hi[2] = mx32(c0, mx32(h12, n3));
+          lo[3] = mn32(c0, mn32(n2, l34)), hi[3] = mx32(c0, mx32(n2, h34));
+          lo[4] = mn32(c0, mn32(l34, n5)), hi[4] = mx32(c0, mx32(h34, n5));
+          lo[5] = mn32(c0, mn32(n4, l56)), hi[5] = mx32(c0, mx32(n4, h56));
+          lo[6] = mn32(c0, mn32(l56, n1)), hi[6] = mx32(c0, mx32(h56, n1));
           float qnmin = c0, qnmax = c0, CQmin = 0.0f, CQmax = 0.0f;
 #pragma unroll
           for (int m = 1; m <= 6; ++m) {
@@ -612,7 +652,7 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst 
     // ---- (C) limited values of the faces owned by ring cells x, y in [-1, T-1]
     if (owner) {
       const int nbt[3] = {tid + 1, tid + RW + 1, tid + RW};  // ring thread of the neighbour
-      const int nbs[3] = {ec + 1, ec + WW + 1, ec + WW};       // window slot of the neighbour
+      const int nbs[3] = {eq + 1, eq + QW + 1, eq + QW};       // q slot of the neighbour
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const int ni = (a < 2) ? ci + 1 : ci, nj = (a > 0) ? cj + 1 : cj;
@@ -633,18 +673,18 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst 
           continue;
         }
         const bool cmu = (cmown >> a) & 1u;  // 1: the neighbour is upwind
-        const int ut = cmu ? nbt[a] : tid, us = cmu ? nbs[a] : ec;
+        const int ut = cmu ? nbt[a] : tid, us = cmu ? nbs[a] : eq;
 #pragma unroll
         for (int tt = 0; tt < TB; ++tt) {
           float v = s.q[tt][us];
           v = v + s.u.t.gq[tt][0][ut] * dup[a][0];
           v = v + s.u.t.gq[tt][1][ut] * dup[a][1];
           v = v + s.u.t.gq[tt][2][ut] * dup[a][2];
-          const float c0 = s.q[tt][ec];
+          const float c0 = s.q[tt][eq];
           float b1, b2, b3;
-          if (a == 0) b1 = s.q[tt][ec - WW], b2 = s.q[tt][ec + 1], b3 = s.q[tt][ec + WW + 1];
-          else if (a == 1) b1 = s.q[tt][ec + 1], b2 = s.q[tt][ec + WW + 1], b3 = s.q[tt][ec + WW];
-          else b1 = s.q[tt][ec + WW + 1], b2 = s.q[tt][ec + WW], b3 = s.q[tt][ec - 1];
+          if (a == 0) b1 = s.q[tt][eq - QW], b2 = s.q[tt][eq + 1], b3 = s.q[tt][eq + QW + 1];
+          else if (a == 1) b1 = s.q[tt][eq + 1], b2 = s.q[tt][eq + QW + 1], b3 = s.q[tt][eq + QW];
+          else b1 = s.q[tt][eq + QW + 1], b2 = s.q[tt][eq + QW], b3 = s.q[tt][eq - 1];
           const float lo = mn32(mn32(mn32(c0, b1), b2), b3), hi = mx32(mx32(mx32(c0, b1), b2), b3);
           v = mn32(mx32(v, lo), hi);
           v = mx32(mn32(v, s.u.t.gq[tt][4][ut]), s.u.t.gq[tt][3][ut]);
@@ -659,108 +699,154 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(FastInst 
       for (int tt = 0; tt < TB; ++tt) {
         if (tt >= ntg) break;
         const size_t o = (size_t)(t0 + tt) * tstride + base + ccell;
+        const double Qin = s.stage[b & 1][tt][ec];
         const float qa[7] = {0.0f, s.u.t.qa[tt][0][tid], s.u.t.qa[tt][1][tid], s.u.t.qa[tt][2][tid],
                              s.u.t.qa[tt][0][tid - 1], s.u.t.qa[tt][1][tid - RW - 1], s.u.t.qa[tt][2][tid - RW]};
         double sum = flx[1] * (double)qa[1];
 #pragma unroll
         for (int m = 2; m <= 6; ++m) sum = sum + flx[m] * (double)qa[m];
-        I.Q_out[o] = I.Q_in[o] - sum;
+        I.Q_out[o] = Qin - sum;
       }
     }
   }
 }
 
-// ---- vertical sub-step: one thread per (interior column, tracer), streaming the levels
-// with the limiter two levels behind; FP32 limiter, FP64 update.  rhogq after the
-// horizontal sub-step is read from (and the result written to) Q_out; tracer 0's threads
-// also finish rhog.  blockIdx.x = tracer, so the tracers of a column block run together
-// and share the per-level inputs (vco) in L2.
+// ---- vertical sub-step: one thread per (interior column, TV tracers), streaming the
+// levels with the limiter two levels behind and the next level's loads in flight; FP32
+// limiter, FP64 update.  rhogq after the horizontal sub-step is read from (and the result
+// written to) Q_out; the threads of the first tracer group also finish rhog.
+// blockIdx.x = tracer group, so the groups of a column block run together and share the
+// per-level inputs (vco) in L2.
+template <int TV>
 __global__ void __launch_bounds__(256) k_fast_vert(FastInst I) {
-  const int t = blockIdx.x;
+  const int t0 = blockIdx.x * TV;
+  const int ntv = min(TV, I.ntr - t0);
   const int n = I.gmax - I.gmin + 1;
   const long long col = (long long)blockIdx.y * blockDim.x + threadIdx.x;
   if (col >= (long long)I.lall * n * n) return;
   const int l = (int)(col / ((long long)n * n)), r = (int)(col % ((long long)n * n));
   const int i = I.gmin + r % n, j = I.gmin + r / n;
   const int K = I.K;
-  const size_t slab = (size_t)I.gall;
+  const size_t slab = (size_t)I.gall, tstride = (size_t)I.lall * K * slab;
   const size_t cbase = (size_t)l * K * slab + (size_t)(j - 1) * I.G + (i - 1);
-  double *Q = I.Q_out + (size_t)t * I.lall * K * slab + cbase;
+  double *Q = I.Q_out + (size_t)t0 * tstride + cbase;
   double *R = I.rho_out + cbase;
   const float4 *V = I.vco + cbase;
-  const bool dens = t == 0;
+  const bool dens = t0 == 0;
   const double dt = I.dt;
   float ck1w[3] = {0.0f, 0.0f, 0.0f}, ck2w[3] = {0.0f, 0.0f, 0.0f}, wf[3] = {0.0f, 0.0f, 0.0f};
-  double Qh[3] = {0.0, 0.0, 0.0}, rh[3] = {0.0, 0.0, 0.0};
-  float qv[3] = {0.0f, 0.0f, 0.0f};
-  float qmn_km1 = 0.0f, qmx_km1 = 0.0f, qh_last = 0.0f;
+  double rh[3] = {0.0, 0.0, 0.0};
+  double Qh[TV][3];
+  float qv[TV][3], qmn_km1[TV], qmx_km1[TV], qh_last[TV];
+  double qnext[TV];
+#pragma unroll
+  for (int tt = 0; tt < TV; ++tt) {
+    Qh[tt][0] = Qh[tt][1] = Qh[tt][2] = 0.0;
+    qv[tt][0] = qv[tt][1] = qv[tt][2] = 0.0f;
+    qmn_km1[tt] = qmx_km1[tt] = qh_last[tt] = 0.0f;
+    qnext[tt] = (tt < ntv) ? Q[tt * tstride + slab] : 0.0;
+  }
+  float4 cnext = V[slab];
+  double rnext = dens ? R[slab] : 0.0;
   for (int k = 1; k <= K - 2; ++k) {
-    const float4 c = V[(size_t)k * slab];
+    const float4 c = cnext;
+    double Qk[TV];
+#pragma unroll
+    for (int tt = 0; tt < TV; ++tt) Qk[tt] = qnext[tt];
+    const double rk = rnext;
+    if (k + 1 <= K - 2) {  // the next level's loads, in flight during this level's work
+      const size_t o = (size_t)(k + 1) * slab;
+      cnext = V[o];
+#pragma unroll
+      for (int tt = 0; tt < TV; ++tt)
+        if (tt < ntv) qnext[tt] = Q[tt * tstride + o];
+      if (dens) rnext = R[o];
+    }
     ck1w[0] = ck1w[1], ck1w[1] = ck1w[2], ck1w[2] = c.x;
     ck2w[0] = ck2w[1], ck2w[1] = ck2w[2], ck2w[2] = c.y;
     wf[0] = wf[1], wf[1] = wf[2], wf[2] = c.w;
-    const double Qhk = Q[(size_t)k * slab];
-    Qh[0] = Qh[1], Qh[1] = Qh[2], Qh[2] = Qhk;
-    qv[0] = qv[1], qv[1] = qv[2], qv[2] = (float)(Qhk * (double)c.z);
-    if (dens) rh[0] = rh[1], rh[1] = rh[2], rh[2] = R[(size_t)k * slab];
+    rh[0] = rh[1], rh[1] = rh[2], rh[2] = rk;
     if (k == 1) {  // ghost level below: q(kmin-1) = q(kmin)
-      qv[1] = qv[2];
-      qh_last = 0.0f;
+#pragma unroll
+      for (int tt = 0; tt < TV; ++tt) {
+        Qh[tt][2] = Qk[tt];
+        qv[tt][1] = qv[tt][2] = (float)(Qk[tt] * (double)c.z);
+        qh_last[tt] = 0.0f;
+      }
       continue;
     }
     // Qout of level k-1 from q at k-2, k-1, k; the face k-1 between levels k-2 and k-1
     const VLim vp = vlim_params(ck1w[1], ck2w[1], ck1w[2]);
-    float Qmin, Qmax;
-    vlim_qout(vp, qv[0], qv[1], qv[2], Qmin, Qmax);
     const int f = k - 1;
-    float qh = (float)I.afact[f] * qv[1] + (float)I.bfact[f] * qv[0];
-    if (f >= 2) qh = vp.infl * mx32(mn32(qh, qmx_km1), qmn_km1) + (1.0f - vp.infl) * mx32(mn32(qh, Qmax), Qmin);
-    if (k - 2 >= 1) {  // level k-2 is final once faces k-2 and k-1 are
-      const int L = k - 2;
-      const double fu = (double)wf[1] * (double)qh, fl = (double)wf[0] * (double)qh_last;
-      const double Qn = Qh[0] - (fu - fl) * dt * I.rdgz[L];
-      Q[(size_t)L * slab] = Qn;
-      if (L == 1) Q[0] = Qn;
-      if (dens) {
-        const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dt * I.rdgz[L];
-        R[(size_t)L * slab] = rn;
-        if (L == 1) R[0] = rn;
+    const float af = (float)I.afact[f], bf = (float)I.bfact[f];
+    const double rdz = I.rdgz[k - 2];
+#pragma unroll
+    for (int tt = 0; tt < TV; ++tt) {
+      if (tt >= ntv) break;
+      Qh[tt][0] = Qh[tt][1], Qh[tt][1] = Qh[tt][2], Qh[tt][2] = Qk[tt];
+      qv[tt][0] = qv[tt][1], qv[tt][1] = qv[tt][2], qv[tt][2] = (float)(Qk[tt] * (double)c.z);
+      float Qmin, Qmax;
+      vlim_qout(vp, qv[tt][0], qv[tt][1], qv[tt][2], Qmin, Qmax);
+      float qh = af * qv[tt][1] + bf * qv[tt][0];
+      if (f >= 2)
+        qh = vp.infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - vp.infl) * mx32(mn32(qh, Qmax), Qmin);
+      if (k - 2 >= 1) {  // level k-2 is final once faces k-2 and k-1 are
+        const int L = k - 2;
+        const double fu = (double)wf[1] * (double)qh, fl = (double)wf[0] * (double)qh_last[tt];
+        const double Qn = Qh[tt][0] - (fu - fl) * dt * rdz;
+        Q[tt * tstride + (size_t)L * slab] = Qn;
+        if (L == 1) Q[tt * tstride] = Qn;
       }
+      qh_last[tt] = qh;
+      qmn_km1[tt] = Qmin;
+      qmx_km1[tt] = Qmax;
     }
-    qh_last = qh;
-    qmn_km1 = Qmin;
-    qmx_km1 = Qmax;
+    if (dens && k - 2 >= 1) {
+      const int L = k - 2;
+      const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dt * rdz;
+      R[(size_t)L * slab] = rn;
+      if (L == 1) R[0] = rn;
+    }
   }
   // ---- drain: levels K-3 and K-2 (faces K-2 and K-1); ghost level above: q(kmax+1) = q(kmax)
   const int kk = K - 1;
   const float wk1 = I.w[cbase + (size_t)kk * slab];
   const float c1top = (float)(-(double)wk1 * dt * I.rdgz[kk] / I.rho_in[cbase + (size_t)kk * slab]);
   const VLim vd = vlim_params(ck1w[2], ck2w[2], c1top);  // level K-2 with q(K-1) := q(K-2)
-  float Qmin, Qmax;
-  vlim_qout(vd, qv[1], qv[2], qv[2], Qmin, Qmax);
   const int f = K - 2;
-  float qh = (float)I.afact[f] * qv[2] + (float)I.bfact[f] * qv[1];
-  if (f >= 2) qh = vd.infl * mx32(mn32(qh, qmx_km1), qmn_km1) + (1.0f - vd.infl) * mx32(mn32(qh, Qmax), Qmin);
-  if (K - 3 >= 1) {
-    const int L = K - 3;
-    const double fu = (double)wf[2] * (double)qh, fl = (double)wf[1] * (double)qh_last;
-    const double Qn = Qh[1] - (fu - fl) * dt * I.rdgz[L];
-    Q[(size_t)L * slab] = Qn;
-    if (L == 1) Q[0] = Qn;
-    if (dens) {
+  const float af = (float)I.afact[f], bf = (float)I.bfact[f];
+  const float ak = (float)I.afact[kk], bk = (float)I.bfact[kk];
+#pragma unroll
+  for (int tt = 0; tt < TV; ++tt) {
+    if (tt >= ntv) break;
+    float Qmin, Qmax;
+    vlim_qout(vd, qv[tt][1], qv[tt][2], qv[tt][2], Qmin, Qmax);
+    float qh = af * qv[tt][2] + bf * qv[tt][1];
+    if (f >= 2)
+      qh = vd.infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - vd.infl) * mx32(mn32(qh, Qmax), Qmin);
+    double *Qt = Q + tt * tstride;
+    if (K - 3 >= 1) {
+      const int L = K - 3;
+      const double fu = (double)wf[2] * (double)qh, fl = (double)wf[1] * (double)qh_last[tt];
+      const double Qn = Qh[tt][1] - (fu - fl) * dt * I.rdgz[L];
+      Qt[(size_t)L * slab] = Qn;
+      if (L == 1) Qt[0] = Qn;
+    }
+    // top face K-1: unlimited
+    const float qtop = ak * qv[tt][2] + bk * qv[tt][2];
+    const double fu = (double)wk1 * (double)qtop, fl = (double)wf[2] * (double)qh;
+    const double Qn = Qh[tt][2] - (fu - fl) * dt * I.rdgz[K - 2];
+    Qt[(size_t)(K - 2) * slab] = Qn;
+    Qt[(size_t)(K - 1) * slab] = Qn;
+    if (K - 2 == 1) Qt[0] = Qn;
+  }
+  if (dens) {
+    if (K - 3 >= 1) {
+      const int L = K - 3;
       const double rn = rh[1] - ((double)wf[2] - (double)wf[1]) * dt * I.rdgz[L];
       R[(size_t)L * slab] = rn;
       if (L == 1) R[0] = rn;
     }
-  }
-  // top face K-1: unlimited
-  const float qtop = (float)I.afact[kk] * qv[2] + (float)I.bfact[kk] * qv[2];
-  const double fu = (double)wk1 * (double)qtop, fl = (double)wf[2] * (double)qh;
-  const double Qn = Qh[2] - (fu - fl) * dt * I.rdgz[K - 2];
-  Q[(size_t)(K - 2) * slab] = Qn;
-  Q[(size_t)(K - 1) * slab] = Qn;
-  if (K - 2 == 1) Q[0] = Qn;
-  if (dens) {
     const double rn = rh[2] - ((double)wk1 - (double)wf[2]) * dt * I.rdgz[K - 2];
     R[(size_t)(K - 2) * slab] = rn;
     R[(size_t)(K - 1) * slab] = rn;
@@ -929,7 +1015,8 @@ cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t
   if (e != cudaSuccess) return e;
   const int n = I.gmax - I.gmin + 1;
   const long long ncol = (long long)I.lall * n * n;
-  k_fast_vert<<<dim3((unsigned)I.ntr, (unsigned)((ncol + 255) / 256)), 256, 0, st>>>(I);
+  constexpr int TV = 4;
+  k_fast_vert<TV><<<dim3((unsigned)((I.ntr + TV - 1) / TV), (unsigned)((ncol + 255) / 256)), 256, 0, st>>>(I);
   const long long nc = (long long)I.ncarry * I.K;
   k_fast_carry<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(I);
   launches += 6;
