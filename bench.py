@@ -45,6 +45,18 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def measured_traffic(kernel, shape, updates):
+    """DRAM bytes per launch of `kernel` from the committed ncu figure (profiles/dram_traffic.json),
+    scaled by the updates per launch; None when no capture of this kernel and tile shape exists."""
+    p = ROOT / "profiles" / "dram_traffic.json"
+    if not p.exists():
+        return None, None
+    d = json.loads(p.read_text()).get(kernel)
+    if not d or list(d["tile_txtytg"]) != list(shape):
+        return None, None
+    return d["bytes_per_update"] * updates, "ncu " + d["capture"] + ", scaled by updates"
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
 
@@ -233,9 +245,13 @@ def run_ours(args, world, rank, local):
         kern = runner.kernel_stats()
     if kern:  # dominant kernel timed with its own events inside the step loop
         achieved = kern["bytes_per_launch"] / (kern["ms_per_launch"] * 1e-3) / 1e9
+        shape = list(ctx.fast_shapes()[runner.shape])
+        traffic, tsrc = args.traffic, None
+        if traffic is None:
+            traffic, tsrc = measured_traffic(kern["name"], shape, upd)
         roof = {"bound": "hbm", "kernel": kern["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": args.traffic,
-                "alg_bytes_per_update": b_alg}
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic, "traffic_source": tsrc,
+                "alg_bytes_per_update": runner.alg_bytes}
     else:
         achieved = upd * b_alg / (ms * 1e-3) / 1e9
         roof = {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": peak, "unit": "GB/s",
