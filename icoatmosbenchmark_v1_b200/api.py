@@ -371,3 +371,109 @@ class FastRunner:
             return None
         return {"name": "k_fast_horiz", "ms_per_launch": ms / n, "launches": n,
                 "bytes_per_launch": self.updates * self.alg_bytes}
+
+
+# ---- batches of grid instances (uneven grid levels) ------------------------------
+class FastArgs(C.Structure):
+    """ica_fast_args: one instance's step arguments (device pointers)."""
+    _fields_ = [("ntr", C.c_int), ("dt", C.c_double)] + [
+        (n, C.c_void_p) for n in ("rhog_in", "rhog_in_pl", "rhogq_in", "rhogq_in_pl", "rhog_out", "rhog_out_pl",
+                                  "rhogq_out", "rhogq_out_pl") + FIELD_KEYS]
+
+
+def _fast_args(dt, state_in, state_out, fields32):
+    a = FastArgs()
+    a.ntr, a.dt = int(state_in["rhogq"].shape[0]), float(dt)
+    for k, kin, kout in (("rhog", "rhog_in", "rhog_out"), ("rhog_pl", "rhog_in_pl", "rhog_out_pl"),
+                         ("rhogq", "rhogq_in", "rhogq_out"), ("rhogq_pl", "rhogq_in_pl", "rhogq_out_pl")):
+        setattr(a, kin, state_in[k].data_ptr())
+        setattr(a, kout, state_out[k].data_ptr())
+    for k in FIELD_KEYS:
+        setattr(a, k, fields32[k].data_ptr())
+    return a
+
+
+class Batch:
+    """Several grid instances (each an IcoAdv context with its geometry) advanced by the same
+    launches (ica_batch_*): one launch per stage over all instances, the horizontal kernel
+    persistent; a step can be captured in a CUDA graph and replayed."""
+
+    def __init__(self, ctxs):
+        self.ctxs = list(ctxs)
+        self.h = C.c_void_p()
+        arr = (C.c_void_p * len(self.ctxs))(*[c.h.value for c in self.ctxs])
+        _check("ica_batch_create", lib().ica_batch_create(arr, len(self.ctxs), C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().ica_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_shape(self, shape):
+        _check("ica_batch_set_shape", lib().ica_batch_set_shape(self.h, int(shape)))
+
+    def _args(self, args):
+        return (FastArgs * len(args))(*args)
+
+    def step(self, args):
+        with self.ctxs[0]._ordered():
+            _check("ica_batch_step_dev", lib().ica_batch_step_dev(self.h, self._args(args)))
+
+    def capture(self, args, slot):
+        _check("ica_batch_capture", lib().ica_batch_capture(self.h, self._args(args), int(slot)))
+
+    def replay(self, slot):
+        with self.ctxs[0]._ordered():
+            _check("ica_batch_replay", lib().ica_batch_replay(self.h, int(slot)))
+
+
+class BatchRunner:
+    """Device-resident loop over a batch of instances: per instance a double-buffered FP64
+    state and FP32 fields; step() launches directly, or, after use_graph(), replays the
+    captured CUDA graph of the current direction."""
+
+    def __init__(self, ctxs, states, fields, dts, shape=0):
+        import torch
+        self.batch = Batch(ctxs)
+        self.batch.set_shape(shape)
+        self.a = list(states)
+        self.b = [{k: torch.empty_like(v) for k, v in s.items()} for s in states]
+        self.f32 = [{k: f[k].to(torch.float32).contiguous() for k in FIELD_KEYS} for f in fields]
+        self.dts = list(dts)
+        self.graphs = False
+        self.parity = 0  # 0: a -> b next, 1: b -> a next
+        # tracer cell-level updates per step: columns (10 * 4^glevel + 2) x kall x tracers
+        self.updates = sum((10 * 4 ** c.glevel + 2) * int(s["rhogq"].shape[2]) * int(s["rhogq"].shape[0])
+                           for c, s in zip(ctxs, states))
+
+    def _argsets(self):
+        fwd = [_fast_args(dt, a, b, f) for dt, a, b, f in zip(self.dts, self.a, self.b, self.f32)]
+        bwd = [_fast_args(dt, b, a, f) for dt, a, b, f in zip(self.dts, self.a, self.b, self.f32)]
+        return fwd, bwd
+
+    @property
+    def states(self):
+        return self.a if self.parity == 0 else self.b
+
+    def step(self):
+        if self.graphs:
+            self.batch.replay(self.parity)
+        else:
+            self.batch.step(self._argsets()[self.parity])
+        self.parity ^= 1
+
+    def use_graph(self):
+        """Capture both directions (after one uncaptured step has set up every buffer)."""
+        fwd, bwd = self._argsets()
+        self.batch.capture(fwd, 0)
+        self.batch.capture(bwd, 1)
+        self.graphs = True
+
+    def close(self):
+        self.batch.close()

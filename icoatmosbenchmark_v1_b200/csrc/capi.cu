@@ -732,6 +732,8 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
   if (!I.sflux || !I.sval) return set_error("cudaMalloc(fast seam buffers)"), ICA_ERR_NOMEM;
   I.vco = (float4 *)buf("fast_vco", (size_t)sz.lall * sz.kall * sz.gall * sizeof(float4));
   if (!I.vco) return set_error("cudaMalloc(fast vertical coefficients)"), ICA_ERR_NOMEM;
+  I.work_next = (unsigned long long *)buf("fast_work_next", sizeof(unsigned long long));
+  if (!I.work_next) return set_error("cudaMalloc(fast work counter)"), ICA_ERR_NOMEM;
   return ICA_OK;
 }
 
@@ -805,6 +807,140 @@ int ica_advect_fast_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, c
   launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, ntr, rhogq_out, rhogq_out_pl, c->stream);
   c->launches += 2;
   return c->check_launch("ica_advect_fast");
+}
+
+}  // extern "C"
+
+struct ica_batch {
+  std::vector<Ctx *> ctx;
+  int shape = 0;
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+};
+
+namespace icoadv {
+
+static int fast_args_ok(const ica_fast_args &a) {
+  return a.ntr >= 1 && a.rhog_in && a.rhog_in_pl && a.rhogq_in && a.rhogq_in_pl && a.rhog_out && a.rhog_out_pl &&
+         a.rhogq_out && a.rhogq_out_pl && a.rhogvx && a.rhogvx_pl && a.rhogvy && a.rhogvy_pl && a.rhogvz &&
+         a.rhogvz_pl && a.rhogw && a.rhogw_pl && a.rhogq_in != a.rhogq_out && a.rhog_in != a.rhog_out;
+}
+
+// instance table of a batch step (device buffers of every instance set up here)
+static int batch_insts(ica_batch *b, const ica_fast_args *args, MultiInst &M) {
+  M.n = (int)b->ctx.size();
+  for (int i = 0; i < M.n; ++i) {
+    Ctx *c = b->ctx[i];
+    const ica_fast_args &a = args[i];
+    if (!fast_args_ok(a)) return set_error("ica_batch: bad arguments of instance " + std::to_string(i)), ICA_ERR_ARG;
+    c->fast.shape = b->shape;
+    FastInst &I = M.inst[i];
+    const int rc = c->fast_inst(I, a.ntr, a.dt);
+    if (rc) return rc;
+    I.vx = a.rhogvx, I.vy = a.rhogvy, I.vz = a.rhogvz, I.w = a.rhogw;
+    I.vx_pl = a.rhogvx_pl, I.vy_pl = a.rhogvy_pl, I.vz_pl = a.rhogvz_pl, I.w_pl = a.rhogw_pl;
+    I.rho_in = a.rhog_in, I.rho_in_pl = a.rhog_in_pl, I.Q_in = a.rhogq_in, I.Q_in_pl = a.rhogq_in_pl;
+    I.rho_out = a.rhog_out, I.rho_out_pl = a.rhog_out_pl, I.Q_out = a.rhogq_out, I.Q_out_pl = a.rhogq_out_pl;
+  }
+  return ICA_OK;
+}
+
+static int batch_enqueue(ica_batch *b, const MultiInst &M, const ica_fast_args *args) {
+  Ctx *c0 = b->ctx[0];
+  long long launches = 0;
+  cudaError_t e = fast_step_multi(M, b->shape, c0->stream, nullptr, nullptr, launches);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_batch step");
+  for (int i = 0; i < M.n; ++i) {
+    Ctx *c = b->ctx[i];
+    const Plan &p = c->plan[0];
+    launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, 1, args[i].rhog_out, args[i].rhog_out_pl, c0->stream);
+    launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, args[i].ntr, args[i].rhogq_out, args[i].rhogq_out_pl,
+                          c0->stream);
+    launches += 2;
+  }
+  c0->launches += launches;
+  return c0->check_launch("ica_batch step");
+}
+
+}  // namespace icoadv
+
+extern "C" {
+
+int ica_batch_create(ica_ctx *const *ctxs, int n, ica_batch **out) {
+  if (!ctxs || !out || n < 1 || n > ICA_BATCH_MAX) return set_error("ica_batch_create: bad arguments"), ICA_ERR_ARG;
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i]) return set_error("ica_batch_create: NULL context"), ICA_ERR_ARG;
+    if (ctxs[i]->device != ctxs[0]->device)
+      return set_error("ica_batch_create: instances on different devices"), ICA_ERR_ARG;
+  }
+  ica_batch *b = new ica_batch;
+  for (int i = 0; i < n; ++i) b->ctx.push_back(ctxs[i]);
+  *out = b;
+  return ICA_OK;
+}
+
+int ica_batch_destroy(ica_batch *b) {
+  if (!b) return ICA_ERR_ARG;
+  cudaSetDevice(b->ctx[0]->device);
+  for (int s = 0; s < 2; ++s) {
+    if (b->exec[s]) cudaGraphExecDestroy(b->exec[s]);
+    if (b->graph[s]) cudaGraphDestroy(b->graph[s]);
+  }
+  delete b;
+  return ICA_OK;
+}
+
+int ica_batch_set_shape(ica_batch *b, int shape) {
+  if (!b) return ICA_ERR_ARG;
+  if (shape < 0 || shape >= fast_tile_shapes(nullptr, nullptr, nullptr, 0))
+    return set_error("ica_batch_set_shape: no such tile shape"), ICA_ERR_ARG;
+  b->shape = shape;
+  return ICA_OK;
+}
+
+int ica_batch_step_dev(ica_batch *b, const ica_fast_args *args) {
+  if (!b || !args) return set_error("ica_batch_step_dev: NULL argument"), ICA_ERR_ARG;
+  cudaSetDevice(b->ctx[0]->device);
+  MultiInst M;
+  int rc = batch_insts(b, args, M);
+  if (rc) return rc;
+  return batch_enqueue(b, M, args);
+}
+
+int ica_batch_capture(ica_batch *b, const ica_fast_args *args, int slot) {
+  if (!b || !args || slot < 0 || slot > 1) return set_error("ica_batch_capture: bad arguments"), ICA_ERR_ARG;
+  cudaSetDevice(b->ctx[0]->device);
+  MultiInst M;
+  int rc = batch_insts(b, args, M);  // every buffer exists before the capture starts
+  if (rc) return rc;
+  cudaStream_t st = b->ctx[0]->stream;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_batch_capture");
+  e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+  rc = batch_enqueue(b, M, args);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(st, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  if (b->exec[slot]) cudaGraphExecDestroy(b->exec[slot]);
+  if (b->graph[slot]) cudaGraphDestroy(b->graph[slot]);
+  b->graph[slot] = g;
+  b->exec[slot] = nullptr;
+  e = cudaGraphInstantiate(&b->exec[slot], g, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  return ICA_OK;
+}
+
+int ica_batch_replay(ica_batch *b, int slot) {
+  if (!b || slot < 0 || slot > 1 || !b->exec[slot]) return set_error("ica_batch_replay: no graph in slot"), ICA_ERR_STATE;
+  cudaSetDevice(b->ctx[0]->device);
+  cudaError_t e = cudaGraphLaunch(b->exec[slot], b->ctx[0]->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+  return ICA_OK;
 }
 
 int ica_advect_fast(ica_ctx *c, int ntr, double dt, double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,

@@ -40,7 +40,28 @@ struct FastInst {
   float *sval;    // (ntr, K, ns): limited face values of the seam faces
   double *bbuf;  // (ntr, K, nb, 5): grad x, y, z, Qout min, Qout max
   float4 *vco;   // (lall, K, gall): ck(k,1), ck(k,2), 1/rhog, rhogw(k) after the horizontal sub-step
+  unsigned long long *work_next;  // work-item counter of the persistent horizontal kernel
 };
+
+// Up to kMaxInst grid instances advanced by the same launches (batches of uneven grid
+// levels); passed by value as a __grid_constant__ kernel parameter.
+constexpr int kMaxInst = 4;
+struct MultiInst {
+  int n;
+  FastInst inst[kMaxInst];
+};
+
+// Instance of flat work item w, given the number of work items cnt(inst) of each
+// instance; w becomes the index within that instance.  -1 when w is past the end.
+template <class F>
+__device__ __forceinline__ int find_inst(const MultiInst &M, long long &w, F cnt) {
+  for (int i = 0; i < M.n; ++i) {
+    const long long c = cnt(M.inst[i]);
+    if (w < c) return i;
+    w -= c;
+  }
+  return -1;
+}
 
 __device__ __forceinline__ double fsg(double a, double b) { return copysign(fabs(a), b); }
 __device__ __forceinline__ double mn64(double a, double b) { return (b < a) ? b : a; }

@@ -16,5 +16,11 @@ cudaError_t fast_build_offsets(const FastInst &I, float *off, cudaStream_t st);
 // (optional) are recorded around k_fast_horiz, the dominant launch.
 cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
                       long long &launches);
+// The same step for M.n grid instances (uneven grid levels) together: each kernel is one
+// launch over the work of every instance; the horizontal kernel is persistent (one wave of
+// CTAs striding over all (instance, level, tile) items).  Launches nothing that allocates,
+// so it can be captured in a CUDA graph once every instance has run one step uncaptured.
+cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
+                            long long &launches);
 
 }  // namespace icoadv

@@ -271,6 +271,34 @@ int ica_fast_set_shape(ica_ctx *ctx, int shape);
  * disables (0) recording for the following calls.  Synchronises the stream. */
 int ica_fast_timing(ica_ctx *ctx, int enable, double *ms_total, long long *count);
 
+/* ---- Batches: up to ICA_BATCH_MAX grid instances (for example uneven grid levels, each
+ * with its own context, geometry and tracer count) advanced by the same launches: every
+ * stage of ica_advect_fast_dev is one launch over the work of all instances, the horizontal
+ * kernel persistent (one wave of CTAs striding over (instance, level, tile) items).  The
+ * work runs on the first context's stream.  A step can be captured into a CUDA graph
+ * (two slots, for the two directions of a double-buffered state) and replayed; capture
+ * only after one uncaptured ica_batch_step_dev with the same arguments has set up every
+ * instance's device buffers.  Instances must live on the same device. */
+#define ICA_BATCH_MAX 4
+typedef struct ica_batch ica_batch;
+typedef struct {
+  int ntr;
+  double dt;
+  const double *rhog_in, *rhog_in_pl, *rhogq_in, *rhogq_in_pl;
+  double *rhog_out, *rhog_out_pl, *rhogq_out, *rhogq_out_pl;
+  const float *rhogvx, *rhogvx_pl, *rhogvy, *rhogvy_pl, *rhogvz, *rhogvz_pl, *rhogw, *rhogw_pl;
+} ica_fast_args;
+int ica_batch_create(ica_ctx *const *ctxs, int n, ica_batch **out);
+int ica_batch_destroy(ica_batch *b);
+/* Tile shape (index into ica_fast_shapes) used for every instance of the batch. */
+int ica_batch_set_shape(ica_batch *b, int shape);
+/* One step of every instance (args[i] for instance i), device pointers, asynchronous. */
+int ica_batch_step_dev(ica_batch *b, const ica_fast_args *args);
+/* Capture the step with these arguments into graph slot 0 or 1 (replacing what was there). */
+int ica_batch_capture(ica_batch *b, const ica_fast_args *args, int slot);
+/* Launch the graph in slot 0 or 1 on the batch stream. */
+int ica_batch_replay(ica_batch *b, int slot);
+
 /* ---- Host-only topology helpers (no GPU needed).
  * Point index of region cell (i,j) of region r (all 1-based):
  *   (r-1)*gall + (j-1)*gall_1d + (i-1);  pole p (0 north, 1 south), slot v:
