@@ -214,6 +214,18 @@ def run_ours(args, world, rank, local):
         dtype = "f32"
         s_bytes = 48
 
+    err = m0 = None
+    if args.mode != "plain" and not args.no_check:
+        # one FP64 plain-path step on a copy: the reference of the batched step's first step
+        ref = {k: v.clone() for k, v in runner.state.items()}
+        ctx.advect_step(dt, ref["rhog"], ref["rhog_pl"], ref["rhogq"], ref["rhogq_pl"], f["rhogvx"], f["rhogvx_pl"],
+                        f["rhogvy"], f["rhogvy_pl"], f["rhogvz"], f["rhogvz_pl"], f["rhogw"], f["rhogw_pl"])
+        m0 = tracer_mass(g, runner.state)
+        step()
+        torch.cuda.synchronize()
+        err = float(((runner.state["rhogq"] - ref["rhogq"]).abs().max() / ref["rhogq"].abs().max()).item())
+        del ref
+        torch.cuda.empty_cache()
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         step()
@@ -235,6 +247,10 @@ def run_ours(args, world, rank, local):
     barrier(world)
     clocks = sampler.stop()
     launches = ctx.launch_count - n0
+    drift = None
+    if m0 is not None:
+        m1 = tracer_mass(g, runner.state)
+        drift = float(((m1 - m0).abs() / m0.abs()).max().item())
     ms = e0.elapsed_time(e1) / args.steps
     ms = allreduce_max(ms, world)
     value = upd * world / (ms * 1e-3)
@@ -277,8 +293,125 @@ def run_ours(args, world, rank, local):
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": cfg,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+        if err is not None:
+            line["max_rel_err_vs_fp64"] = err  # first step vs the FP64 plain path (bit-exact to the oracle)
+            line["mass_drift"] = {"value": drift, "steps": 1 + args.warmup + args.steps}
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+UNEVEN = ((7, 96, 40), (6, 42, 12))  # (glevel, kall, tracers) of the two instances
+
+
+def tracer_mass(g, S):
+    """Global mass of every tracer (FP64): sum over interior cells and pole centres of
+    rhogq * area * dz over the physical levels."""
+    import torch
+    dev = S["rhogq"].device
+    m = torch.as_tensor(g.interior_mask(), device=dev)
+    kk = slice(g.kmin - 1, g.kmax)
+    area = torch.as_tensor(g.arrays["GMTR_p"][0], device=dev)
+    dz = torch.as_tensor(g.arrays["dz"], device=dev)
+    apl = torch.as_tensor(g.arrays["GMTR_p_pl"][0][:, 0], device=dev)
+    a = (S["rhogq"][:, :, kk] * (area * m)[None, :, None] * dz[kk][None, None, :, None]).sum((1, 2, 3))
+    return a + (S["rhogq_pl"][:, :, kk, 0] * apl[None, :, None] * dz[kk][None, None]).sum((1, 2))
+
+
+def run_uneven(args, world, rank, local):
+    """Batch of two uneven grid instances (glevel 7 / kall 96 / 40 tracers and glevel 6 / kall 42 /
+    12 tracers) advanced by the same launches and replayed from a CUDA graph (FP32 variant);
+    the FP64 variant is the plain per-tracer path of each instance.  Reports the FP32 variant's
+    max relative error against the FP64 path after one step and the relative mass drift over the
+    timed steps."""
+    import torch
+
+    from icoatmosbenchmark_v1_b200 import api
+    from icoatmosbenchmark_v1_b200 import fields as F
+    from icoatmosbenchmark_v1_b200.grid import Grid, default_dt
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    grids = [Grid(gl, 0, K) for gl, K, _ in UNEVEN]
+    fs, sts, ctxs, dts = [], [], [], []
+    for g, (gl, K, T) in zip(grids, UNEVEN):
+        f = F.make_fields(g, device=dev)
+        st = F.make_state(g, T, "mixed", device=dev, fields=f)
+        ctx = api.IcoAdv(gl, 0, K - 2, device=local)
+        ctx.set_grid(g)
+        fs.append(f), sts.append(st), ctxs.append(ctx), dts.append(default_dt(gl))
+    upd = sum((10 * 4 ** gl + 2) * K * T for gl, K, T in UNEVEN)
+
+    def masses(states):
+        return [tracer_mass(g, S) for g, S in zip(grids, states)]
+
+    # FP64 variant (plain path) for one step: the error reference, and its time (after a
+    # warm-up step on a copy, which sets up its buffers)
+    for ctx, st, f, dt in zip(ctxs, sts, fs, dts):
+        S = {k: v.clone() for k, v in st.items()}
+        ctx.advect_step(dt, S["rhog"], S["rhog_pl"], S["rhogq"], S["rhogq_pl"], f["rhogvx"], f["rhogvx_pl"],
+                        f["rhogvy"], f["rhogvy_pl"], f["rhogvz"], f["rhogvz_pl"], f["rhogw"], f["rhogw_pl"])
+        del S
+    ref = [{k: v.clone() for k, v in st.items()} for st in sts]
+    torch.cuda.synchronize()
+    t64 = time.perf_counter()
+    for ctx, S, f, dt in zip(ctxs, ref, fs, dts):
+        ctx.advect_step(dt, S["rhog"], S["rhog_pl"], S["rhogq"], S["rhogq_pl"], f["rhogvx"], f["rhogvx_pl"],
+                        f["rhogvy"], f["rhogvy_pl"], f["rhogvz"], f["rhogvz_pl"], f["rhogw"], f["rhogw_pl"])
+    torch.cuda.synchronize()
+    ms64 = (time.perf_counter() - t64) * 1e3
+    # tile shape: the fastest over two direct steps each
+    best, tuning = None, []
+    for shape in range(len(ctxs[0].fast_shapes())):
+        br = api.BatchRunner(ctxs, [{k: v.clone() for k, v in st.items()} for st in sts], fs, dts, shape=shape)
+        br.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        br.step(), br.step()
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 500.0
+        tuning.append(round(ms, 3))
+        if best is None or ms < best[1]:
+            best = (shape, ms)
+        br.close()
+        del br
+    br = api.BatchRunner(ctxs, sts, fs, dts, shape=best[0])
+    m0 = masses(br.states)
+    br.step()
+    torch.cuda.synchronize()
+    err = max(float(((a["rhogq"] - b["rhogq"]).abs().max() / b["rhogq"].abs().max()).item())
+              for a, b in zip(br.states, ref))
+    br.use_graph()
+    for _ in range(args.warmup):
+        br.step()
+    stream = torch.cuda.ExternalStream(ctxs[0].stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    sampler.start()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        br.step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    m1 = masses(br.states)
+    drift = max(float(((b - a).abs() / a.abs()).max().item()) for a, b in zip(m0, m1))
+    if rank == 0:
+        shape = list(ctxs[0].fast_shapes()[best[0]])
+        line = {"metric": METRIC, "value": upd / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "uneven_gl7_k96_t40+gl6_k42_t12", "instances": [list(x) for x in UNEVEN],
+                           "updates_per_step": upd, "launch": "one launch per stage over both instances, "
+                           "persistent horizontal kernel, step replayed from a CUDA graph",
+                           "tile": {"shape_txtytg": shape, "autotune_ms": tuning}},
+                "fp64_plain_ms_per_step": ms64, "max_rel_err_vs_fp64": err,
+                "mass_drift": {"value": drift, "steps": args.steps + args.warmup},
+                "gpu_launches": None, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    br.close()
+    for c in ctxs:
+        c.close()
 
 
 def measure_e2e(args, ctx, g, st, f, dt, upd, world):
@@ -321,7 +454,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["fast", "plain"], default="fast")
+    ap.add_argument("--mode", choices=["fast", "plain", "uneven"], default="fast",
+                    help="fast: batched step (headline); plain: FP64 per-tracer path; uneven: batch of two grid levels")
     ap.add_argument("--glevel", type=int, default=8)
     ap.add_argument("--kall", type=int, default=96)
     ap.add_argument("--ntr", type=int, default=32)
@@ -329,6 +463,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-check", action="store_true", help="skip the error / mass-drift check")
     ap.add_argument("--tile-shape", type=int, default=-1, help="tile shape index of the horizontal kernel (default: autotune)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")
@@ -337,6 +472,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, world, rank)
+        elif args.mode == "uneven":
+            run_uneven(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

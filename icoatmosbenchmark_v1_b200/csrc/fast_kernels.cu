@@ -299,6 +299,15 @@ __global__ void k_fast_offsets(FastInst I, float *off) {
   }
 }
 
+// Threshold of the upwind masks (0.5 - sign(0.5, ch - EPS)) and of the zero-outflow guards
+// (zerosw) in the FP32 arithmetic: the FP64 EPS, not epsilon(1.0).  These are switches, not
+// roundings: with FP32's own EPS a face whose Courant number lies in (2.2e-16, 1.2e-7) is
+// taken from the other side than in FP64, which moves its 4-point bounds into or out of the
+// cell's qnext; at a slotted-cylinder edge (glevel 7, kall 96) that gave 9e-4 relative error
+// against the FP64 oracle in 10 cells.  With the FP64 threshold the same run is at 1.6e-7.
+// (The standalone *_f32 kernel entry points keep the reference's RP = SP semantics.)
+constexpr float kEpsThr = (float)DBL_EPSILON;
+
 // ---- vertical Thuburn limiter (dyn_vert_adv_limiter/src/mod_src_tracer.f90:107-186), d = 0, FP32:
 // the tracer-independent part of a level (upwind flags, Courant sums) and the per-tracer bounds
 struct VLim {
@@ -315,7 +324,7 @@ __device__ __forceinline__ VLim vlim_params(float c1, float c2, float c1p) {
   const float Cin = v.a1 + v.a2;
   const float Cout = (1.0f - v.infl) * c1 + (1.0f - infu) * c2;
   v.icm = Cin + Cout;
-  v.zsw = 0.5f - copysignf(0.5f, fabsf(Cout) - FLT_EPSILON);
+  v.zsw = 0.5f - copysignf(0.5f, fabsf(Cout) - kEpsThr);
   v.rden = (1.0f - v.zsw) / (Cout + v.zsw);
   return v;
 }
@@ -382,7 +391,7 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   const size_t base = (size_t)l * lk + (size_t)k * slab;
   const double dt = I.dt;
   const float dtf = (float)dt;
-  const float BIGf = FLT_MAX, EPSf = FLT_EPSILON;
+  const float BIGf = FLT_MAX, EPSf = kEpsThr;
 
   // this thread's ring cell
   const bool ring = tid < NR;
