@@ -147,6 +147,21 @@ void orc_step(const orc_dims *d, const int *have_sgp, const orc_topo *topo,
               const double *coef_grad, const double *coef_grad_pl,
               int nthreads);
 
+/* Adjoint of orc_step (oracle_adjoint.c): given the step's input state and, in
+ * a_rhog / a_rhogq (+ _pl), the adjoint of its output, overwrites them with the
+ * adjoint of its input and adds the adjoint of rhogvx/vy/vz (+ _pl) to a_vx/a_vy/a_vz. */
+void orc_step_adjoint(const orc_dims *d, const int *have_sgp, const orc_topo *topo, int ntr, double dt,
+                      const double *rhog, const double *rhog_pl, const double *rhogq, const double *rhogq_pl,
+                      const double *rhogvx, const double *rhogvx_pl, const double *rhogvy, const double *rhogvy_pl,
+                      const double *rhogvz, const double *rhogvz_pl, const double *rhogw, const double *rhogw_pl,
+                      const double *rdgz, const double *afact, const double *bfact,
+                      const double *GRD_x, const double *GRD_x_pl, const double *GRD_xr, const double *GRD_xr_pl,
+                      const double *GMTR_p, const double *GMTR_p_pl, const double *GMTR_t, const double *GMTR_t_pl,
+                      const double *GMTR_a, const double *GMTR_a_pl, const double *coef_grad,
+                      const double *coef_grad_pl, double *a_rhog, double *a_rhog_pl, double *a_rhogq,
+                      double *a_rhogq_pl, double *a_vx, double *a_vx_pl, double *a_vy, double *a_vy_pl, double *a_vz,
+                      double *a_vz_pl);
+
 #ifdef __cplusplus
 }
 #endif

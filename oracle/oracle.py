@@ -195,6 +195,27 @@ def remap(d, q, q_pl, gr, gr_pl, cm, cm_pl, xc, xc_pl, geo):
     return qa, qa_pl
 
 
+def step_adjoint(d, have_sgp, topo, dt, state, fields, geo, adj_state, adj_wind):
+    """Adjoint of one step at input `state`: adj_state (rhog, rhog_pl, rhogq, rhogq_pl) holds the
+    adjoint of the step's output and is overwritten with the adjoint of its input; adj_wind
+    (rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz, rhogvz_pl) is accumulated."""
+    s, sp = _sgp(have_sgp)
+    ntr = state["rhogq"].shape[0]
+    lib().orc_step_adjoint(C.byref(d), sp, C.c_void_p(topo.h), ntr, C.c_double(dt),
+                           _p(state["rhog"]), _p(state["rhog_pl"]), _p(state["rhogq"]), _p(state["rhogq_pl"]),
+                           _p(fields["rhogvx"]), _p(fields["rhogvx_pl"]), _p(fields["rhogvy"]),
+                           _p(fields["rhogvy_pl"]), _p(fields["rhogvz"]), _p(fields["rhogvz_pl"]),
+                           _p(fields["rhogw"]), _p(fields["rhogw_pl"]),
+                           _p(geo["rdgz"]), _p(geo["afact"]), _p(geo["bfact"]),
+                           _p(geo["GRD_x"]), _p(geo["GRD_x_pl"]), _p(geo["GRD_xr"]), _p(geo["GRD_xr_pl"]),
+                           _p(geo["GMTR_p"]), _p(geo["GMTR_p_pl"]), _p(geo["GMTR_t"]), _p(geo["GMTR_t_pl"]),
+                           _p(geo["GMTR_a"]), _p(geo["GMTR_a_pl"]), _p(geo["coef_grad"]), _p(geo["coef_grad_pl"]),
+                           _p(adj_state["rhog"]), _p(adj_state["rhog_pl"]), _p(adj_state["rhogq"]),
+                           _p(adj_state["rhogq_pl"]), _p(adj_wind["rhogvx"]), _p(adj_wind["rhogvx_pl"]),
+                           _p(adj_wind["rhogvy"]), _p(adj_wind["rhogvy_pl"]), _p(adj_wind["rhogvz"]),
+                           _p(adj_wind["rhogvz_pl"]))
+
+
 def step(d, have_sgp, topo, dt, state, fields, geo, nthreads=None):
     """One composed tracer step in place on state = dict(rhog, rhog_pl, rhogq, rhogq_pl)."""
     s, sp = _sgp(have_sgp)
