@@ -265,6 +265,44 @@ class IcoAdv:
         with self._ordered(bool(kinds[0])):
             _check(name, getattr(lib(), name)(self.h, int(ntr), C.c_double(dt), *ptrs))
 
+    # ---- adjoint of the plain step ---------------------------------------------------
+    def advect_step_adjoint(self, dt, state, fields, a_state, a_wind):
+        """Reverse mode of one plain FP64 step.  state / fields: dicts (STATE_KEYS, FIELD_KEYS)
+        of the step's input (unchanged); a_state (STATE_KEYS): adjoint of the step's output
+        on entry, of its input on return; a_wind (WIND_KEYS): accumulated.  All numpy
+        (host) or all CUDA tensors (device)."""
+        ntr = state["rhogq"].shape[0]
+        arrs = ([state[k] for k in STATE_KEYS] + [fields[k] for k in FIELD_KEYS] + [a_state[k] for k in STATE_KEYS]
+                + [a_wind[k] for k in WIND_KEYS])
+        ptrs, kinds = zip(*[_ptr(a, np.float64) for a in arrs])
+        if len(set(kinds)) != 1:
+            raise TypeError("mix of host and device arrays")
+        name = "ica_advect_step_adjoint" + ("_dev" if kinds[0] else "")
+        with self._ordered(bool(kinds[0])):
+            _check(name, getattr(lib(), name)(self.h, int(ntr), C.c_double(dt), *ptrs))
+
+    def adjoint_record(self, dt, nsteps, every, state, fields):
+        """Advances the device state nsteps plain FP64 steps in place, keeping a checkpoint
+        every `every` steps for adjoint_sweep."""
+        ntr = state["rhogq"].shape[0]
+        sp = [_ptr(state[k], np.float64)[0] for k in STATE_KEYS]
+        fp = [_ptr(fields[k], np.float64)[0] for k in FIELD_KEYS]
+        with self._ordered():
+            _check("ica_adjoint_record", lib().ica_adjoint_record(self.h, int(ntr), C.c_double(dt), int(nsteps),
+                                                                  int(every), *sp, *fp))
+
+    def adjoint_sweep(self, fields, a_state, a_wind):
+        """Adjoint of the recorded run: a_state holds the adjoint of the final state on entry
+        and of the initial state on return; a_wind is accumulated (device tensors)."""
+        fp = [_ptr(fields[k], np.float64)[0] for k in FIELD_KEYS]
+        ap = [_ptr(a_state[k], np.float64)[0] for k in STATE_KEYS] + [_ptr(a_wind[k], np.float64)[0]
+                                                                      for k in WIND_KEYS]
+        with self._ordered():
+            _check("ica_adjoint_sweep", lib().ica_adjoint_sweep(self.h, *fp, *ap))
+
+    def adjoint_release(self):
+        _check("ica_adjoint_release", lib().ica_adjoint_release(self.h))
+
     # ---- batched path (all tracers per launch) -------------------------------------
     def advect_fast_dev(self, dt, state_in, state_out, fields32):
         """One batched step on device tensors: state dicts (rhog, rhog_pl, rhogq, rhogq_pl) FP64,
@@ -310,6 +348,7 @@ class IcoAdv:
 
 STATE_KEYS = ("rhog", "rhog_pl", "rhogq", "rhogq_pl")
 FIELD_KEYS = ("rhogvx", "rhogvx_pl", "rhogvy", "rhogvy_pl", "rhogvz", "rhogvz_pl", "rhogw", "rhogw_pl")
+WIND_KEYS = ("rhogvx", "rhogvx_pl", "rhogvy", "rhogvy_pl", "rhogvz", "rhogvz_pl")
 
 
 class FastRunner:

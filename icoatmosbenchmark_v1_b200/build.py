@@ -32,6 +32,7 @@ SOURCES = {
     "step.cu": ["--fmad=false"],
     "fast_kernels.cu": [],
     "noalloc.cu": [],
+    "adjoint.cu": ["--fmad=false"],
 }
 
 

@@ -2,6 +2,7 @@
 // points that keep the reference subroutines' argument lists.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -34,6 +35,13 @@ void *Ctx::buf(const char *name, size_t bytes) {
     b.bytes = bytes;
   }
   return b.ptr;
+}
+
+void Ctx::release(const char *name) {
+  auto it = bufs.find(name);
+  if (it == bufs.end()) return;
+  if (it->second.ptr) cudaFree(it->second.ptr);
+  bufs.erase(it);
 }
 
 int Ctx::check_launch(const char *what) {
@@ -596,6 +604,204 @@ int ica_advect_step(ica_ctx *c, int ntr, double dt, double *rhog, double *rhog_p
   s.out(rhogq, d_q, n3 * ntr);
   s.out(rhogq_pl, d_qp, n3p * ntr);
   return s.sync();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// adjoint of the composed step, and multi-step runs with step checkpointing
+#include "adjoint.cuh"
+
+namespace icoadv {
+
+static int adj_scratch(Ctx *c, AdjScratch &A) {
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  struct B {
+    double **p;
+    const char *name;
+    size_t n;
+  } bl[] = {{&A.rh, "adj_rh", n3},         {&A.rh_pl, "adj_rhp", n3p},     {&A.qa1, "adj_tr", 8 * n3},
+            {&A.qa1_pl, "adj_qa1p", n3p},  {&A.Qh_pl, "adj_Qhp", n3p},     {&A.a_q_pl, "adj_aqp", n3p},
+            {&A.a_flx, "adj_aflx", 6 * n3}, {&A.a_flx_pl, "adj_aflxp", n3p}, {&A.a_xc, "adj_axc", 9 * n3},
+            {&A.a_xc_pl, "adj_axcp", 3 * n3p}, {&A.a_ch, "adj_ach", 6 * n3}, {&A.a_ch_pl, "adj_achp", n3p},
+            {&A.a_rh, "adj_arh", n3},      {&A.a_rh_pl, "adj_arhp", n3p},  {&A.a_gr, "adj_agr", 3 * n3},
+            {&A.a_gr_pl, "adj_agrp", 3 * n3p}, {&A.a_qo, "adj_aqo", 2 * n3}, {&A.a_qo_pl, "adj_aqop", 2 * n3p}};
+  for (auto &b : bl) {
+    *b.p = (double *)c->buf(b.name, b.n * sizeof(double));
+    if (!*b.p) return set_error(std::string("cudaMalloc ") + b.name), ICA_ERR_NOMEM;
+  }
+  // qa1 | Qh | a_q are one block, reused as the 8 triangle-adjoint fields after the tracers
+  A.Qh = A.qa1 + 6 * n3;
+  A.a_q = A.qa1 + 7 * n3;
+  A.aT = A.qa1;
+  return ICA_OK;
+}
+
+// one state = rhog | rhog_pl | rhogq | rhogq_pl
+struct StateView {
+  double *r, *rp, *q, *qp;
+};
+static size_t state_doubles(const Ctx *c, int ntr) {
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  return (size_t)(ntr + 1) * (n3 + n3p);
+}
+static StateView state_at(const Ctx *c, double *base, int ntr) {
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  return StateView{base, base + n3, base + n3 + n3p, base + n3 + n3p + ntr * n3};
+}
+static void copy_state(const Ctx *c, const StateView &d, const double *r, const double *rp, const double *q,
+                       const double *qp, int ntr) {
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  const size_t B = sizeof(double);
+  cudaMemcpyAsync(d.r, r, n3 * B, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(d.rp, rp, n3p * B, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(d.q, q, ntr * n3 * B, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(d.qp, qp, ntr * n3p * B, cudaMemcpyDeviceToDevice, c->stream);
+}
+
+}  // namespace icoadv
+
+extern "C" {
+
+int ica_advect_step_adjoint_dev(ica_ctx *c, int ntr, double dt, const double *rhog, const double *rhog_pl,
+                                const double *rhogq, const double *rhogq_pl, const double *vx, const double *vx_pl,
+                                const double *vy, const double *vy_pl, const double *vz, const double *vz_pl,
+                                const double *w, const double *w_pl, double *a_rhog, double *a_rhog_pl,
+                                double *a_rhogq, double *a_rhogq_pl, double *a_vx, double *a_vx_pl, double *a_vy,
+                                double *a_vy_pl, double *a_vz, double *a_vz_pl) {
+  CTX_OK(c);
+  const void *ptrs[] = {rhog, rhog_pl, rhogq, rhogq_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl,
+                        a_rhog, a_rhog_pl, a_rhogq, a_rhogq_pl, a_vx, a_vx_pl, a_vy, a_vy_pl, a_vz, a_vz_pl};
+  for (const void *p : ptrs)
+    if (!p) return set_error("ica_advect_step_adjoint: NULL argument"), ICA_ERR_ARG;
+  if (ntr < 1) return set_error("ica_advect_step_adjoint: ntr < 1"), ICA_ERR_ARG;
+  if (c->sz.kall < 4 || c->sz.kall > 128) return set_error("ica_advect_step_adjoint: needs 4 <= kall <= 128"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  StepCtx S;
+  AdjScratch A;
+  int rc = c->step_ctx(S);
+  if (!rc) rc = adj_scratch(c, A);
+  if (rc) return rc;
+  rc = step_adjoint(S, A, ntr, dt, rhog, rhog_pl, rhogq, rhogq_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl, a_rhog,
+                    a_rhog_pl, a_rhogq, a_rhogq_pl, a_vx, a_vx_pl, a_vy, a_vy_pl, a_vz, a_vz_pl, c->stream,
+                    c->launches);
+  if (rc) return set_error("ica_advect_step_adjoint: bad vertical grid"), rc;
+  return c->check_launch("ica_advect_step_adjoint");
+}
+
+int ica_advect_step_adjoint(ica_ctx *c, int ntr, double dt, const double *rhog, const double *rhog_pl,
+                            const double *rhogq, const double *rhogq_pl, const double *vx, const double *vx_pl,
+                            const double *vy, const double *vy_pl, const double *vz, const double *vz_pl,
+                            const double *w, const double *w_pl, double *a_rhog, double *a_rhog_pl, double *a_rhogq,
+                            double *a_rhogq_pl, double *a_vx, double *a_vx_pl, double *a_vy, double *a_vy_pl,
+                            double *a_vz, double *a_vz_pl) {
+  CTX_OK(c);
+  if (ntr < 1 || !rhog || !rhog_pl || !rhogq || !rhogq_pl || !vx || !vx_pl || !vy || !vy_pl || !vz || !vz_pl || !w ||
+      !w_pl || !a_rhog || !a_rhog_pl || !a_rhogq || !a_rhogq_pl || !a_vx || !a_vx_pl || !a_vy || !a_vy_pl || !a_vz ||
+      !a_vz_pl)
+    return set_error("ica_advect_step_adjoint: bad argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  Stage<double> s(c);
+  const double *d[12] = {s.in("h0", rhog, n3),   s.in("h1", rhog_pl, n3p), s.in("h2", rhogq, n3 * ntr),
+                         s.in("h3", rhogq_pl, n3p * ntr), s.in("h4", vx, n3), s.in("h5", vx_pl, n3p),
+                         s.in("h6", vy, n3),     s.in("h7", vy_pl, n3p),   s.in("h8", vz, n3),
+                         s.in("h9", vz_pl, n3p), s.in("h10", w, n3),       s.in("h11", w_pl, n3p)};
+  double *a[10] = {s.in("j0", a_rhog, n3), s.in("j1", a_rhog_pl, n3p), s.in("j2", a_rhogq, n3 * ntr),
+                   s.in("j3", a_rhogq_pl, n3p * ntr), s.in("j4", a_vx, n3), s.in("j5", a_vx_pl, n3p),
+                   s.in("j6", a_vy, n3), s.in("j7", a_vy_pl, n3p), s.in("j8", a_vz, n3), s.in("j9", a_vz_pl, n3p)};
+  if (s.rc) return s.rc;
+  int rc = ica_advect_step_adjoint_dev(c, ntr, dt, d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7], d[8], d[9], d[10],
+                                       d[11], a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9]);
+  if (rc) return rc;
+  double *h[10] = {a_rhog, a_rhog_pl, a_rhogq, a_rhogq_pl, a_vx, a_vx_pl, a_vy, a_vy_pl, a_vz, a_vz_pl};
+  const size_t n[10] = {n3, n3p, n3 * ntr, n3p * ntr, n3, n3p, n3, n3p, n3, n3p};
+  for (int i = 0; i < 10; ++i) s.out(h[i], a[i], n[i]);
+  return s.sync();
+}
+
+int ica_adjoint_record(ica_ctx *c, int ntr, double dt, int nsteps, int every, double *rhog, double *rhog_pl,
+                       double *rhogq, double *rhogq_pl, const double *vx, const double *vx_pl, const double *vy,
+                       const double *vy_pl, const double *vz, const double *vz_pl, const double *w,
+                       const double *w_pl) {
+  CTX_OK(c);
+  if (ntr < 1 || nsteps < 1 || every < 1 || !rhog || !rhog_pl || !rhogq || !rhogq_pl || !vx || !vx_pl || !vy ||
+      !vy_pl || !vz || !vz_pl || !w || !w_pl)
+    return set_error("ica_adjoint_record: bad argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  c->tape = AdjTape{};
+  StepCtx S;
+  int rc = c->step_ctx(S);
+  if (rc) return rc;
+  const int ncp = (nsteps + every - 1) / every;
+  const size_t sd = state_doubles(c, ntr);
+  double *ck = (double *)c->buf("adj_ckpt", (size_t)ncp * sd * sizeof(double));
+  if (!ck) return set_error("ica_adjoint_record: cudaMalloc of the checkpoints"), ICA_ERR_NOMEM;
+  for (int s = 0; s < nsteps; ++s) {
+    if (s % every == 0) copy_state(c, state_at(c, ck + (size_t)(s / every) * sd, ntr), rhog, rhog_pl, rhogq, rhogq_pl, ntr);
+    rc = step_plain(S, ntr, dt, rhog, rhog_pl, rhogq, rhogq_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl, c->stream,
+                    c->launches);
+    if (rc) return set_error("ica_adjoint_record: kall above 128"), rc;
+  }
+  c->tape = AdjTape{true, ntr, nsteps, every, dt};
+  return c->check_launch("ica_adjoint_record");
+}
+
+int ica_adjoint_sweep(ica_ctx *c, const double *vx, const double *vx_pl, const double *vy, const double *vy_pl,
+                      const double *vz, const double *vz_pl, const double *w, const double *w_pl, double *a_rhog,
+                      double *a_rhog_pl, double *a_rhogq, double *a_rhogq_pl, double *a_vx, double *a_vx_pl,
+                      double *a_vy, double *a_vy_pl, double *a_vz, double *a_vz_pl) {
+  CTX_OK(c);
+  const void *ptrs[] = {vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl, a_rhog, a_rhog_pl, a_rhogq, a_rhogq_pl,
+                        a_vx, a_vx_pl, a_vy, a_vy_pl, a_vz, a_vz_pl};
+  for (const void *p : ptrs)
+    if (!p) return set_error("ica_adjoint_sweep: NULL argument"), ICA_ERR_ARG;
+  if (!c->tape.ready) return set_error("ica_adjoint_sweep: no recorded run"), ICA_ERR_STATE;
+  if (c->sz.kall < 4 || c->sz.kall > 128) return set_error("ica_adjoint_sweep: needs 4 <= kall <= 128"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  const AdjTape T = c->tape;
+  StepCtx S;
+  AdjScratch A;
+  int rc = c->step_ctx(S);
+  if (!rc) rc = adj_scratch(c, A);
+  if (rc) return rc;
+  const size_t sd = state_doubles(c, T.ntr);
+  double *ck = (double *)c->buf("adj_ckpt", 0);
+  if (!ck) return set_error("ica_adjoint_sweep: no recorded run"), ICA_ERR_STATE;
+  double *seg = T.every > 1 ? (double *)c->buf("adj_seg", (size_t)(T.every - 1) * sd * sizeof(double)) : nullptr;
+  if (T.every > 1 && !seg) return set_error("ica_adjoint_sweep: cudaMalloc of the segment states"), ICA_ERR_NOMEM;
+  const int ncp = (T.nsteps + T.every - 1) / T.every;
+  std::vector<StateView> st((size_t)T.every);
+  for (int g = ncp - 1; g >= 0; --g) {
+    const int s0 = g * T.every, L = std::min(T.every, T.nsteps - s0);
+    st[0] = state_at(c, ck + (size_t)g * sd, T.ntr);
+    for (int u = 1; u < L; ++u) {  // recompute the segment from its checkpoint
+      st[u] = state_at(c, seg + (size_t)(u - 1) * sd, T.ntr);
+      copy_state(c, st[u], st[u - 1].r, st[u - 1].rp, st[u - 1].q, st[u - 1].qp, T.ntr);
+      rc = step_plain(S, T.ntr, T.dt, st[u].r, st[u].rp, st[u].q, st[u].qp, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl,
+                      c->stream, c->launches);
+      if (rc) return set_error("ica_adjoint_sweep: kall above 128"), rc;
+    }
+    for (int u = L - 1; u >= 0; --u) {
+      rc = step_adjoint(S, A, T.ntr, T.dt, st[u].r, st[u].rp, st[u].q, st[u].qp, vx, vx_pl, vy, vy_pl, vz, vz_pl, w,
+                        w_pl, a_rhog, a_rhog_pl, a_rhogq, a_rhogq_pl, a_vx, a_vx_pl, a_vy, a_vy_pl, a_vz, a_vz_pl,
+                        c->stream, c->launches);
+      if (rc) return set_error("ica_adjoint_sweep: bad vertical grid"), rc;
+    }
+  }
+  return c->check_launch("ica_adjoint_sweep");
+}
+
+int ica_adjoint_release(ica_ctx *c) {
+  CTX_OK(c);
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (const char *n : {"adj_ckpt", "adj_seg", "adj_rh", "adj_rhp", "adj_tr", "adj_qa1p", "adj_Qhp", "adj_aqp",
+                        "adj_aflx", "adj_aflxp", "adj_axc", "adj_axcp", "adj_ach", "adj_achp", "adj_arh", "adj_arhp",
+                        "adj_agr", "adj_agrp", "adj_aqo", "adj_aqop"})
+    c->release(n);
+  c->tape = AdjTape{};
+  return ICA_OK;
 }
 
 }  // extern "C"

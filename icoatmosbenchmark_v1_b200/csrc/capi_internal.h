@@ -39,6 +39,12 @@ struct FastState {  // fused path: boundary tables, tile shape, kernel timing
 
 struct FastInst;
 
+struct AdjTape {  // a recorded multi-step run: checkpoints every `every` steps
+  bool ready = false;
+  int ntr = 0, nsteps = 0, every = 0;
+  double dt = 0.0;
+};
+
 struct Ctx {
   std::unique_ptr<Topology> topo;
   ica_sizes sz{};
@@ -58,6 +64,7 @@ struct Ctx {
 
   ~Ctx();
   void *buf(const char *name, size_t bytes);
+  void release(const char *name);
   int check_launch(const char *what);
   int upload_geometry(const double *const h[8], const size_t n[8]);
   template <typename T> Geo<T> geo() const;
@@ -65,6 +72,7 @@ struct Ctx {
   FastState fast;
   int build_fast_tables();
   int fast_inst(FastInst &I, int ntr, double dt);
+  AdjTape tape;
 };
 
 int cuda_fail(cudaError_t e, const char *what);

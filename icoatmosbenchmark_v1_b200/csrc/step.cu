@@ -269,41 +269,74 @@ __global__ void k_vertical(Dims D, int ntr, double dt, double *rho, double *Q, c
 
 // ---------------------------------------------------------------------------
 static dim3 slab(const Dims &D, int th) { return dim3((D.gall + th - 1) / th, D.kall * D.lall); }
+static constexpr int kSlabThreads = 128;
+
+static size_t n3_of(const Dims &D) { return (size_t)D.gall * D.kall * D.lall; }
+static size_t n3p_of(const Dims &D) { return (size_t)kGallPl * D.kall * kLallPl; }
+
+void launch_courant(const StepCtx &S, const double *rhog, const double *rhog_pl, cudaStream_t st) {
+  const size_t n3 = n3_of(S.D), n3p = n3p_of(S.D);
+  k_courant<<<(unsigned)((6 * n3 + 255) / 256), 256, 0, st>>>((int)n3, S.flx, rhog, S.ch, S.cm);
+  k_courant_pl<<<(unsigned)((n3p + 255) / 256), 256, 0, st>>>(S.D.kall, S.flx_pl, rhog_pl, S.ch_pl, S.cm_pl);
+}
+
+void launch_divide(const StepCtx &S, const double *Q, const double *Qp, const double *rhog, const double *rhog_pl,
+                   cudaStream_t st) {
+  const size_t n3 = n3_of(S.D), n3p = n3p_of(S.D);
+  k_divide<<<(unsigned)((n3 + n3p + 255) / 256), 256, 0, st>>>((long long)n3, (int)n3p, Q, rhog, Qp, rhog_pl, S.q,
+                                                               S.q_pl);
+}
+
+void launch_gradient(const StepCtx &S, cudaStream_t st) {
+  const Dims &D = S.D;
+  k_gradient<<<slab(D, kSlabThreads), kSlabThreads, 0, st>>>(D, S.q, S.cg, S.grad);
+  k_gradient_pl<<<(unsigned)((kLallPl * D.kall + 255) / 256), 256, 0, st>>>(D.kall, S.q_pl, S.cg_pl, S.grad_pl);
+  launch_gather<double>(D, S.plan.n, S.plan.dst, S.plan.src, D.kall, 3, S.grad, S.grad_pl, st);
+}
+
+void launch_remap(const StepCtx &S, cudaStream_t st) {
+  const Dims &D = S.D;
+  k_remap<<<slab(D, kSlabThreads), kSlabThreads, 0, st>>>(D, S.q, S.grad, S.cm, S.xc, S.GRD_x, S.qa);
+  k_remap_pl<<<(unsigned)((n3p_of(D) + 255) / 256), 256, 0, st>>>(D.kall, S.q_pl, S.grad_pl, S.cm_pl, S.xc_pl,
+                                                                   S.GRD_x_pl, S.qa_pl);
+}
+
+void launch_update_h(const StepCtx &S, const double *qa, const double *qa_pl, double *Q, double *Qp, cudaStream_t st) {
+  const Dims &D = S.D;
+  k_update_h<<<slab(D, kSlabThreads), kSlabThreads, 0, st>>>(D, S.flx, qa, Q);
+  k_update_h_pl<<<(unsigned)((kLallPl * D.kall + 255) / 256), 256, 0, st>>>(D.kall, S.flx_pl, qa_pl, Qp);
+}
+
+void launch_update_rho(const StepCtx &S, double *rho, double *rho_pl, cudaStream_t st) {
+  const Dims &D = S.D;
+  k_update_rho<<<slab(D, kSlabThreads), kSlabThreads, 0, st>>>(D, S.flx, rho);
+  k_update_rho_pl<<<(unsigned)((kLallPl * D.kall + 255) / 256), 256, 0, st>>>(D.kall, S.flx_pl, rho_pl);
+}
 
 int step_plain(StepCtx &S, int ntr, double dt, double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
                const double *vx, const double *vx_pl, const double *vy, const double *vy_pl, const double *vz,
                const double *vz_pl, const double *w, const double *w_pl, cudaStream_t st, long long &launches) {
   const Dims &D = S.D;
-  const size_t n3 = (size_t)D.gall * D.kall * D.lall, n3p = (size_t)kGallPl * D.kall * kLallPl;
-  const int T = 128;
-  const unsigned nb6 = (unsigned)((n3p + 255) / 256);                // one thread per pole point
-  const unsigned nb1 = (unsigned)((kLallPl * D.kall + 255) / 256);   // one thread per pole level
+  const size_t n3 = n3_of(D), n3p = n3p_of(D);
   // shared per step
   FluxIn<double> fin{rhog, rhog_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl};
   FluxOut<double> fout{S.flx, S.flx_pl, S.xc, S.xc_pl};
   launch_horizontal_flux<double>(D, fin, fout, S.geo, dt, st);
-  k_courant<<<(unsigned)((6 * n3 + 255) / 256), 256, 0, st>>>((int)n3, S.flx, rhog, S.ch, S.cm);
-  k_courant_pl<<<nb6, 256, 0, st>>>(D.kall, S.flx_pl, rhog_pl, S.ch_pl, S.cm_pl);
+  launch_courant(S, rhog, rhog_pl, st);
   launches += 4;
   LimIn<double> lin{S.q, S.q_pl, S.zero, S.zero_pl, S.ch, S.ch_pl, S.cm, S.cm_pl};
   for (int t = 0; t < ntr; ++t) {
     double *Q = rhogq + t * n3, *Qp = rhogq_pl + t * n3p;
-    k_divide<<<(unsigned)((n3 + n3p + 255) / 256), 256, 0, st>>>((long long)n3, (int)n3p, Q, rhog, Qp, rhog_pl,
-                                                                 S.q, S.q_pl);
-    k_gradient<<<slab(D, T), T, 0, st>>>(D, S.q, S.cg, S.grad);
-    k_gradient_pl<<<nb1, 256, 0, st>>>(D.kall, S.q_pl, S.cg_pl, S.grad_pl);
-    launch_gather<double>(D, S.plan.n, S.plan.dst, S.plan.src, D.kall, 3, S.grad, S.grad_pl, st);
-    k_remap<<<slab(D, T), T, 0, st>>>(D, S.q, S.grad, S.cm, S.xc, S.GRD_x, S.qa);
-    k_remap_pl<<<nb6, 256, 0, st>>>(D.kall, S.q_pl, S.grad_pl, S.cm_pl, S.xc_pl, S.GRD_x_pl, S.qa_pl);
+    launch_divide(S, Q, Qp, rhog, rhog_pl, st);
+    launch_gradient(S, st);
+    launch_remap(S, st);
     launch_hlim_qout<double>(D, lin, S.qout, S.qout_pl, S.qin_pl, st);
     launch_gather<double>(D, S.plan.n, S.plan.dst, S.plan.src, D.kall, 2, S.qout, S.qout_pl, st);
     launch_hlim_apply<double>(D, lin, S.qa, S.qa_pl, S.qout, S.qout_pl, S.qin_pl, st);
-    k_update_h<<<slab(D, T), T, 0, st>>>(D, S.flx, S.qa, Q);
-    k_update_h_pl<<<nb1, 256, 0, st>>>(D.kall, S.flx_pl, S.qa_pl, Qp);
+    launch_update_h(S, S.qa, S.qa_pl, Q, Qp, st);
     launches += 14;
   }
-  k_update_rho<<<slab(D, T), T, 0, st>>>(D, S.flx, rhog);
-  k_update_rho_pl<<<nb1, 256, 0, st>>>(D.kall, S.flx_pl, rhog_pl);
+  launch_update_rho(S, rhog, rhog_pl, st);
   const int ncol = D.lall * D.gall + kLallPl;
   if (D.kall <= 48)
     k_vertical<48><<<(ncol + 127) / 128, 128, 0, st>>>(D, ntr, dt, rhog, rhogq, w, rhog_pl, rhogq_pl, w_pl, S.rdgz,

@@ -22,6 +22,16 @@ struct StepCtx {
   double *q, *q_pl, *grad, *grad_pl, *qa, *qa_pl, *qout, *qout_pl, *qin_pl;
 };
 
+// Pieces of the plain step, also used by the adjoint's forward recompute.
+void launch_courant(const StepCtx &S, const double *rhog, const double *rhog_pl, cudaStream_t st);  // flx -> ch, cm
+void launch_divide(const StepCtx &S, const double *Q, const double *Qp, const double *rhog, const double *rhog_pl,
+                   cudaStream_t st);                                  // q = Q / rhog
+void launch_gradient(const StepCtx &S, cudaStream_t st);             // q -> grad, halo filled
+void launch_remap(const StepCtx &S, cudaStream_t st);                // q, grad -> qa
+void launch_update_h(const StepCtx &S, const double *qa, const double *qa_pl, double *Q, double *Qp,
+                     cudaStream_t st);                                // Q -= sum flx qa (interior, pole centres)
+void launch_update_rho(const StepCtx &S, double *rho, double *rho_pl, cudaStream_t st);  // rho -= sum flx
+
 int step_plain(StepCtx &S, int ntr, double dt, double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
                const double *vx, const double *vx_pl, const double *vy, const double *vy_pl, const double *vz,
                const double *vz_pl, const double *w, const double *w_pl, cudaStream_t st, long long &launches);

@@ -237,6 +237,70 @@ int ica_advect_step_dev(ica_ctx *ctx, int ntr, double dt,
                         const double *rhogvz, const double *rhogvz_pl,
                         const double *rhogw, const double *rhogw_pl);
 
+/* Adjoint (reverse mode) of the plain FP64 step, for gradients of a function
+ * of the state after the step.  Subgradients at the limiter kinks: min / max /
+ * clamp pass the adjoint to the operand the forward step returned, the upwind
+ * masks, inflow flags and zero-outflow switches are held fixed, and the
+ * +-BIG terms of a masked bound carry no derivative.  rhogw, the geometry and
+ * the vertical grid are constants.
+ *   in:      the step's input state (rhog, rhogq + pole arrays; unchanged), the fields
+ *   in/out:  a_rhog(gall,kall,lall) a_rhog_pl, a_rhogq(gall,kall,lall,ntr) a_rhogq_pl:
+ *            the adjoint of the step's output on entry, of its input on return
+ *   +=:      a_rhogvx/vy/vz (+ _pl), the adjoint of the horizontal wind
+ * Needs 4 <= kall <= 128.  Halo points of the adjoint follow the state's halo
+ * fill: on return the adjoint of a halo point is what the step's output depends
+ * on it through (its own value before the fill), not a copy. */
+int ica_advect_step_adjoint_dev(ica_ctx *ctx, int ntr, double dt,
+                                const double *rhog, const double *rhog_pl,
+                                const double *rhogq, const double *rhogq_pl,
+                                const double *rhogvx, const double *rhogvx_pl,
+                                const double *rhogvy, const double *rhogvy_pl,
+                                const double *rhogvz, const double *rhogvz_pl,
+                                const double *rhogw, const double *rhogw_pl,
+                                double *a_rhog, double *a_rhog_pl,
+                                double *a_rhogq, double *a_rhogq_pl,
+                                double *a_rhogvx, double *a_rhogvx_pl,
+                                double *a_rhogvy, double *a_rhogvy_pl,
+                                double *a_rhogvz, double *a_rhogvz_pl);
+int ica_advect_step_adjoint(ica_ctx *ctx, int ntr, double dt,
+                            const double *rhog, const double *rhog_pl,
+                            const double *rhogq, const double *rhogq_pl,
+                            const double *rhogvx, const double *rhogvx_pl,
+                            const double *rhogvy, const double *rhogvy_pl,
+                            const double *rhogvz, const double *rhogvz_pl,
+                            const double *rhogw, const double *rhogw_pl,
+                            double *a_rhog, double *a_rhog_pl,
+                            double *a_rhogq, double *a_rhogq_pl,
+                            double *a_rhogvx, double *a_rhogvx_pl,
+                            double *a_rhogvy, double *a_rhogvy_pl,
+                            double *a_rhogvz, double *a_rhogvz_pl);
+/* Multi-step runs with step checkpointing (device pointers, context stream).
+ * ica_adjoint_record advances the state nsteps plain FP64 steps in place and
+ * keeps a copy of the state every `every` steps (ceil(nsteps/every) states of
+ * device memory held by the context).  ica_adjoint_sweep runs the adjoint
+ * backwards over the recorded run: each segment is recomputed from its
+ * checkpoint (every-1 more states held) and transposed step by step; the
+ * a_* arguments mean what they mean for ica_advect_step_adjoint_dev, for the
+ * whole run.  The fields must be the ones the run was recorded with.
+ * ica_adjoint_release frees the checkpoints and the adjoint scratch. */
+int ica_adjoint_record(ica_ctx *ctx, int ntr, double dt, int nsteps, int every,
+                       double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
+                       const double *rhogvx, const double *rhogvx_pl,
+                       const double *rhogvy, const double *rhogvy_pl,
+                       const double *rhogvz, const double *rhogvz_pl,
+                       const double *rhogw, const double *rhogw_pl);
+int ica_adjoint_sweep(ica_ctx *ctx,
+                      const double *rhogvx, const double *rhogvx_pl,
+                      const double *rhogvy, const double *rhogvy_pl,
+                      const double *rhogvz, const double *rhogvz_pl,
+                      const double *rhogw, const double *rhogw_pl,
+                      double *a_rhog, double *a_rhog_pl,
+                      double *a_rhogq, double *a_rhogq_pl,
+                      double *a_rhogvx, double *a_rhogvx_pl,
+                      double *a_rhogvy, double *a_rhogvy_pl,
+                      double *a_rhogvz, double *a_rhogvz_pl);
+int ica_adjoint_release(ica_ctx *ctx);
+
 /* Batched step: all tracers of the step together, a horizontal kernel (one
  * CTA per region tile and level) and a vertical kernel (one thread per column
  * and tracer); FP32 flux-form remap / limiter arithmetic on interior faces,
