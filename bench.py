@@ -296,8 +296,15 @@ def run_ours(args, world, rank, local):
         if err is not None:
             line["max_rel_err_vs_fp64"] = err  # first step vs the FP64 plain path (bit-exact to the oracle)
             line["mass_drift"] = {"value": drift, "steps": 1 + args.warmup + args.steps}
-        print(json.dumps(line), flush=True)
     ctx.close()
+    if rank == 0 and world == 1 and not args.no_adjoint and args.mode == "fast":
+        runner = st = f = None
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+        line["adjoint"] = measure_adjoint(args, local, fast_ms=ms)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 UNEVEN = ((7, 96, 40), (6, 42, 12))  # (glevel, kall, tracers) of the two instances
@@ -414,6 +421,83 @@ def run_uneven(args, world, rank, local):
         c.close()
 
 
+def measure_adjoint(args, local, fast_ms=None, steps=12, every=4):
+    """Adjoint of the plain FP64 step over a checkpointed run, on this GPU alone: the FP64
+    forward timed over `steps` steps, then ica_adjoint_record (the same steps, a checkpoint
+    every `every`) and ica_adjoint_sweep (segments recomputed from their checkpoints and
+    transposed step by step), each timed with CUDA events on the context stream.  The adjoint
+    is seeded with J = sum of squared q over region 0, levels 10-20."""
+    import torch
+
+    from icoatmosbenchmark_v1_b200 import api
+    from icoatmosbenchmark_v1_b200 import fields as F
+    from icoatmosbenchmark_v1_b200.grid import Grid, default_dt
+
+    dev = torch.device("cuda", local)
+    g = Grid(args.glevel, 0, args.kall)
+    dt = default_dt(args.glevel)
+    f = F.make_fields(g, device=dev)
+    st = F.make_state(g, args.ntr, "mixed", device=dev, fields=f)
+    del f["rhog"], f["rhog_pl"]
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()  # temporaries of the state set-up
+    ctx = api.IcoAdv(args.glevel, 0, args.kall - 2, device=local)
+    ctx.set_grid(g)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    a = {k: torch.zeros_like(v) for k, v in st.items()}
+    aw = {k: torch.zeros_like(f[k]) for k in api.WIND_KEYS}
+    kr = slice(9, 20)  # levels 10-20
+
+    def seed():
+        for v in a.values():
+            v.zero_()
+        q = st["rhogq"][:, 0, kr] / st["rhog"][None, 0, kr]
+        a["rhogq"][:, 0, kr] = 2 * q / st["rhog"][None, 0, kr]
+        a["rhog"][0, kr] = -(2 * q * q / st["rhog"][None, 0, kr]).sum(0)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def fwd(n):
+        for _ in range(n):
+            ctx.advect_step(dt, st["rhog"], st["rhog_pl"], st["rhogq"], st["rhogq_pl"], f["rhogvx"], f["rhogvx_pl"],
+                            f["rhogvy"], f["rhogvy_pl"], f["rhogvz"], f["rhogvz_pl"], f["rhogw"], f["rhogw_pl"])
+
+    fwd(1)  # warm
+    # warm the adjoint: allocates the scratch and the segment states
+    ctx.adjoint_record(dt, every, every, st, f)
+    seed()
+    ctx.adjoint_sweep(f, a, aw)
+    t_fwd = timed(lambda: fwd(steps))
+    t_rec = timed(lambda: ctx.adjoint_record(dt, steps, every, st, f))
+    seed()
+    n1 = ctx.launch_count
+    t_sweep = timed(lambda: ctx.adjoint_sweep(f, a, aw))
+    launches = ctx.launch_count - n1
+    free_gb = torch.cuda.mem_get_info(dev)[0] / 1e9
+    finite = all(bool(torch.isfinite(v.sum()).item()) for v in (a["rhogq"], a["rhog"], aw["rhogvx"], aw["rhogvy"],
+                                                                 aw["rhogvz"]))
+    ctx.adjoint_release()
+    ctx.close()
+    del st, f, a, aw
+    torch.cuda.empty_cache()
+    out = {"workload": f"gl{args.glevel}_k{args.kall}_t{args.ntr}: {steps}-step sweep, checkpoint every {every}",
+           "objective": "sum of squared q over region 0, levels 10-20", "dtype": "f64",
+           "forward_fp64_ms_per_step": t_fwd / steps, "record_ms": t_rec, "sweep_ms": t_sweep,
+           "sweep_ms_per_step": t_sweep / steps, "ratio_vs_fp64_forward": t_sweep / t_fwd,
+           "gpu_launches_sweep": launches, "gradients_finite": finite,
+           "device_free_gb_during_sweep": round(free_gb, 1)}
+    if fast_ms:
+        out["ratio_vs_batched_forward"] = t_sweep / (steps * fast_ms)
+    return out
+
+
 def measure_e2e(args, ctx, g, st, f, dt, upd, world):
     """Per step: pinned host -> device copy of the state and fields, the step, device -> host copy of
     the state, all inside one host-pointer C ABI call (ica_advect_step / ica_advect_fast)."""
@@ -454,8 +538,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["fast", "plain", "uneven"], default="fast",
-                    help="fast: batched step (headline); plain: FP64 per-tracer path; uneven: batch of two grid levels")
+    ap.add_argument("--mode", choices=["fast", "plain", "uneven", "adjoint"], default="fast",
+                    help="fast: batched step (headline, followed by the adjoint sweep); plain: FP64 per-tracer "
+                         "path; uneven: batch of two grid levels; adjoint: the adjoint sweep alone")
     ap.add_argument("--glevel", type=int, default=8)
     ap.add_argument("--kall", type=int, default=96)
     ap.add_argument("--ntr", type=int, default=32)
@@ -464,6 +549,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true", help="skip the error / mass-drift check")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint sweep measurement")
     ap.add_argument("--tile-shape", type=int, default=-1, help="tile shape index of the horizontal kernel (default: autotune)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")
@@ -474,6 +560,11 @@ def main():
             run_reference_arm(args, world, rank)
         elif args.mode == "uneven":
             run_uneven(args, world, rank, local)
+        elif args.mode == "adjoint":
+            import torch
+            torch.cuda.set_device(local)
+            if rank == 0:
+                print(json.dumps({"adjoint": measure_adjoint(args, local)}), flush=True)
         else:
             run_ours(args, world, rank, local)
     finally:
