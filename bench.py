@@ -302,7 +302,8 @@ def run_ours(args, world, rank, local):
         import gc
         gc.collect()
         torch.cuda.empty_cache()
-        line["adjoint"] = measure_adjoint(args, local, fast_ms=ms)
+        line["adjoint"] = measure_adjoint(args, local, fast_ms=ms, steps=args.adjoint_steps,
+                                          every=args.adjoint_every)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -550,6 +551,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true", help="skip the error / mass-drift check")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint sweep measurement")
+    ap.add_argument("--adjoint-steps", type=int, default=12, help="steps of the adjoint sweep")
+    ap.add_argument("--adjoint-every", type=int, default=4, help="checkpoint interval of the adjoint sweep")
     ap.add_argument("--tile-shape", type=int, default=-1, help="tile shape index of the horizontal kernel (default: autotune)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")
@@ -564,7 +567,8 @@ def main():
             import torch
             torch.cuda.set_device(local)
             if rank == 0:
-                print(json.dumps({"adjoint": measure_adjoint(args, local)}), flush=True)
+                print(json.dumps({"adjoint": measure_adjoint(args, local, steps=args.adjoint_steps,
+                                                             every=args.adjoint_every)}), flush=True)
         else:
             run_ours(args, world, rank, local)
     finally:

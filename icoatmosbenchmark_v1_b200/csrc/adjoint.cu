@@ -355,6 +355,69 @@ __global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const doubl
 }
 
 // ---------------------------------------------------------------------------
+// Forward recompute of rhogq after the horizontal sub-step, Qh = Q - sum_m flx(m) qa(m),
+// with each face's limited value formed from the pre-limit remap value in the
+// same operation sequence as the limiter apply (mod_src_tracer.f90:378-410), so
+// Qh equals the forward step's value bit for bit without storing the limited faces.
+__device__ __forceinline__ double limited_face(const Dims &D, const double *qs, const double *qa0,
+                                               const double *qo, const double *cm, size_t off, size_t fs, int oi,
+                                               int oj, int a, bool sgp) {
+  const int G = D.gall_1d, o = (oj - 1) * G + oi - 1;
+  const int nb = (a == 1) ? o + 1 : ((a == 2) ? o + G + 1 : o + G);
+  int p[4];
+  face_points(D, oi, oj, a, sgp, p);
+  const double lo = mn(mn(mn(qs[p[0]], qs[p[1]]), qs[p[2]]), qs[p[3]]);
+  const double hi = mx(mx(mx(qs[p[0]], qs[p[1]]), qs[p[2]]), qs[p[3]]);
+  const double cc = cm[(size_t)(a - 1) * fs + off + o];
+  const double own_min = cc * lo + (1.0 - cc) * kBig, own_max = cc * hi + (1.0 - cc) * (-kBig);
+  const double nb_min = cc * kBig + (1.0 - cc) * lo, nb_max = cc * (-kBig) + (1.0 - cc) * hi;
+  double v = qa0[(size_t)(a - 1) * fs + off + o];
+  v = cc * mn(mx(v, own_min), own_max) + (1.0 - cc) * mn(mx(v, nb_min), nb_max);
+  const double on_max = qo[fs + off + nb], on_min = qo[off + nb];
+  const double os_max = qo[fs + off + o], os_min = qo[off + o];
+  return cc * mx(mn(v, on_max), on_min) + (1.0 - cc) * mx(mn(v, os_max), os_min);
+}
+
+__global__ void k_adj_qh(Dims D, const double *__restrict__ q, const double *__restrict__ qa0,
+                         const double *__restrict__ qo, const double *__restrict__ cm,
+                         const double *__restrict__ flx, const double *__restrict__ Q, double *Qh) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= D.gall) return;
+  const int kl = blockIdx.y, l = kl / D.kall, G = D.gall_1d;
+  const int i = c % G + 1, j = c / G + 1;
+  if (!inner(D, i, j)) return;
+  const size_t off = (size_t)kl * D.gall, fs = (size_t)D.lall * D.kall * D.gall;
+  const bool sgp = D.have_sgp[l] != 0;
+  const double *qs = q + off;
+  // faces 1..3 are owned by (i,j); 4..6 by (i-1,j), (i-1,j-1), (i,j-1) as their faces 1..3
+  const int oi[6] = {i, i, i, i - 1, i - 1, i}, oj[6] = {j, j, j, j, j - 1, j - 1};
+  double s = flx[off + c] * limited_face(D, qs, qa0, qo, cm, off, fs, oi[0], oj[0], 1, sgp);
+  for (int m = 1; m < 6; ++m)
+    s = s + flx[(size_t)m * fs + off + c] * limited_face(D, qs, qa0, qo, cm, off, fs, oi[m], oj[m], m % 3 + 1, sgp);
+  Qh[off + c] = Q[off + c] - s;
+}
+
+// pole centres (mod_src_tracer.f90:412-425 with the Qin bounds kept by the Qout pass)
+__global__ void k_adj_qh_pl(int kall, const double *qa0_pl, const double *cm_pl, const double *qo_pl,
+                            const double *qin_pl, const double *flx_pl, const double *Qp, double *Qh_pl) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= kLallPl * kall) return;
+  const size_t off = (size_t)t * kGallPl, fsp = (size_t)kLallPl * kall * kGallPl;
+  double s = 0.0;
+  for (int v = 2; v <= 6; ++v) {
+    const double c = cm_pl[off + v - 1];
+    double x = qa0_pl[off + v - 1];
+    const double i1min = qin_pl[0 * fsp + off + v - 1], i2min = qin_pl[1 * fsp + off + v - 1];
+    const double i1max = qin_pl[2 * fsp + off + v - 1], i2max = qin_pl[3 * fsp + off + v - 1];
+    x = c * mn(mx(x, i1min), i1max) + (1.0 - c) * mn(mx(x, i2min), i2max);
+    x = c * mx(mn(x, qo_pl[fsp + off + v - 1]), qo_pl[off + v - 1]) +
+        (1.0 - c) * mx(mn(x, qo_pl[fsp + off]), qo_pl[off]);
+    s = (v == 2) ? flx_pl[off + v - 1] * x : s + flx_pl[off + v - 1] * x;
+  }
+  Qh_pl[off] = Qp[off] - s;
+}
+
+// ---------------------------------------------------------------------------
 // One face (owner (i,j), a = 1..3): the horizontal update, the limiter apply
 // (mod_src_tracer.f90:378-410) and the upwind remap, transposed together.
 __global__ void k_adj_face(Dims D, const double *__restrict__ q, const double *__restrict__ qa0,
@@ -937,12 +1000,8 @@ int step_adjoint(StepCtx &S, const AdjScratch &A, int ntr, double dt, const doub
     launch_remap(S, st);
     launch_hlim_qout<double>(D, lin, S.qout, S.qout_pl, S.qin_pl, st);
     launch_gather<double>(D, S.plan.n, S.plan.dst, S.plan.src, D.kall, 2, S.qout, S.qout_pl, st);
-    cudaMemcpyAsync(A.qa1, S.qa, 6 * n3 * B, cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(A.qa1_pl, S.qa_pl, n3p * B, cudaMemcpyDeviceToDevice, st);
-    launch_hlim_apply<double>(D, lin, A.qa1, A.qa1_pl, S.qout, S.qout_pl, S.qin_pl, st);
-    cudaMemcpyAsync(A.Qh, Q, n3 * B, cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(A.Qh_pl, Qp, n3p * B, cudaMemcpyDeviceToDevice, st);
-    launch_update_h(S, A.qa1, A.qa1_pl, A.Qh, A.Qh_pl, st);
+    k_adj_qh<<<slab(D, T), T, 0, st>>>(D, S.q, S.qa, S.qout, S.cm, S.flx, Q, A.Qh);
+    k_adj_qh_pl<<<nbl, 128, 0, st>>>(D.kall, S.qa_pl, S.cm_pl, S.qout_pl, S.qin_pl, S.flx_pl, Qp, A.Qh_pl);
     // vertical sub-step: aQ becomes the adjoint of rhogq after the horizontal sub-step
     k_adj_vert<<<(ncol + 127) / 128, 128, 0, st>>>(D, dt, A.Qh, A.rh, w, aQ, A.a_rh, A.Qh_pl, A.rh_pl, w_pl, aQp,
                                                    A.a_rh_pl, S.rdgz, S.afact, S.bfact);
@@ -966,7 +1025,7 @@ int step_adjoint(StepCtx &S, const AdjScratch &A, int ntr, double dt, const doub
     k_adj_div<<<(unsigned)((n3 + n3p + 255) / 256), 256, 0, st>>>((long long)n3, (int)n3p, A.a_q, S.q, rhog,
                                                                   A.a_q_pl, S.q_pl, rhog_pl, aQ, aQp, a_rhog,
                                                                   a_rhog_pl);
-    launches += 29;
+    launches += 27;
   }
   // ---- density update and Courant numbers, then horizontal_flux
   k_adj_rhoh_ch<<<slab(D, T), T, 0, st>>>(D, rhog, S.ch, A.a_rh, A.a_ch, A.a_flx, a_rhog);
