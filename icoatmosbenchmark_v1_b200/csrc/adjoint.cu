@@ -194,8 +194,9 @@ __device__ __forceinline__ void vlim_level_adj(const VLim &v, double qm, double 
   const double CQmax = v.infL * c1 * v.mxL + v.infU * c2 * v.mxU;
   const double CQmin = v.infL * c1 * v.mnL + v.infU * c2 * v.mnU;
   const double Nmn = (qk - v.qnmax) + v.qnmax * S - CQmax, Nmx = (qk - v.qnmin) + v.qnmin * S - CQmin;
-  const double aNmn = aQm / Dn, aNmx = aQx / Dn;
-  const double aD = -(aQm * Nmn + aQx * Nmx) / (Dn * Dn);
+  const double rD = 1.0 / Dn;
+  const double aNmn = aQm * rD, aNmx = aQx * rD;
+  const double aD = -(aNmn * Nmn + aNmx * Nmx) * rD;
   double a_qk = aNmn + aNmx;
   const double a_qnmax = aNmn * (S - 1.0), a_qnmin = aNmx * (S - 1.0);
   const double aS = aNmn * v.qnmax + aNmx * v.qnmin;
@@ -230,10 +231,12 @@ __device__ __forceinline__ void vlim_level_adj(const VLim &v, double qm, double 
   ac2 += a2;
 }
 
-__global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const double *Qh, const double *rh,
-                                                  const double *w, double *aQ, double *a_rh, const double *Qh_pl,
-                                                  const double *rh_pl, const double *w_pl, double *aQ_pl,
-                                                  double *a_rh_pl, const double *__restrict__ rdgz,
+__global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const double *__restrict__ Qh,
+                                                  const double *__restrict__ rh, const double *__restrict__ w,
+                                                  double *__restrict__ aQ, double *__restrict__ a_rh,
+                                                  const double *__restrict__ Qh_pl, const double *__restrict__ rh_pl,
+                                                  const double *__restrict__ w_pl, double *__restrict__ aQ_pl,
+                                                  double *__restrict__ a_rh_pl, const double *__restrict__ rdgz,
                                                   const double *__restrict__ afact,
                                                   const double *__restrict__ bfact) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,13 +277,13 @@ __global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const doubl
     }
     return v;
   };
-  // window: levels k+1 (P), k (Z), k-1 (M), k-2 (M2)
+  // window: levels k+1 (P), k (Z), k-1 (M), k-2 (M2); the Thuburn bounds of a level are
+  // recomputed where they are needed instead of carried, which keeps the thread's state small
   VLev P{}, Z = level(K), M = level(K - 1), M2{};
-  VLim LZ{}, LM{};
   double aQmZ = 0.0, aQxZ = 0.0, aQmM = 0.0, aQxM = 0.0;  // adjoints of the Qout bounds of k, k-1
   double accP = 0.0, accZ = 0.0, accM = 0.0;             // limiter adjoints into qc(k+1), qc(k), qc(k-1)
-  double ac1P = 0.0, ac2P = 0.0, ac1Z = 0.0, ac2Z = 0.0;  // adjoints of ck1, ck2 of k+1, k
-  double ahP2 = 0.0, ahP = 0.0, ahZ = 0.0;                // post-clamp adjoints of qh(k+2), qh(k+1), qh(k)
+  double ac1P = 0.0, ac2P = 0.0;                          // adjoints of ck1, ck2 of level k+1
+  double ahP2 = 0.0, ahP = 0.0;                           // post-clamp adjoints of qh(k+2), qh(k+1)
   double aqcTop = 0.0;                                    // adjoint of the ghost qc(kall)
   for (int k = K; k >= kmin; --k) {
     if (k - 2 >= 1) M2 = level(k - 2);
@@ -292,28 +295,34 @@ __global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const doubl
       const double t2 = hi ? Z.aO * Z.w * dt * rdgz[k - 1] : 0.0;
       ah = (lo && hi) ? t1 + t2 : (lo ? t1 : t2);
     }
-    if (k - 1 >= kmin) LM = vlim_level(M2.qc, M.qc, Z.qc, M.c1, Z.c1, M.c2);
-    // the clamp of qh(k) to the bounds of level k-1 (inflow from below) or k
-    if (k >= kmin + 1 && k <= kmax) {
-      const bool below = (LZ.infL != 0.0);
-      const double Qmx = below ? LM.Qmx : LZ.Qmx, Qmn = below ? LM.Qmn : LZ.Qmn;
-      const double h = afact[k - 1] * Z.qc + bfact[k - 1] * M.qc;
-      const double m1 = mn(h, Qmx);
-      int sel = (Qmx < h) ? 1 : 0;
-      if (Qmn > m1) sel = 2;
-      if (sel == 1) {
-        if (below) aQxM += ah;
-        else aQxZ += ah;
-        ah = 0.0;
-      } else if (sel == 2) {
-        if (below) aQmM += ah;
-        else aQmZ += ah;
-        ah = 0.0;
+    double ac1Z = 0.0, ac2Z = 0.0;
+    if (k <= kmax) {
+      const VLim LZ = vlim_level(M.qc, Z.qc, P.qc, Z.c1, P.c1, Z.c2);
+      // the clamp of qh(k) to the bounds of level k-1 (inflow from below) or k
+      if (k >= kmin + 1) {
+        const bool below = (LZ.infL != 0.0);
+        double Qmx = LZ.Qmx, Qmn = LZ.Qmn;
+        if (below) {
+          const VLim LM = vlim_level(M2.qc, M.qc, Z.qc, M.c1, Z.c1, M.c2);
+          Qmx = LM.Qmx, Qmn = LM.Qmn;
+        }
+        const double h = afact[k - 1] * Z.qc + bfact[k - 1] * M.qc;
+        const double m1 = mn(h, Qmx);
+        int sel = (Qmx < h) ? 1 : 0;
+        if (Qmn > m1) sel = 2;
+        if (sel == 1) {
+          if (below) aQxM += ah;
+          else aQxZ += ah;
+          ah = 0.0;
+        } else if (sel == 2) {
+          if (below) aQmM += ah;
+          else aQmZ += ah;
+          ah = 0.0;
+        }
       }
+      // Qout bounds of level k
+      vlim_level_adj(LZ, M.qc, Z.qc, P.qc, aQmZ, aQxZ, accM, accZ, accP, ac1Z, ac2Z);
     }
-    ahZ = ah;
-    // Qout bounds of level k
-    if (k <= kmax) vlim_level_adj(LZ, M.qc, Z.qc, P.qc, aQmZ, aQxZ, accM, accZ, accP, ac1Z, ac2Z);
     // level k+1 is complete
     if (k + 1 == K) {
       aqcTop = accP + afact[K - 1] * ahP;
@@ -322,19 +331,19 @@ __global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const doubl
       a += afact[k] * ahP;
       a += bfact[k + 1] * ahP2;
       if (k + 1 == kmax) a += aqcTop;
-      AQ[X(k + 1)] = P.aO + a / P.R;
+      const double rR = 1.0 / P.R;
+      AQ[X(k + 1)] = P.aO + a * rR;
       double r = ARH[X(k + 1)];
-      r += -a * P.qc / P.R;
-      r += -(ac1P * P.c1 + ac2P * P.c2) / P.R;
+      r += -a * P.qc * rR;
+      r += -(ac1P * P.c1 + ac2P * P.c2) * rR;
       ARH[X(k + 1)] = r;
     }
     // shift the window down one level
     P = Z, Z = M, M = M2;
-    LZ = LM;
     aQmZ = aQmM, aQxZ = aQxM, aQmM = aQxM = 0.0;
     accP = accZ, accZ = accM, accM = 0.0;
-    ac1P = ac1Z, ac2P = ac2Z, ac1Z = ac2Z = 0.0;
-    ahP2 = ahP, ahP = ahZ;
+    ac1P = ac1Z, ac2P = ac2Z;
+    ahP2 = ahP, ahP = ah;
   }
   // level kmin (now P) with the ghost qc(1) (now Z's accumulator)
   {
@@ -344,10 +353,11 @@ __global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const doubl
     a += bfact[kmin] * ahP2;
     if (kmin == kmax) a += aqcTop;
     a += aqcBot;
-    AQ[X(kmin)] = P.aO + a / P.R;
+    const double rR = 1.0 / P.R;
+    AQ[X(kmin)] = P.aO + a * rR;
     double r = ARH[X(kmin)];
-    r += -a * P.qc / P.R;
-    r += -(ac1P * P.c1 + ac2P * P.c2) / P.R;
+    r += -a * P.qc * rR;
+    r += -(ac1P * P.c1 + ac2P * P.c2) * rR;
     ARH[X(kmin)] = r;
   }
   AQ[X(1)] = 0.0;
