@@ -304,7 +304,7 @@ def run_ours(args, world, rank, local):
             line["mass_drift"] = {"value": drift, "steps": 1 + args.warmup + args.steps}
     ctx.close()
     if rank == 0 and world == 1 and not args.no_adjoint and args.mode == "fast":
-        runner = st = f = None
+        runner = st = f = step = None  # the bound step method holds the runner and its buffers
         import gc
         gc.collect()
         torch.cuda.empty_cache()
