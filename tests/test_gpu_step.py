@@ -22,7 +22,8 @@ def _ctx(grid):
     return ctx
 
 
-@pytest.mark.parametrize("glevel,rlevel,kall,ntr,nsteps", [(5, 0, 42, 2, 3), (4, 1, 10, 3, 2), (3, 0, 6, 1, 4)])
+@pytest.mark.parametrize("glevel,rlevel,kall,ntr,nsteps",
+                         [(5, 0, 42, 8, 10), (5, 0, 42, 2, 3), (4, 1, 10, 3, 2), (3, 0, 6, 1, 4)])
 def test_plain_step_bit_exact(O, glevel, rlevel, kall, ntr, nsteps):
     c = case(glevel, rlevel, kall, ntr)
     g, f = c["grid"], c["fields"]
