@@ -66,8 +66,10 @@ __device__ __forceinline__ int find_inst(const MultiInst &M, long long &w, F cnt
 __device__ __forceinline__ double fsg(double a, double b) { return copysign(fabs(a), b); }
 __device__ __forceinline__ double mn64(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double mx64(double a, double b) { return (b > a) ? b : a; }
-__device__ __forceinline__ float mn32(float a, float b) { return (b < a) ? b : a; }
-__device__ __forceinline__ float mx32(float a, float b) { return (b > a) ? b : a; }
+// FP32 min / max: one FMNMX instruction each (the select form takes a compare and a select).
+// Operands here are never NaN; for them the two agree except for the sign of a zero result.
+__device__ __forceinline__ float mn32(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ float mx32(float a, float b) { return fmaxf(a, b); }
 
 // geometry readers (region coords i,j 1-based)
 __device__ __forceinline__ double gt(const FastInst &I, int l, int i, int j, int t, int w) {
