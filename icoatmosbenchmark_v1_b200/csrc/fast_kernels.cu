@@ -582,23 +582,29 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     }
     asm volatile("cp.async.commit_group;\n" ::);
   };
-  issue(0, 0);
-  for (int t0 = 0, b = 0; t0 < ntr; t0 += TB, ++b) {
-    const int ntg = min(TB, ntr - t0);
-    asm volatile("cp.async.wait_group 0;\n" ::);  // this thread's copies of batch b have landed
-    __syncthreads();
-    // ---- (A) q of the batch's tracers in the window x, y in [-2, T+1]
+  // q of the batch starting at tracer tb from stage[buf] (window x, y in [-2, T+1])
+  auto load_q = [&](int tb, int buf) {
+    const int nb = min(TB, ntr - tb);
 #pragma unroll
     for (int tt = 0; tt < TB; ++tt)
 #pragma unroll
       for (int r = 0; r < NSLOT; ++r) {
         const int e = tid + r * NT;
-        if (e < NW) s.q[tt][sq[r]] = (sok[r] && tt < ntg) ? (float)(s.stage[b & 1][tt][e] * s.rinv[e]) : 0.0f;
+        if (e < NW) s.q[tt][sq[r]] = (sok[r] && tt < nb) ? (float)(s.stage[buf][tt][e] * s.rinv[e]) : 0.0f;
       }
-    __syncthreads();
-    // the next batch's window streams in during this batch's work (its buffer was last
-    // read by the previous batch's update, which every thread has finished here)
-    if (t0 + TB < ntr) issue(t0 + TB, (b + 1) & 1);
+  };
+  // Per batch b: (B) gradient + Qout, (C) face values, then (D) the update of batch b
+  // together with (A) q of batch b+1, whose rhogq window streamed in during B and C.
+  // Three barriers per batch.
+  issue(0, 0);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+  // ---- (A) q of the first batch
+  load_q(0, 0);
+  __syncthreads();
+  if (TB < ntr) issue(TB, 1);
+  for (int t0 = 0, b = 0; t0 < ntr; t0 += TB, ++b) {
+    const int ntg = min(TB, ntr - t0);
     // ---- (B) gradient and Qout of the ring cells
     if (in_arr) {
       if (bs >= 0) {  // region-boundary cell or halo cell: the FP64 boundary values
@@ -703,6 +709,7 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
         }
       }
     }
+    asm volatile("cp.async.wait_group 0;\n" ::);  // this thread's copies of batch b+1 have landed
     __syncthreads();
     // ---- (D) horizontal update of the tile cells (FP64): rhogq after the horizontal sub-step
     if (active) {
@@ -719,6 +726,10 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
         I.Q_out[o] = Qin - sum;
       }
     }
+    // ---- (A) q of the next batch; then its buffer's successor streams in
+    if (t0 + TB < ntr) load_q(t0 + TB, (b + 1) & 1);
+    __syncthreads();
+    if (t0 + 2 * TB < ntr) issue(t0 + 2 * TB, b & 1);
   }
 }
 
