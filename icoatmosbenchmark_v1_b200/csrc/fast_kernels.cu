@@ -500,17 +500,17 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
 #pragma unroll
   for (int n = 0; n < 21; ++n) cgr[n] = fp32_cell ? I.cg32[((size_t)l * 21 + n) * I.gall + ccell] : 0.0f;
   if (fp32_cell) {
-    const float rc = s.rho[ec];
+    const float rcinv = (float)s.rinv[ec];  // Courant numbers by the reciprocal of rho (one division per cell)
     float ch[7];
 #pragma unroll
     for (int m = 1; m <= 6; ++m) {
       const float Fm = (float)s.F[(m - 1) % 3][nbe[m]];
-      ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) / rc;
+      ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) * rcinv;
       chm[m] = mn32(ch[m], 0.0f);
       float chown = ch[m];
-      if (m >= 4) {  // the owner's own Courant number of this face
+      if (m >= 4) {  // the owner's own Courant number of this face, as the owner forms it
         const int oi = (m == 6) ? ci : ci - 1, oj = (m == 4) ? cj : cj - 1;
-        chown = (Fm * (float)rarea(I, l, oi, oj) * dtf) / s.rho[nbe[m]];
+        chown = (Fm * (float)rarea(I, l, oi, oj) * dtf) * (float)s.rinv[nbe[m]];
       }
       const float cm = 0.5f - copysignf(0.5f, chown - EPSf);
       const bool in = (m <= 3) ? (cm != 0.0f) : (cm == 0.0f);
@@ -528,7 +528,7 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     dup[a][0] = dup[a][1] = dup[a][2] = 0.0f;
     if (owner && c_int) {
       const float Fa = (float)s.F[a][ec];
-      const float chown = (Fa * ra32 * dtf) / s.rho[ec];
+      const float chown = (Fa * ra32 * dtf) * (float)s.rinv[ec];
       const bool cm = (0.5f - copysignf(0.5f, chown - EPSf)) != 0.0f;
       cmown |= cm ? (1u << a) : 0u;
 #pragma unroll
@@ -549,8 +549,9 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     const double rho_h = I.rho_in[base + ccell] - sum;
     I.rho_out[base + ccell] = rho_h;
     const float wk = I.w[base + ccell], wk1 = I.w[base + slab + ccell];
-    I.vco[base + ccell] = make_float4((float)(-(double)wk * dt * I.rdgz[k] / rho_h),
-                                      (float)((double)wk1 * dt * I.rdgz[k] / rho_h), (float)(1.0 / rho_h), wk);
+    const double rhinv = 1.0 / rho_h;
+    I.vco[base + ccell] = make_float4((float)(-(double)wk * dt * I.rdgz[k] * rhinv),
+                                      (float)((double)wk1 * dt * I.rdgz[k] * rhinv), (float)rhinv, wk);
   }
 
   // the window slots of this thread (e = tid + r*NT): global offset in the level, q slot
