@@ -362,7 +362,7 @@ class FastRunner:
         self.b = {k: torch.empty_like(v) for k, v in state.items()}
         self.f32 = {k: fields[k].to(torch.float32).contiguous() for k in FIELD_KEYS}
         self.updates = (10 * 4 ** grid.glevel + 2) * grid.kall * state["rhogq"].shape[0]
-        # k_fast_horiz per tracer cell-level: rhogq read + write (FP64); per cell-level, shared by
+        # horizontal sub-step per tracer cell-level: rhogq read + write (FP64); per cell-level, shared by
         # the tracers: rhog read + write (FP64), rhogv x/y/z + rhogw (FP32), vertical inputs (16 B)
         self.alg_bytes = 16.0 + 48.0 / state["rhogq"].shape[0]
         self.shape = 0
@@ -404,11 +404,13 @@ class FastRunner:
         self.ctx.fast_timing(1)
 
     def kernel_stats(self):
-        """Average CUDA-event duration of the horizontal kernel over the steps since start_timing()."""
+        """Average CUDA-event duration of the horizontal sub-step (the face-flux prologue
+        k_fast_faces and the tile kernel k_fast_horiz, timed together) over the steps since
+        start_timing()."""
         ms, n = self.ctx.fast_timing(0)
         if n == 0:
             return None
-        return {"name": "k_fast_horiz", "ms_per_launch": ms / n, "launches": n,
+        return {"name": "k_fast_faces+k_fast_horiz", "ms_per_launch": ms / n, "launches": n,
                 "bytes_per_launch": self.updates * self.alg_bytes}
 
 

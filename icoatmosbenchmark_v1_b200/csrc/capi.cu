@@ -938,6 +938,10 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
   if (!I.sflux || !I.sval) return set_error("cudaMalloc(fast seam buffers)"), ICA_ERR_NOMEM;
   I.vco = (float4 *)buf("fast_vco", (size_t)sz.lall * sz.kall * sz.gall * sizeof(float4));
   if (!I.vco) return set_error("cudaMalloc(fast vertical coefficients)"), ICA_ERR_NOMEM;
+  const size_t n3 = (size_t)sz.lall * sz.kall * sz.gall;
+  I.Fg = (double *)buf("fast_Fg", 3 * n3 * sizeof(double));
+  I.Dg = (float *)buf("fast_Dg", 9 * n3 * sizeof(float));
+  if (!I.Fg || !I.Dg) return set_error("cudaMalloc(fast face fluxes)"), ICA_ERR_NOMEM;
   I.work_next = (unsigned long long *)buf("fast_work_next", sizeof(unsigned long long));
   if (!I.work_next) return set_error("cudaMalloc(fast work counter)"), ICA_ERR_NOMEM;
   return ICA_OK;

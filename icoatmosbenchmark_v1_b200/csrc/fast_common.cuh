@@ -39,6 +39,8 @@ struct FastInst {
   double *sflux;  // (K, ns): 0.5 (rhov . HN) of the seam faces
   float *sval;    // (ntr, K, ns): limited face values of the seam faces
   double *bbuf;  // (ntr, K, nb, 5): grad x, y, z, Qout min, Qout max
+  double *Fg;    // (3, lall, K, gall): face flux 0.5 (rhov . HN) of the 3 faces of each owner, per step
+  float *Dg;     // (9, lall, K, gall): face a, component c at a*3+c: -rhov rr dt / 2 (GRD_xc - GRD_xr)
   float4 *vco;   // (lall, K, gall): ck(k,1), ck(k,2), 1/rhog, rhogw(k) after the horizontal sub-step
   unsigned long long *work_next;  // work-item counter of the persistent horizontal kernel
 };

@@ -299,6 +299,69 @@ __global__ void k_fast_offsets(FastInst I, float *off) {
   }
 }
 
+// Face fluxes and centroid displacements of every owner cell and level, once per step
+// (dyn_horiz_adv_flux/src/mod_src_tracer.f90:141-309): FP32 triangle values and faces
+// between interior cells, the FP64 value of k_fast_seam on seam faces, zero where the
+// reference has no face.  One thread per (owner cell, level); every tile that needs a
+// face reads this one value, so its two cells see the same flux.
+__global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
+  long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int ii = find_inst(M, w, [](const FastInst &I) { return (long long)I.lall * (I.K - 2) * I.gall; });
+  if (ii < 0) return;
+  const FastInst &I = M.inst[ii];
+  const int G = I.G, c = (int)(w % I.gall);
+  const int lk = (int)(w / I.gall), k = 1 + lk % (I.K - 2), l = lk / (I.K - 2);
+  const int i = c % G + 1, j = c / G + 1;
+  const size_t n3 = (size_t)I.lall * I.K * I.gall, o = ((size_t)l * I.K + k) * I.gall + c;
+  const float dtf = (float)I.dt;
+  auto interior = [&](int a, int b) { return a >= I.gmin && a <= I.gmax && b >= I.gmin && b <= I.gmax; };
+  // rho, rhovx, rhovy, rhovz (FP32) of cell (a, b) of this slab
+  auto fld = [&](int a, int b, float f[4]) {
+    const size_t q = ((size_t)l * I.K + k) * I.gall + (size_t)(b - 1) * G + (a - 1);
+    f[0] = (float)I.rho_in[q], f[1] = I.vx[q], f[2] = I.vy[q], f[3] = I.vz[q];
+  };
+  // triangle TI (t = 0: cells (a,b), (a+1,b), (a+1,b+1)) or TJ (t = 1: (a,b), (a+1,b+1), (a,b+1))
+  auto tri = [&](int a, int b, int t, float v[4]) {
+    const float w1 = (float)gt(I, l, a, b, t + 1, W1), w2 = (float)gt(I, l, a, b, t + 1, W2),
+                w3 = (float)gt(I, l, a, b, t + 1, W3);
+    float f0[4], f1[4], f2[4];
+    fld(a, b, f0);
+    fld(a + 1, b + 1, t == 0 ? f2 : f1);
+    if (t == 0) fld(a + 1, b, f1);
+    else fld(a, b + 1, f2);
+#pragma unroll
+    for (int x = 0; x < 4; ++x) v[x] = f0[x] * w1 + f1[x] * w2 + f2[x] * w3;
+  };
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double F = 0.0;
+    float d[3] = {0.0f, 0.0f, 0.0f};
+    if (i < G && j < G && face_exists(I, i, j, a + 1)) {
+      const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
+      if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64 flux of k_fast_seam
+        const int sid = I.seam_id[((size_t)l * I.gall + c) * 3 + a];
+        F = I.sflux[(size_t)k * I.ns + sid];
+      } else {  // AI = TJ(i,j-1) + TI(i,j); AIJ = TI(i,j) + TJ(i,j); AJ = TJ(i,j) + TI(i-1,j)
+        float p[4], q[4];
+        if (a == 0) tri(i, j - 1, 1, p), tri(i, j, 0, q);
+        else if (a == 1) tri(i, j, 0, p), tri(i, j, 1, q);
+        else tri(i, j, 1, p), tri(i - 1, j, 0, q);
+        const float vx = p[1] + q[1], vy = p[2] + q[2], vz = p[3] + q[3];
+        const float rr = 1.0f / mx32(p[0] + q[0], FLT_EPSILON);
+        const float Ff = 0.5f * (vx * (float)ga(I, l, i, j, a + 1, HNX) + vy * (float)ga(I, l, i, j, a + 1, HNY) +
+                                 vz * (float)ga(I, l, i, j, a + 1, HNZ));
+        F = (double)Ff;
+        d[0] = -(vx * rr * dtf * 0.5f);
+        d[1] = -(vy * rr * dtf * 0.5f);
+        d[2] = -(vz * rr * dtf * 0.5f);
+      }
+    }
+    I.Fg[(size_t)a * n3 + o] = F;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) I.Dg[(size_t)(a * 3 + x) * n3 + o] = d[x];
+  }
+}
+
 // Threshold of the upwind masks (0.5 - sign(0.5, ch - EPS)) and of the zero-outflow guards
 // (zerosw) in the FP32 arithmetic: the FP64 EPS, not epsilon(1.0).  These are switches, not
 // roundings: with FP32's own EPS a face whose Courant number lies in (2.2e-16, 1.2e-7) is
@@ -356,21 +419,13 @@ template <int TX, int TY, int TB>
 struct TileSmem {
   static constexpr int NT = TileGeo<TX, TY>::NT, NW = TileGeo<TX, TY>::NW;
   double rinv[NW];  // 1 / rho
-  double F[3][NW];  // face flux 0.5 (rhov . HN) by owner (FP32 arithmetic on interior faces)
-  float rho[NW];
-  float v[3][NW];
+  double F[3][NW];  // face flux 0.5 (rhov . HN) by owner, from k_fast_faces
   double stage[2][TB][NW];  // rhogq of the window, FP64, two batches in flight (cp.async)
   float q[TB][TileGeo<TX, TY>::NQ];
-  union {
-    struct {
-      float gq[TB][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
-      float qa[TB][3][NT];  // limited face values of the faces owned by ring cells
-    } t;
-    struct {
-      float tri[2][4][NW];   // rho, rhovx, rhovy, rhovz at TI / TJ
-      float disp[3][3][NW];  // -rhov rr dt / 2 of each face: GRD_xc - GRD_xr
-    } f;
-  } u;
+  struct {
+    float gq[TB][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
+    float qa[TB][3][NT];  // limited face values of the faces owned by ring cells
+  } t;
 };
 
 // one work item (tile, level) of instance I.  I is taken by value and the body inlined once
@@ -410,82 +465,17 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   const double ra64 = c_int ? rarea(I, l, ci, cj) : 1.0;
   const float ra32 = (float)ra64;
 
-  // ---- (0a) fields of this level in the window
-  for (int e = tid; e < NW; e += NT) {
-    const int i = i0 - 3 + e % WW, j = j0 - 3 + e / WW;
-    if (i >= 1 && i <= G && j >= 1 && j <= G) {
-      const size_t o = base + (size_t)(j - 1) * G + (i - 1);
-      const double r = I.rho_in[o];
-      s.rinv[e] = 1.0 / r;
-      s.rho[e] = (float)r;
-      s.v[0][e] = I.vx[o];
-      s.v[1][e] = I.vy[o];
-      s.v[2][e] = I.vz[o];
-    } else {
-      s.rinv[e] = 1.0;
-      s.rho[e] = 1.0f;
-      s.v[0][e] = s.v[1][e] = s.v[2][e] = 0.0f;
-    }
-  }
-  __syncthreads();
-  // ---- (0b) triangle values TI, TJ (dyn_horiz_adv_flux/src/mod_src_tracer.f90:141-201), FP32
-  for (int e = tid; e < NW; e += NT) {
-    const int i = i0 - 3 + e % WW, j = j0 - 3 + e / WW;
-    const bool ok = i >= 1 && j >= 1 && i + 1 <= G && j + 1 <= G;
-    float ti[4] = {0, 0, 0, 0}, tj[4] = {0, 0, 0, 0};
-    if (ok && e % WW + 1 < WW && e / WW + 1 < Gm::WH) {
-      const float a1 = (float)gt(I, l, i, j, TI, W1), a2 = (float)gt(I, l, i, j, TI, W2),
-                  a3 = (float)gt(I, l, i, j, TI, W3);
-      const float b1 = (float)gt(I, l, i, j, TJ, W1), b2 = (float)gt(I, l, i, j, TJ, W2),
-                  b3 = (float)gt(I, l, i, j, TJ, W3);
-      const int e1 = e + 1, e2 = e + WW + 1, e3 = e + WW;
-      ti[0] = s.rho[e] * a1 + s.rho[e1] * a2 + s.rho[e2] * a3;
-      tj[0] = s.rho[e] * b1 + s.rho[e2] * b2 + s.rho[e3] * b3;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        ti[c + 1] = s.v[c][e] * a1 + s.v[c][e1] * a2 + s.v[c][e2] * a3;
-        tj[c + 1] = s.v[c][e] * b1 + s.v[c][e2] * b2 + s.v[c][e3] * b3;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 4; ++c) s.u.f.tri[0][c][e] = ti[c], s.u.f.tri[1][c][e] = tj[c];
-  }
-  __syncthreads();
-  // ---- (0c) face fluxes and centroid displacements of owners x, y in [-2, T]
+  // ---- (0a) 1/rho and the face fluxes (k_fast_faces) of this level in the window
   for (int e = tid; e < NW; e += NT) {
     const int lx = e % WW, ly = e / WW;  // local slot: x = lx - 3
     const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-    const bool own = lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3 && i >= 1 && j >= 1 && i < G && j < G;
+    const bool in = i >= 1 && i <= G && j >= 1 && j <= G;
+    const size_t o = base + (size_t)(j - 1) * G + (i - 1);
+    s.rinv[e] = in ? 1.0 / I.rho_in[o] : 1.0;
+    // owners x, y in [-2, T] are read by the Courant numbers of the ring cells
+    const bool own = in && lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      double F = 0.0;
-      float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
-      if (own && face_exists(I, i, j, a + 1)) {
-        const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
-        if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64 flux of k_fast_seam
-          const int sid = I.seam_id[((size_t)l * I.gall + (size_t)(j - 1) * G + (i - 1)) * 3 + a];
-          F = I.sflux[(size_t)k * I.ns + sid];
-        } else {
-          const int ep = (a == 0) ? e - WW : e, eq = (a == 2) ? e - 1 : e;  // TJ slot, TI slot
-          const int sp = (a == 0) ? 1 : (a == 1 ? 0 : 1), sq = (a == 0) ? 0 : (a == 1 ? 1 : 0);
-          const float pr = s.u.f.tri[sp][0][ep], qr = s.u.f.tri[sq][0][eq];
-          const float vx = s.u.f.tri[sp][1][ep] + s.u.f.tri[sq][1][eq];
-          const float vy = s.u.f.tri[sp][2][ep] + s.u.f.tri[sq][2][eq];
-          const float vz = s.u.f.tri[sp][3][ep] + s.u.f.tri[sq][3][eq];
-          const float rr = 1.0f / mx32(pr + qr, FLT_EPSILON);
-          const float Ff = 0.5f * (vx * (float)ga(I, l, i, j, a + 1, HNX) + vy * (float)ga(I, l, i, j, a + 1, HNY) +
-                                   vz * (float)ga(I, l, i, j, a + 1, HNZ));
-          F = (double)Ff;
-          d0 = -(vx * rr * dtf * 0.5f);
-          d1 = -(vy * rr * dtf * 0.5f);
-          d2 = -(vz * rr * dtf * 0.5f);
-        }
-      }
-      s.F[a][e] = F;
-      s.u.f.disp[a][0][e] = d0;
-      s.u.f.disp[a][1][e] = d1;
-      s.u.f.disp[a][2][e] = d2;
-    }
+    for (int a = 0; a < 3; ++a) s.F[a][e] = own ? I.Fg[(size_t)a * tstride + o] : 0.0;
   }
   __syncthreads();
   // ---- (0d) per ring cell: Courant numbers, masks, outflow sums, gradient coefficients;
@@ -533,7 +523,8 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
       cmown |= cm ? (1u << a) : 0u;
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        dup[a][c] = I.off32[((size_t)l * 18 + a * 6 + (cm ? 3 : 0) + c) * I.gall + ccell] + s.u.f.disp[a][c][ec];
+        dup[a][c] = I.off32[((size_t)l * 18 + a * 6 + (cm ? 3 : 0) + c) * I.gall + ccell] +
+                    I.Dg[(size_t)(a * 3 + c) * tstride + base + ccell];
     }
   }
   double flx[7];
@@ -614,13 +605,13 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
           if (tt >= ntg) break;
           const double *bv = bval(I, t0 + tt, k, bs);
 #pragma unroll
-          for (int c = 0; c < 5; ++c) s.u.t.gq[tt][c][tid] = (float)bv[c];
+          for (int c = 0; c < 5; ++c) s.t.gq[tt][c][tid] = (float)bv[c];
         }
       } else if (!fp32_cell) {  // halo point no list reaches: grad 0, Qout = q
 #pragma unroll
         for (int tt = 0; tt < TB; ++tt) {
-          s.u.t.gq[tt][0][tid] = s.u.t.gq[tt][1][tid] = s.u.t.gq[tt][2][tid] = 0.0f;
-          s.u.t.gq[tt][3][tid] = s.u.t.gq[tt][4][tid] = s.q[tt][eq];
+          s.t.gq[tt][0][tid] = s.t.gq[tt][1][tid] = s.t.gq[tt][2][tid] = 0.0f;
+          s.t.gq[tt][3][tid] = s.t.gq[tt][4][tid] = s.q[tt][eq];
         }
       } else {
         const int st7[7] = {eq, eq + 1, eq + QW + 1, eq + QW, eq - 1, eq - QW - 1, eq - QW};
@@ -658,11 +649,11 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
             CQmin = (m == 1) ? chm[1] * qmn : CQmin + chm[m] * qmn;
             CQmax = (m == 1) ? chm[1] * qmx : CQmax + chm[m] * qmx;
           }
-          s.u.t.gq[tt][0][tid] = g[0];
-          s.u.t.gq[tt][1][tid] = g[1];
-          s.u.t.gq[tt][2][tid] = g[2];
-          s.u.t.gq[tt][3][tid] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
-          s.u.t.gq[tt][4][tid] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
+          s.t.gq[tt][0][tid] = g[0];
+          s.t.gq[tt][1][tid] = g[1];
+          s.t.gq[tt][2][tid] = g[2];
+          s.t.gq[tt][3][tid] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
+          s.t.gq[tt][4][tid] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
         }
       }
     }
@@ -678,7 +669,7 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
         const bool need = (x >= 0 && y >= 0) || (ni - i0 >= 0 && nj - j0 >= 0 && ni - i0 < TX && nj - j0 < TY);
         if (!need || !face_exists(I, ci, cj, a + 1)) {
 #pragma unroll
-          for (int tt = 0; tt < TB; ++tt) s.u.t.qa[tt][a][tid] = 0.0f;
+          for (int tt = 0; tt < TB; ++tt) s.t.qa[tt][a][tid] = 0.0f;
           continue;
         }
         if (!c_int || !interior(ni, nj)) {  // seam face: value of k_fast_seam
@@ -686,7 +677,7 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
 #pragma unroll
           for (int tt = 0; tt < TB; ++tt) {
             if (tt >= ntg) break;
-            s.u.t.qa[tt][a][tid] = I.sval[((size_t)(t0 + tt) * K + k) * I.ns + sid];
+            s.t.qa[tt][a][tid] = I.sval[((size_t)(t0 + tt) * K + k) * I.ns + sid];
           }
           continue;
         }
@@ -695,9 +686,9 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
 #pragma unroll
         for (int tt = 0; tt < TB; ++tt) {
           float v = s.q[tt][us];
-          v = v + s.u.t.gq[tt][0][ut] * dup[a][0];
-          v = v + s.u.t.gq[tt][1][ut] * dup[a][1];
-          v = v + s.u.t.gq[tt][2][ut] * dup[a][2];
+          v = v + s.t.gq[tt][0][ut] * dup[a][0];
+          v = v + s.t.gq[tt][1][ut] * dup[a][1];
+          v = v + s.t.gq[tt][2][ut] * dup[a][2];
           const float c0 = s.q[tt][eq];
           float b1, b2, b3;
           if (a == 0) b1 = s.q[tt][eq - QW], b2 = s.q[tt][eq + 1], b3 = s.q[tt][eq + QW + 1];
@@ -705,8 +696,8 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
           else b1 = s.q[tt][eq + QW + 1], b2 = s.q[tt][eq + QW], b3 = s.q[tt][eq - 1];
           const float lo = mn32(mn32(mn32(c0, b1), b2), b3), hi = mx32(mx32(mx32(c0, b1), b2), b3);
           v = mn32(mx32(v, lo), hi);
-          v = mx32(mn32(v, s.u.t.gq[tt][4][ut]), s.u.t.gq[tt][3][ut]);
-          s.u.t.qa[tt][a][tid] = v;
+          v = mx32(mn32(v, s.t.gq[tt][4][ut]), s.t.gq[tt][3][ut]);
+          s.t.qa[tt][a][tid] = v;
         }
       }
     }
@@ -719,8 +710,8 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
         if (tt >= ntg) break;
         const size_t o = (size_t)(t0 + tt) * tstride + base + ccell;
         const double Qin = s.stage[b & 1][tt][ec];
-        const float qa[7] = {0.0f, s.u.t.qa[tt][0][tid], s.u.t.qa[tt][1][tid], s.u.t.qa[tt][2][tid],
-                             s.u.t.qa[tt][0][tid - 1], s.u.t.qa[tt][1][tid - RW - 1], s.u.t.qa[tt][2][tid - RW]};
+        const float qa[7] = {0.0f, s.t.qa[tt][0][tid], s.t.qa[tt][1][tid], s.t.qa[tt][2][tid],
+                             s.t.qa[tt][0][tid - 1], s.t.qa[tt][1][tid - RW - 1], s.t.qa[tt][2][tid - RW]};
         double sum = flx[1] * (double)qa[1];
 #pragma unroll
         for (int m = 2; m <= 6; ++m) sum = sum + flx[m] * (double)qa[m];
@@ -1115,7 +1106,7 @@ cudaError_t fast_build_offsets(const FastInst &I, float *off, cudaStream_t st) {
 cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
                             long long &launches) {
   if (M.n < 1 || M.n > kMaxInst) return cudaErrorInvalidValue;
-  long long nbk = 0, nsk = 0, npl = 0, nc = 0, nvb = 0;
+  long long nbk = 0, nsk = 0, npl = 0, nc = 0, nvb = 0, nfk = 0;
   int kmax = 0;
   constexpr int TV = 4;
   for (int i = 0; i < M.n; ++i) {
@@ -1123,6 +1114,7 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
     const long long n = I.gmax - I.gmin + 1, ncol = (long long)I.lall * n * n;
     nbk += (long long)I.nb * (I.K - 2);
     nsk += (long long)I.ns * (I.K - 2);
+    nfk += (long long)I.lall * (I.K - 2) * I.gall;
     npl += (long long)kLallPl * I.ntr;
     nc += (long long)I.ncarry * I.K;
     nvb += (long long)((I.ntr + TV - 1) / TV) * ((ncol + 255) / 256);
@@ -1134,6 +1126,7 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
   else if (kmax <= 128) k_fast_pole<128><<<(unsigned)((npl + 63) / 64), 64, 0, st>>>(M);
   else return cudaErrorInvalidValue;
   if (ev0) cudaEventRecord(ev0, st);
+  k_fast_faces<<<(unsigned)((nfk + 127) / 128), 128, 0, st>>>(M);
   cudaError_t e;
   switch (shape) {
     case 0: e = launch_tile<16, 16, 4>(M, st); break;
@@ -1148,7 +1141,7 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
   if (M.n == 1) k_fast_vert1<TV><<<(unsigned)nvb, 256, 0, st>>>(M.inst[0]);
   else k_fast_vert<TV><<<(unsigned)nvb, 256, 0, st>>>(M);
   k_fast_carry<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(M);
-  launches += 6;
+  launches += 7;
   return cudaGetLastError();
 }
 
