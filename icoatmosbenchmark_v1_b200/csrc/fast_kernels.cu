@@ -22,7 +22,7 @@
 //
 // Faces are "seam" faces when one of their two cells is a halo cell; the
 // neighbouring region computes the same face from its own halo copy, so those
-// faces are done in FP64 (seam_face, in k_fast_seam) from the FP64 boundary values.  An
+// faces are done in FP64 (k_fast_seam) from the FP64 boundary values.  An
 // interior face is computed by every tile that needs it from the same inputs by the same
 // instructions (cell positions enter only through the per-face offsets GRD_xr - GRD_x,
 // fixed per face), so both of its cells see the same value and the flux form conserves
@@ -48,15 +48,6 @@ struct GFields {
     return (double)p[off];
   }
 };
-struct GQ {
-  const FastInst *I;
-  int l, k, t;
-  __device__ double operator()(int i, int j) const {
-    const size_t off = ((size_t)l * I->K + k) * I->gall + (size_t)(j - 1) * I->G + (i - 1);
-    return I->Q_in[(size_t)t * I->lall * I->K * I->gall + off] / I->rho_in[off];
-  }
-};
-
 // ---- poles: the 5 ring faces of pole p at level k (mod_src_tracer.f90:326-374), FP64
 __device__ void pole_faces(const FastInst &I, int p, int k, double flux[7], double xc[7][3]) {
   const size_t off = ((size_t)p * I.K + k) * kGallPl;
@@ -177,6 +168,7 @@ __global__ void k_fast_boundary(const __grid_constant__ MultiInst M) {
   const double Cout =
       ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
   const double zerosw = 0.5 - fsg(0.5, fabs(Cout) - EPS);
+  const double rden = (1.0 - zerosw) / (Cout + zerosw), omc = 1.0 - Cin - Cout;
   double rinv[3][3];
   for (int dj = 0; dj < 3; ++dj)
     for (int di = 0; di < 3; ++di) rinv[dj][di] = 1.0 / f(0, i - 1 + di, j - 1 + dj);
@@ -217,8 +209,8 @@ __global__ void k_fast_boundary(const __grid_constant__ MultiInst M) {
                          chm[6] * qmn[6];
     const double CQmax = chm[1] * qmx[1] + chm[2] * qmx[2] + chm[3] * qmx[3] + chm[4] * qmx[4] + chm[5] * qmx[5] +
                          chm[6] * qmx[6];
-    out[3] = (q0 - CQmax - qnmax * (1.0 - Cin - Cout + 0.0)) / (Cout + zerosw) * (1.0 - zerosw) + q0 * zerosw;
-    out[4] = (q0 - CQmin - qnmin * (1.0 - Cin - Cout + 0.0)) / (Cout + zerosw) * (1.0 - zerosw) + q0 * zerosw;
+    out[3] = (q0 - CQmax - qnmax * omc) * rden + q0 * zerosw;
+    out[4] = (q0 - CQmin - qnmin * omc) * rden + q0 * zerosw;
     double *dst = dst0 + t * dstride;
     for (int x = 0; x < 5; ++x) dst[x] = out[x];
   }
@@ -228,40 +220,9 @@ __device__ __forceinline__ const double *bval(const FastInst &I, int t, int k, i
   return I.bbuf + (((size_t)t * I.K + k) * I.nb + b) * 5;
 }
 
-// ---- the value of a seam face (one side a halo cell), FP64, from global memory
-__device__ double seam_face(const FastInst &I, int l, int k, int t, int i, int j, int a, double flux,
-                            const double xc[3]) {
-  const bool sgp = I.have_sgp[l] != 0;
-  const GFields f{&I, l, k};
-  const GQ q{&I, l, k, t};
-  const int G = I.G;
-  const int ni = (a == AI || a == AIJ) ? i + 1 : i, nj = (a == AIJ || a == AJ) ? j + 1 : j;
-  const double ch = (flux * rarea(I, l, i, j) * I.dt) / f(0, i, j);
-  const double cm = 0.5 - fsg(0.5, ch - DBL_EPSILON);
-  const int bo = I.bsrc[(size_t)l * I.gall + (j - 1) * G + (i - 1)];
-  const int bn = I.bsrc[(size_t)l * I.gall + (nj - 1) * G + (ni - 1)];
-  // gradient and Qout of both cells (both are boundary or halo cells of this region)
-  double go[5] = {0, 0, 0, 0, 0}, gn[5] = {0, 0, 0, 0, 0};
-  const double qo = q(i, j), qn = q(ni, nj);
-  if (bo >= 0) for (int x = 0; x < 5; ++x) go[x] = bval(I, t, k, bo)[x];
-  else go[3] = go[4] = qo;  // halo point no list reaches: Qout = q, grad = 0 (as after the reference fill)
-  if (bn >= 0) for (int x = 0; x < 5; ++x) gn[x] = bval(I, t, k, bn)[x];
-  else gn[3] = gn[4] = qn;
-  double vu = qn, vs = qo;
-  for (int x = 0; x < 3; ++x) vu = vu + gn[x] * (xc[x] - gx(I, l, ni, nj, x));
-  for (int x = 0; x < 3; ++x) vs = vs + go[x] * (xc[x] - gx(I, l, i, j, x));
-  double v = cm * vu + (1.0 - cm) * vs;
-  double lo, hi;
-  bounds64(I, i, j, a, sgp, q, lo, hi);
-  const double BIG = DBL_MAX;
-  const double own_min = cm * lo + (1.0 - cm) * BIG, own_max = cm * hi + (1.0 - cm) * (-BIG);
-  const double nb_min = cm * BIG + (1.0 - cm) * lo, nb_max = cm * (-BIG) + (1.0 - cm) * hi;
-  v = cm * mn64(mx64(v, own_min), own_max) + (1.0 - cm) * mn64(mx64(v, nb_min), nb_max);
-  v = cm * mx64(mn64(v, gn[4]), gn[3]) + (1.0 - cm) * mx64(mn64(v, go[4]), go[3]);
-  return v;
-}
-
-// ---- seam faces: FP64 flux once per (face, level), then the limited value of every tracer
+// ---- seam faces (one side a halo cell): FP64 flux once per (face, level), then the limited
+// value of every tracer.  The face's Courant number and upwind mask, the remap offsets and
+// 1/rho of the cells involved do not depend on the tracer and are formed once.
 __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
   long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int ii = find_inst(M, tid, [](const FastInst &J) { return (long long)J.ns * (J.K - 2); });
@@ -271,13 +232,62 @@ __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
   const int code = I.seam_list[sidx];
   const int a = code % 3 + 1, p = code / 3;
   const int l = p / I.gall, c = p % I.gall;
-  const int i = c % I.G + 1, j = c / I.G + 1;
+  const int G = I.G, i = c % G + 1, j = c / G + 1;
+  const bool sgp = I.have_sgp[l] != 0;
   const GFields gf{&I, l, k};
   double xc[3];
-  const double fl = face_geo(I, l, i, j, a, I.have_sgp[l] != 0, gf, xc);
+  const double fl = face_geo(I, l, i, j, a, sgp, gf, xc);
   I.sflux[(size_t)k * I.ns + sidx] = fl;
-  for (int t = 0; t < I.ntr; ++t)
-    I.sval[((size_t)t * I.K + k) * I.ns + sidx] = (float)seam_face(I, l, k, t, i, j, a, fl, xc);
+  const int ni = (a == AI || a == AIJ) ? i + 1 : i, nj = (a == AIJ || a == AJ) ? j + 1 : j;
+  const double ch = (fl * rarea(I, l, i, j) * I.dt) / gf(0, i, j);
+  const double cm = 0.5 - fsg(0.5, ch - DBL_EPSILON);
+  const int bo = I.bsrc[(size_t)l * I.gall + (j - 1) * G + (i - 1)];
+  const int bn = I.bsrc[(size_t)l * I.gall + (nj - 1) * G + (ni - 1)];
+  double dxo[3], dxn[3];
+  for (int x = 0; x < 3; ++x) dxo[x] = xc[x] - gx(I, l, i, j, x), dxn[x] = xc[x] - gx(I, l, ni, nj, x);
+  // the 4 cells of the face's bounds (bounds64's selection) and 1/rho there; the owner is [0]
+  int pc[4];
+  {
+    const int ij = (j - 1) * G + i;
+    int im1j = ij - 1, ijm1 = ij - G;
+    if (im1j < 1) im1j = 1;
+    if (ijm1 < 1) ijm1 = 1;
+    pc[0] = ij;
+    if (a == AI) pc[1] = ijm1, pc[2] = ij + 1, pc[3] = ij + G + 1;
+    else if (a == AIJ) {
+      if (sgp && i == I.gmin - 1 && j == I.gmin - 1) pc[1] = ij + G + 1, pc[2] = ij + G + 2, pc[3] = ij + G;
+      else pc[1] = ij + 1, pc[2] = ij + G + 1, pc[3] = ij + G;
+    } else pc[1] = ij + G + 1, pc[2] = ij + G, pc[3] = im1j;
+  }
+  const size_t slab = ((size_t)l * I.K + k) * I.gall, tstride = (size_t)I.lall * I.K * I.gall;
+  const size_t on = (size_t)(nj - 1) * G + (ni - 1);
+  double rv[4];
+  for (int n = 0; n < 4; ++n) rv[n] = 1.0 / I.rho_in[slab + pc[n] - 1];
+  const double rn = 1.0 / I.rho_in[slab + on];
+  const double BIG = DBL_MAX;
+  for (int t = 0; t < I.ntr; ++t) {
+    const double *Qt = I.Q_in + t * tstride + slab;
+    double qv[4];
+    for (int n = 0; n < 4; ++n) qv[n] = Qt[pc[n] - 1] * rv[n];
+    const double qo = qv[0], qn = Qt[on] * rn;
+    // gradient and Qout of both cells (boundary or halo cells of this region)
+    double go[5] = {0, 0, 0, 0, 0}, gn[5] = {0, 0, 0, 0, 0};
+    if (bo >= 0) for (int x = 0; x < 5; ++x) go[x] = bval(I, t, k, bo)[x];
+    else go[3] = go[4] = qo;  // halo point no list reaches: Qout = q, grad = 0 (as after the reference fill)
+    if (bn >= 0) for (int x = 0; x < 5; ++x) gn[x] = bval(I, t, k, bn)[x];
+    else gn[3] = gn[4] = qn;
+    double vu = qn, vs = qo;
+    for (int x = 0; x < 3; ++x) vu = vu + gn[x] * dxn[x];
+    for (int x = 0; x < 3; ++x) vs = vs + go[x] * dxo[x];
+    double v = cm * vu + (1.0 - cm) * vs;
+    const double lo = mn64(mn64(mn64(qv[0], qv[1]), qv[2]), qv[3]);
+    const double hi = mx64(mx64(mx64(qv[0], qv[1]), qv[2]), qv[3]);
+    const double own_min = cm * lo + (1.0 - cm) * BIG, own_max = cm * hi + (1.0 - cm) * (-BIG);
+    const double nb_min = cm * BIG + (1.0 - cm) * lo, nb_max = cm * (-BIG) + (1.0 - cm) * hi;
+    v = cm * mn64(mx64(v, own_min), own_max) + (1.0 - cm) * mn64(mx64(v, nb_min), nb_max);
+    v = cm * mx64(mn64(v, gn[4]), gn[3]) + (1.0 - cm) * mx64(mn64(v, go[4]), go[3]);
+    I.sval[((size_t)t * I.K + k) * I.ns + sidx] = (float)v;
+  }
 }
 
 // ---- per-face remap offsets GRD_xr - GRD_x of the owner and of the neighbour (FP32),
