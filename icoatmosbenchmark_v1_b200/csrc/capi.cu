@@ -19,6 +19,7 @@ void set_error(const std::string &msg) { g_last_error = msg; }
 
 int cuda_fail(cudaError_t e, const char *what) {
   set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  cudaGetLastError();  // a launch-configuration error is not sticky: do not hand it to the next call
   return ICA_ERR_CUDA;
 }
 
