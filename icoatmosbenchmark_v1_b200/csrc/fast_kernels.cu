@@ -420,9 +420,6 @@ struct TileGeo {
   static constexpr int RW = TX + 2, RH = TY + 2, NR = RW * RH;  // ring cells
   static constexpr int NT = (NR + 31) / 32 * 32;                // threads (whole warps)
   static constexpr int WW = TX + 5, WH = TY + 5, NW = WW * WH;
-  // row stride of the q window: congruent to RW mod 32, so that the cells of a warp (whole
-  // ring rows in thread order) fall on 32 different banks in every stencil access
-  static constexpr int QW = WW + ((RW - WW) % 32 + 32) % 32, NQ = QW * WH;
 };
 
 template <int TX, int TY, int TB>
@@ -431,10 +428,12 @@ struct TileSmem {
   double rinv[NW];  // 1 / rho
   double F[3][NW];  // face flux 0.5 (rhov . HN) by owner, from k_fast_faces
   double stage[2][TB][NW];  // rhogq of the window, FP64, two batches in flight (cp.async)
-  float q[TB][TileGeo<TX, TY>::NQ];
+  // tracer pairs (x: tracer 2p, y: tracer 2p+1): one 8-byte access serves both, and a
+  // half-warp (one ring row) touches consecutive slots, so no padding is needed for banks
+  float2 q2[TB / 2][NW];
   struct {
-    float gq[TB][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
-    float qa[TB][3][NT];  // limited face values of the faces owned by ring cells
+    float2 gq[TB / 2][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
+    float2 qa[TB / 2][3][NT];  // limited face values of the faces owned by ring cells
   } t;
 };
 
@@ -444,7 +443,7 @@ struct TileSmem {
 template <int TX, int TY, int TB>
 __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, const int k, TileSmem<TX, TY, TB> &s) {
   using Gm = TileGeo<TX, TY>;
-  constexpr int RW = Gm::RW, NR = Gm::NR, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW, QW = Gm::QW;
+  constexpr int RW = Gm::RW, NR = Gm::NR, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW;
   const int tiles_per_rgn = I.ntx * I.nty;
   const int l = tile / tiles_per_rgn;
   const int tr = tile % tiles_per_rgn;
@@ -463,7 +462,6 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   const int x = ring ? tid % RW - 1 : TX + 8, y = ring ? tid / RW - 1 : TY + 8;
   const int ci = i0 + x, cj = j0 + y;
   const int ec = ring ? (y + 3) * WW + (x + 3) : 0;   // window slot of the cell
-  const int eq = ring ? (y + 3) * QW + (x + 3) : 0;   // its q slot
   const bool in_arr = ring && ci >= 1 && ci <= G && cj >= 1 && cj <= G;
   auto interior = [&](int i, int j) { return i >= I.gmin && i <= I.gmax && j >= I.gmin && j <= I.gmax; };
   const bool c_int = in_arr && interior(ci, cj);
@@ -555,9 +553,10 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
                                       (float)((double)wk1 * dt * I.rdgz[k] * rhinv), (float)rhinv, wk);
   }
 
-  // the window slots of this thread (e = tid + r*NT): global offset in the level, q slot
+  // the window slots of this thread (e = tid + r*NT): global offset in the level
   constexpr int NSLOT = (NW + NT - 1) / NT;
-  int sofs[NSLOT], sq[NSLOT];
+  constexpr int TP = TB / 2;  // tracer pairs of a batch: one float2 holds tracers 2p and 2p+1
+  int sofs[NSLOT];
   bool sok[NSLOT];
 #pragma unroll
   for (int r = 0; r < NSLOT; ++r) {
@@ -566,7 +565,6 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     const int i = i0 - 3 + lx, j = j0 - 3 + ly;
     sok[r] = e < NW && lx >= 1 && ly >= 1 && i >= 1 && i <= G && j >= 1 && j <= G;
     sofs[r] = sok[r] ? (j - 1) * G + (i - 1) : 0;
-    sq[r] = ly * QW + lx;
   }
   // rhogq window of the batch starting at tracer tb into stage[buf], asynchronously
   auto issue = [&](int tb, int buf) {
@@ -584,16 +582,59 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     }
     asm volatile("cp.async.commit_group;\n" ::);
   };
-  // q of the batch starting at tracer tb from stage[buf] (window x, y in [-2, T+1])
+  // q of the batch starting at tracer tb from stage[buf] (window x, y in [-2, T+1]), by pairs
   auto load_q = [&](int tb, int buf) {
     const int nb = min(TB, ntr - tb);
 #pragma unroll
-    for (int tt = 0; tt < TB; ++tt)
+    for (int pp = 0; pp < TP; ++pp)
 #pragma unroll
       for (int r = 0; r < NSLOT; ++r) {
         const int e = tid + r * NT;
-        if (e < NW) s.q[tt][sq[r]] = (sok[r] && tt < nb) ? (float)(s.stage[buf][tt][e] * s.rinv[e]) : 0.0f;
+        if (e < NW) {
+          float2 v = make_float2(0.0f, 0.0f);
+          if (sok[r]) {
+            const double ri = s.rinv[e];
+            if (2 * pp < nb) v.x = (float)(s.stage[buf][2 * pp][e] * ri);
+            if (2 * pp + 1 < nb) v.y = (float)(s.stage[buf][2 * pp + 1][e] * ri);
+          }
+          s.q2[pp][e] = v;
+        }
       }
+  };
+  auto cx = [](const float2 &v, int h) { return h ? v.y : v.x; };
+  // gradient and Qout of this (FP32) cell from q at the cell and its 6 neighbours
+  auto cell_gq = [&](const float qs[7], float out[5]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float g = cgr[c * 7] * qs[0];
+#pragma unroll
+      for (int n = 1; n < 7; ++n) g = g + cgr[c * 7 + n] * qs[n];
+      out[c] = g;
+    }
+    // 4-point bounds of the 6 faces (mod_src_tracer.f90:152-214): face m is the cell and
+    // the neighbours m-1, m, m+1 (cyclic, n0 = n6)
+    const float c0 = qs[0], n1 = qs[1], n2 = qs[2], n3 = qs[3], n4 = qs[4], n5 = qs[5], n6 = qs[6];
+    float lo[7], hi[7];
+    const float l12 = mn32(n1, n2), l34 = mn32(n3, n4), l56 = mn32(n5, n6);
+    const float h12 = mx32(n1, n2), h34 = mx32(n3, n4), h56 = mx32(n5, n6);
+    lo[1] = mn32(c0, mn32(n6, l12)), hi[1] = mx32(c0, mx32(n6, h12));
+    lo[2] = mn32(c0, mn32(l12, n3)), hi[2] = mx32(c0, mx32(h12, n3));
+    lo[3] = mn32(c0, mn32(n2, l34)), hi[3] = mx32(c0, mx32(n2, h34));
+    lo[4] = mn32(c0, mn32(l34, n5)), hi[4] = mx32(c0, mx32(h34, n5));
+    lo[5] = mn32(c0, mn32(n4, l56)), hi[5] = mx32(c0, mx32(n4, h56));
+    lo[6] = mn32(c0, mn32(l56, n1)), hi[6] = mx32(c0, mx32(h56, n1));
+    float qnmin = c0, qnmax = c0, CQmin = 0.0f, CQmax = 0.0f;
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) {
+      const bool in = (inmask >> m) & 1u;
+      const float qmn = in ? lo[m] : BIGf, qmx = in ? hi[m] : -BIGf;
+      qnmin = mn32(qnmin, qmn);
+      qnmax = mx32(qnmax, qmx);
+      CQmin = (m == 1) ? chm[1] * qmn : CQmin + chm[m] * qmn;
+      CQmax = (m == 1) ? chm[1] * qmx : CQmax + chm[m] * qmx;
+    }
+    out[3] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
+    out[4] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
   };
   // Per batch b: (B) gradient + Qout, (C) face values, then (D) the update of batch b
   // together with (A) q of batch b+1, whose rhogq window streamed in during B and C.
@@ -611,59 +652,42 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     if (in_arr) {
       if (bs >= 0) {  // region-boundary cell or halo cell: the FP64 boundary values
 #pragma unroll
-        for (int tt = 0; tt < TB; ++tt) {
-          if (tt >= ntg) break;
-          const double *bv = bval(I, t0 + tt, k, bs);
+        for (int pp = 0; pp < TP; ++pp) {
+          float o[2][5];
 #pragma unroll
-          for (int c = 0; c < 5; ++c) s.t.gq[tt][c][tid] = (float)bv[c];
+          for (int h = 0; h < 2; ++h) {
+            const bool ok = 2 * pp + h < ntg;
+            const double *bv = bval(I, ok ? t0 + 2 * pp + h : t0, k, bs);
+#pragma unroll
+            for (int c = 0; c < 5; ++c) o[h][c] = ok ? (float)bv[c] : 0.0f;
+          }
+#pragma unroll
+          for (int c = 0; c < 5; ++c) s.t.gq[pp][c][tid] = make_float2(o[0][c], o[1][c]);
         }
       } else if (!fp32_cell) {  // halo point no list reaches: grad 0, Qout = q
 #pragma unroll
-        for (int tt = 0; tt < TB; ++tt) {
-          s.t.gq[tt][0][tid] = s.t.gq[tt][1][tid] = s.t.gq[tt][2][tid] = 0.0f;
-          s.t.gq[tt][3][tid] = s.t.gq[tt][4][tid] = s.q[tt][eq];
+        for (int pp = 0; pp < TP; ++pp) {
+          const float2 qc = s.q2[pp][ec];
+          s.t.gq[pp][0][tid] = s.t.gq[pp][1][tid] = s.t.gq[pp][2][tid] = make_float2(0.0f, 0.0f);
+          s.t.gq[pp][3][tid] = s.t.gq[pp][4][tid] = qc;
         }
       } else {
-        const int st7[7] = {eq, eq + 1, eq + QW + 1, eq + QW, eq - 1, eq - QW - 1, eq - QW};
+        const int st7[7] = {ec, ec + 1, ec + WW + 1, ec + WW, ec - 1, ec - WW - 1, ec - WW};
 #pragma unroll
-        for (int tt = 0; tt < TB; ++tt) {
-          float qs[7];
+        for (int pp = 0; pp < TP; ++pp) {
+          float2 q2[7];
 #pragma unroll
-          for (int n = 0; n < 7; ++n) qs[n] = s.q[tt][st7[n]];
-          float g[3];
+          for (int n = 0; n < 7; ++n) q2[n] = s.q2[pp][st7[n]];
+          float o[2][5];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            g[c] = cgr[c * 7] * qs[0];
+          for (int h = 0; h < 2; ++h) {
+            float qs[7];
 #pragma unroll
-            for (int n = 1; n < 7; ++n) g[c] = g[c] + cgr[c * 7 + n] * qs[n];
+            for (int n = 0; n < 7; ++n) qs[n] = cx(q2[n], h);
+            cell_gq(qs, o[h]);
           }
-          // 4-point bounds of the 6 faces (mod_src_tracer.f90:152-214)
-          const float c0 = qs[0], n1 = qs[1], n2 = qs[2], n3 = qs[3], n4 = qs[4], n5 = qs[5], n6 = qs[6];
-          // face m: the cell and the neighbours m-1, m, m+1 (cyclic, n0 = n6)
-          float lo[7], hi[7];
-          const float l12 = mn32(n1, n2), l34 = mn32(n3, n4), l56 = mn32(n5, n6);
-          const float h12 = mx32(n1, n2), h34 = mx32(n3, n4), h56 = mx32(n5, n6);
-          lo[1] = mn32(c0, mn32(n6, l12)), hi[1] = mx32(c0, mx32(n6, h12));
-          lo[2] = mn32(c0, mn32(l12, n3)), hi[2] = mx32(c0, mx32(h12, n3));
-          lo[3] = mn32(c0, mn32(n2, l34)), hi[3] = mx32(c0, mx32(n2, h34));
-          lo[4] = mn32(c0, mn32(l34, n5)), hi[4] = mx32(c0, mx32(h34, n5));
-          lo[5] = mn32(c0, mn32(n4, l56)), hi[5] = mx32(c0, mx32(n4, h56));
-          lo[6] = mn32(c0, mn32(l56, n1)), hi[6] = mx32(c0, mx32(h56, n1));
-          float qnmin = c0, qnmax = c0, CQmin = 0.0f, CQmax = 0.0f;
 #pragma unroll
-          for (int m = 1; m <= 6; ++m) {
-            const bool in = (inmask >> m) & 1u;
-            const float qmn = in ? lo[m] : BIGf, qmx = in ? hi[m] : -BIGf;
-            qnmin = mn32(qnmin, qmn);
-            qnmax = mx32(qnmax, qmx);
-            CQmin = (m == 1) ? chm[1] * qmn : CQmin + chm[m] * qmn;
-            CQmax = (m == 1) ? chm[1] * qmx : CQmax + chm[m] * qmx;
-          }
-          s.t.gq[tt][0][tid] = g[0];
-          s.t.gq[tt][1][tid] = g[1];
-          s.t.gq[tt][2][tid] = g[2];
-          s.t.gq[tt][3][tid] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
-          s.t.gq[tt][4][tid] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
+          for (int c = 0; c < 5; ++c) s.t.gq[pp][c][tid] = make_float2(o[0][c], o[1][c]);
         }
       }
     }
@@ -671,7 +695,7 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     // ---- (C) limited values of the faces owned by ring cells x, y in [-1, T-1]
     if (owner) {
       const int nbt[3] = {tid + 1, tid + RW + 1, tid + RW};  // ring thread of the neighbour
-      const int nbs[3] = {eq + 1, eq + QW + 1, eq + QW};       // q slot of the neighbour
+      const int nbs[3] = {ec + 1, ec + WW + 1, ec + WW};       // window slot of the neighbour
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const int ni = (a < 2) ? ci + 1 : ci, nj = (a > 0) ? cj + 1 : cj;
@@ -679,35 +703,46 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
         const bool need = (x >= 0 && y >= 0) || (ni - i0 >= 0 && nj - j0 >= 0 && ni - i0 < TX && nj - j0 < TY);
         if (!need || !face_exists(I, ci, cj, a + 1)) {
 #pragma unroll
-          for (int tt = 0; tt < TB; ++tt) s.t.qa[tt][a][tid] = 0.0f;
+          for (int pp = 0; pp < TP; ++pp) s.t.qa[pp][a][tid] = make_float2(0.0f, 0.0f);
           continue;
         }
         if (!c_int || !interior(ni, nj)) {  // seam face: value of k_fast_seam
           const int sid = I.seam_id[((size_t)l * I.gall + ccell) * 3 + a];
 #pragma unroll
-          for (int tt = 0; tt < TB; ++tt) {
-            if (tt >= ntg) break;
-            s.t.qa[tt][a][tid] = I.sval[((size_t)(t0 + tt) * K + k) * I.ns + sid];
+          for (int pp = 0; pp < TP; ++pp) {
+            float v[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+              v[h] = (2 * pp + h < ntg) ? I.sval[((size_t)(t0 + 2 * pp + h) * K + k) * I.ns + sid] : 0.0f;
+            s.t.qa[pp][a][tid] = make_float2(v[0], v[1]);
           }
           continue;
         }
         const bool cmu = (cmown >> a) & 1u;  // 1: the neighbour is upwind
-        const int ut = cmu ? nbt[a] : tid, us = cmu ? nbs[a] : eq;
+        const int ut = cmu ? nbt[a] : tid, us = cmu ? nbs[a] : ec;
+        // the face's 4 points besides the cell: AI {j-1, i+1, i+1j+1}, AIJ {i+1, i+1j+1, j+1},
+        // AJ {i+1j+1, j+1, i-1}
+        const int p1 = (a == 0) ? ec - WW : (a == 1 ? ec + 1 : ec + WW + 1);
+        const int p2 = (a == 0) ? ec + 1 : (a == 1 ? ec + WW + 1 : ec + WW);
+        const int p3 = (a == 0) ? ec + WW + 1 : (a == 1 ? ec + WW : ec - 1);
 #pragma unroll
-        for (int tt = 0; tt < TB; ++tt) {
-          float v = s.q[tt][us];
-          v = v + s.t.gq[tt][0][ut] * dup[a][0];
-          v = v + s.t.gq[tt][1][ut] * dup[a][1];
-          v = v + s.t.gq[tt][2][ut] * dup[a][2];
-          const float c0 = s.q[tt][eq];
-          float b1, b2, b3;
-          if (a == 0) b1 = s.q[tt][eq - QW], b2 = s.q[tt][eq + 1], b3 = s.q[tt][eq + QW + 1];
-          else if (a == 1) b1 = s.q[tt][eq + 1], b2 = s.q[tt][eq + QW + 1], b3 = s.q[tt][eq + QW];
-          else b1 = s.q[tt][eq + QW + 1], b2 = s.q[tt][eq + QW], b3 = s.q[tt][eq - 1];
-          const float lo = mn32(mn32(mn32(c0, b1), b2), b3), hi = mx32(mx32(mx32(c0, b1), b2), b3);
-          v = mn32(mx32(v, lo), hi);
-          v = mx32(mn32(v, s.t.gq[tt][4][ut]), s.t.gq[tt][3][ut]);
-          s.t.qa[tt][a][tid] = v;
+        for (int pp = 0; pp < TP; ++pp) {
+          const float2 qu = s.q2[pp][us], g0 = s.t.gq[pp][0][ut], g1 = s.t.gq[pp][1][ut], g2 = s.t.gq[pp][2][ut];
+          const float2 on = s.t.gq[pp][3][ut], ox = s.t.gq[pp][4][ut];
+          const float2 c0 = s.q2[pp][ec], b1 = s.q2[pp][p1], b2 = s.q2[pp][p2], b3 = s.q2[pp][p3];
+          float v[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            float w = cx(qu, h);
+            w = w + cx(g0, h) * dup[a][0];
+            w = w + cx(g1, h) * dup[a][1];
+            w = w + cx(g2, h) * dup[a][2];
+            const float lo = mn32(mn32(mn32(cx(c0, h), cx(b1, h)), cx(b2, h)), cx(b3, h));
+            const float hi = mx32(mx32(mx32(cx(c0, h), cx(b1, h)), cx(b2, h)), cx(b3, h));
+            w = mn32(mx32(w, lo), hi);
+            v[h] = mx32(mn32(w, cx(ox, h)), cx(on, h));
+          }
+          s.t.qa[pp][a][tid] = make_float2(v[0], v[1]);
         }
       }
     }
@@ -716,16 +751,21 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     // ---- (D) horizontal update of the tile cells (FP64): rhogq after the horizontal sub-step
     if (active) {
 #pragma unroll
-      for (int tt = 0; tt < TB; ++tt) {
-        if (tt >= ntg) break;
-        const size_t o = (size_t)(t0 + tt) * tstride + base + ccell;
-        const double Qin = s.stage[b & 1][tt][ec];
-        const float qa[7] = {0.0f, s.t.qa[tt][0][tid], s.t.qa[tt][1][tid], s.t.qa[tt][2][tid],
-                             s.t.qa[tt][0][tid - 1], s.t.qa[tt][1][tid - RW - 1], s.t.qa[tt][2][tid - RW]};
-        double sum = flx[1] * (double)qa[1];
+      for (int pp = 0; pp < TP; ++pp) {
+        const float2 f1 = s.t.qa[pp][0][tid], f2 = s.t.qa[pp][1][tid], f3 = s.t.qa[pp][2][tid];
+        const float2 f4 = s.t.qa[pp][0][tid - 1], f5 = s.t.qa[pp][1][tid - RW - 1], f6 = s.t.qa[pp][2][tid - RW];
 #pragma unroll
-        for (int m = 2; m <= 6; ++m) sum = sum + flx[m] * (double)qa[m];
-        I.Q_out[o] = Qin - sum;
+        for (int h = 0; h < 2; ++h) {
+          const int tt = 2 * pp + h;
+          if (tt >= ntg) break;
+          const size_t o = (size_t)(t0 + tt) * tstride + base + ccell;
+          const double Qin = s.stage[b & 1][tt][ec];
+          const float qa[7] = {0.0f, cx(f1, h), cx(f2, h), cx(f3, h), cx(f4, h), cx(f5, h), cx(f6, h)};
+          double sum = flx[1] * (double)qa[1];
+#pragma unroll
+          for (int m = 2; m <= 6; ++m) sum = sum + flx[m] * (double)qa[m];
+          I.Q_out[o] = Qin - sum;
+        }
       }
     }
     // ---- (A) q of the next batch; then its buffer's successor streams in
