@@ -839,13 +839,15 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
   float ck1w[3] = {0.0f, 0.0f, 0.0f}, ck2w[3] = {0.0f, 0.0f, 0.0f}, wf[3] = {0.0f, 0.0f, 0.0f};
   double rh[3] = {0.0, 0.0, 0.0};
   double Qh[TV][3];
-  float qv[TV][3], qmn_km1[TV], qmx_km1[TV], qh_last[TV];
+  float qv[TV][3], qmn_km1[TV], qmx_km1[TV];
+  double fu_last[TV];  // w qh of the face below the level being finished (the flux of the level below)
   double qnext[TV];
 #pragma unroll
   for (int tt = 0; tt < TV; ++tt) {
     Qh[tt][0] = Qh[tt][1] = Qh[tt][2] = 0.0;
     qv[tt][0] = qv[tt][1] = qv[tt][2] = 0.0f;
-    qmn_km1[tt] = qmx_km1[tt] = qh_last[tt] = 0.0f;
+    qmn_km1[tt] = qmx_km1[tt] = 0.0f;
+    fu_last[tt] = 0.0;
     qnext[tt] = (tt < ntv) ? Q[tt * tstride + slab] : 0.0;
   }
   float4 cnext = V[slab];
@@ -873,7 +875,7 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
       for (int tt = 0; tt < TV; ++tt) {
         Qh[tt][2] = Qk[tt];
         qv[tt][1] = qv[tt][2] = (float)(Qk[tt] * (double)c.z);
-        qh_last[tt] = 0.0f;
+        fu_last[tt] = 0.0;  // qh(kmin) = 0 at the ground face
       }
       continue;
     }
@@ -881,7 +883,7 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
     const VLim vp = vlim_params(ck1w[1], ck2w[1], ck1w[2]);
     const int f = k - 1;
     const float af = (float)I.afact[f], bf = (float)I.bfact[f];
-    const double rdz = I.rdgz[k - 2];
+    const double dtrdz = dt * I.rdgz[k - 2];
 #pragma unroll
     for (int tt = 0; tt < TV; ++tt) {
       if (tt >= ntv) break;
@@ -892,20 +894,20 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
       float qh = af * qv[tt][1] + bf * qv[tt][0];
       if (f >= 2)
         qh = vp.infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - vp.infl) * mx32(mn32(qh, Qmax), Qmin);
+      const double fu = (double)wf[1] * (double)qh;
       if (k - 2 >= 1) {  // level k-2 is final once faces k-2 and k-1 are
         const int L = k - 2;
-        const double fu = (double)wf[1] * (double)qh, fl = (double)wf[0] * (double)qh_last[tt];
-        const double Qn = Qh[tt][0] - (fu - fl) * dt * rdz;
+        const double Qn = Qh[tt][0] - (fu - fu_last[tt]) * dtrdz;
         Q[tt * tstride + (size_t)L * slab] = Qn;
         if (L == 1) Q[tt * tstride] = Qn;
       }
-      qh_last[tt] = qh;
+      fu_last[tt] = fu;
       qmn_km1[tt] = Qmin;
       qmx_km1[tt] = Qmax;
     }
     if (dens && k - 2 >= 1) {
       const int L = k - 2;
-      const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dt * rdz;
+      const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dtrdz;
       R[(size_t)L * slab] = rn;
       if (L == 1) R[0] = rn;
     }
@@ -927,17 +929,17 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
     if (f >= 2)
       qh = vd.infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - vd.infl) * mx32(mn32(qh, Qmax), Qmin);
     double *Qt = Q + tt * tstride;
+    const double fm = (double)wf[2] * (double)qh;  // face K-2
     if (K - 3 >= 1) {
       const int L = K - 3;
-      const double fu = (double)wf[2] * (double)qh, fl = (double)wf[1] * (double)qh_last[tt];
-      const double Qn = Qh[tt][1] - (fu - fl) * dt * I.rdgz[L];
+      const double Qn = Qh[tt][1] - (fm - fu_last[tt]) * (dt * I.rdgz[L]);
       Qt[(size_t)L * slab] = Qn;
       if (L == 1) Qt[0] = Qn;
     }
     // top face K-1: unlimited
     const float qtop = ak * qv[tt][2] + bk * qv[tt][2];
-    const double fu = (double)wk1 * (double)qtop, fl = (double)wf[2] * (double)qh;
-    const double Qn = Qh[tt][2] - (fu - fl) * dt * I.rdgz[K - 2];
+    const double fu = (double)wk1 * (double)qtop;
+    const double Qn = Qh[tt][2] - (fu - fm) * (dt * I.rdgz[K - 2]);
     Qt[(size_t)(K - 2) * slab] = Qn;
     Qt[(size_t)(K - 1) * slab] = Qn;
     if (K - 2 == 1) Qt[0] = Qn;
@@ -945,11 +947,11 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
   if (dens) {
     if (K - 3 >= 1) {
       const int L = K - 3;
-      const double rn = rh[1] - ((double)wf[2] - (double)wf[1]) * dt * I.rdgz[L];
+      const double rn = rh[1] - ((double)wf[2] - (double)wf[1]) * (dt * I.rdgz[L]);
       R[(size_t)L * slab] = rn;
       if (L == 1) R[0] = rn;
     }
-    const double rn = rh[2] - ((double)wk1 - (double)wf[2]) * dt * I.rdgz[K - 2];
+    const double rn = rh[2] - ((double)wk1 - (double)wf[2]) * (dt * I.rdgz[K - 2]);
     R[(size_t)(K - 2) * slab] = rn;
     R[(size_t)(K - 1) * slab] = rn;
     if (K - 2 == 1) R[0] = rn;
