@@ -218,7 +218,7 @@ def run_ours(args, world, rank, local):
         step = runner.step
         st = runner.state
         dtype = "f32"
-        s_bytes = 48
+        s_bytes = 32
 
     err = m0 = None
     if args.mode != "plain" and not args.no_check:

@@ -362,9 +362,9 @@ class FastRunner:
         self.b = {k: torch.empty_like(v) for k, v in state.items()}
         self.f32 = {k: fields[k].to(torch.float32).contiguous() for k in FIELD_KEYS}
         self.updates = (10 * 4 ** grid.glevel + 2) * grid.kall * state["rhogq"].shape[0]
-        # horizontal sub-step per tracer cell-level: rhogq read + write (FP64); per cell-level, shared by
-        # the tracers: rhog read + write (FP64), rhogv x/y/z + rhogw (FP32), vertical inputs (16 B)
-        self.alg_bytes = 16.0 + 48.0 / state["rhogq"].shape[0]
+        # algorithmic bytes of one tracer cell-level update: rhogq read + write (FP64); per cell-level,
+        # shared by the tracers: rhog old and new (FP64) and rhogv x/y/z + rhogw (FP32)
+        self.alg_bytes = 16.0 + 32.0 / state["rhogq"].shape[0]
         self.shape = 0
         self.tuning = []
         if autotune:
