@@ -315,6 +315,16 @@ class IcoAdv:
             _check("ica_advect_fast_dev", lib().ica_advect_fast_dev(self.h, int(ntr), C.c_double(dt), *sp, *so,
                                                                     *fp))
 
+    def advect_fast64_dev(self, dt, state_in, state_out, fields64):
+        """The FP64 variant of the batched step (FP64 fields, FP64 faces and limiters)."""
+        ntr = state_in["rhogq"].shape[0]
+        sp = [_ptr(state_in[k], np.float64)[0] for k in STATE_KEYS]
+        so = [_ptr(state_out[k], np.float64)[0] for k in STATE_KEYS]
+        fp = [_ptr(fields64[k], np.float64)[0] for k in FIELD_KEYS]
+        with self._ordered():
+            _check("ica_advect_fast64_dev", lib().ica_advect_fast64_dev(self.h, int(ntr), C.c_double(dt), *sp, *so,
+                                                                        *fp))
+
     def advect_fast_host(self, dt, rhog, rhog_pl, rhogq, rhogq_pl, rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz,
                          rhogvz_pl, rhogw, rhogw_pl):
         """One batched step on host arrays, in place on the FP64 state (FP32 fields)."""
@@ -462,12 +472,15 @@ class Batch:
     def _args(self, args):
         return (FastArgs * len(args))(*args)
 
-    def step(self, args):
+    def step(self, args, f64=False):
+        """One step of every instance; f64: the FP64 variant (args with FP64 fields)."""
+        name = "ica_batch_step64_dev" if f64 else "ica_batch_step_dev"
         with self.ctxs[0]._ordered():
-            _check("ica_batch_step_dev", lib().ica_batch_step_dev(self.h, self._args(args)))
+            _check(name, getattr(lib(), name)(self.h, self._args(args)))
 
-    def capture(self, args, slot):
-        _check("ica_batch_capture", lib().ica_batch_capture(self.h, self._args(args), int(slot)))
+    def capture(self, args, slot, f64=False):
+        name = "ica_batch_capture64" if f64 else "ica_batch_capture"
+        _check(name, getattr(lib(), name)(self.h, self._args(args), int(slot)))
 
     def replay(self, slot):
         with self.ctxs[0]._ordered():
@@ -476,16 +489,18 @@ class Batch:
 
 class BatchRunner:
     """Device-resident loop over a batch of instances: per instance a double-buffered FP64
-    state and FP32 fields; step() launches directly, or, after use_graph(), replays the
-    captured CUDA graph of the current direction."""
+    state and FP32 fields (FP64 fields for the FP64 variant, f64=True); step() launches
+    directly, or, after use_graph(), replays the captured CUDA graph of the current direction."""
 
-    def __init__(self, ctxs, states, fields, dts, shape=0):
+    def __init__(self, ctxs, states, fields, dts, shape=0, f64=False):
         import torch
         self.batch = Batch(ctxs)
         self.batch.set_shape(shape)
+        self.f64 = bool(f64)
         self.a = list(states)
         self.b = [{k: torch.empty_like(v) for k, v in s.items()} for s in states]
-        self.f32 = [{k: f[k].to(torch.float32).contiguous() for k in FIELD_KEYS} for f in fields]
+        ft = torch.float64 if self.f64 else torch.float32
+        self.f32 = [{k: f[k].to(ft).contiguous() for k in FIELD_KEYS} for f in fields]
         self.dts = list(dts)
         self.graphs = False
         self.parity = 0  # 0: a -> b next, 1: b -> a next
@@ -506,14 +521,14 @@ class BatchRunner:
         if self.graphs:
             self.batch.replay(self.parity)
         else:
-            self.batch.step(self._argsets()[self.parity])
+            self.batch.step(self._argsets()[self.parity], self.f64)
         self.parity ^= 1
 
     def use_graph(self):
         """Capture both directions (after one uncaptured step has set up every buffer)."""
         fwd, bwd = self._argsets()
-        self.batch.capture(fwd, 0)
-        self.batch.capture(bwd, 1)
+        self.batch.capture(fwd, 0, self.f64)
+        self.batch.capture(bwd, 1, self.f64)
         self.graphs = True
 
     def close(self):

@@ -159,6 +159,7 @@ int ica_set_geometry(ica_ctx *c, const double *GRD_xr, const double *GRD_xr_pl, 
   const double *h[8] = {GRD_xr, GRD_xr_pl, GMTR_p, GMTR_p_pl, GMTR_t, GMTR_t_pl, GMTR_a, GMTR_a_pl};
   const size_t n[8] = {gl * 9, pl * 3, gl * 8, pl * 8, gl * 10, pl * 5, gl * 36, pl * 18};
   c->fast.off_ready = false;
+  c->fast.off64_ready = false;
   return c->upload_geometry(h, n);
 }
 
@@ -181,7 +182,8 @@ Ctx::~Ctx() {
   for (void *p : stepgeo)
     if (p) cudaFree(p);
   for (void *p : {(void *)fast.bsrc, (void *)fast.blist, (void *)fast.ring, (void *)fast.carry, (void *)fast.cg32,
-                  (void *)fast.off32, (void *)fast.seam_list, (void *)fast.seam_id})
+                  (void *)fast.off32, (void *)fast.off64, (void *)fast.seam_list,
+                  (void *)fast.seam_id})
     if (p) cudaFree(p);
   for (auto &ev : fast.events) cudaEventDestroy(ev.first), cudaEventDestroy(ev.second);
   if (stream) cudaStreamDestroy(stream);
@@ -560,6 +562,7 @@ int ica_set_step_geometry(ica_ctx *c, const double *GRD_x, const double *GRD_x_p
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(coef_grad fp32)");
   c->stepgeo_set = true;
   c->fast.off_ready = false;
+  c->fast.off64_ready = false;
   return ICA_OK;
 }
 
@@ -898,7 +901,8 @@ int Ctx::build_fast_tables() {
   return ICA_OK;
 }
 
-int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
+int Ctx::fast_inst(FastInst &I, int ntr, double dt, bool f64) {
+  I = FastInst{};
   if (!geo_set || !stepgeo_set) return set_error("advect_fast: geometry not registered"), ICA_ERR_STATE;
   if (sz.kall < 4 || sz.kall > 128) return set_error("advect_fast: kall must be in [4, 128]"), ICA_ERR_ARG;
   int rc = build_fast_tables();
@@ -928,6 +932,16 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
     fast.off_ready = true;
   }
   I.off32 = fast.off32;
+  I.f64 = f64 ? 1 : 0;
+  if (f64 && !fast.off64_ready) {
+    const size_t noff = (size_t)sz.lall * 18 * sz.gall;
+    if (!fast.off64 && cudaMalloc(&fast.off64, noff * sizeof(double)) != cudaSuccess)
+      return set_error("cudaMalloc(fast remap offsets, FP64)"), ICA_ERR_NOMEM;
+    cudaError_t e = fast_build_offsets64(I, fast.off64, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "fast remap offsets (FP64)");
+    fast.off64_ready = true;
+  }
+  I.off64 = fast.off64;
   I.bsrc = fast.bsrc, I.blist = fast.blist, I.pole_ring_b = fast.ring, I.nb = fast.nb;
   I.carry = fast.carry, I.ncarry = fast.ncarry;
   const size_t nbb = (size_t)ntr * sz.kall * fast.nb * 5;
@@ -935,14 +949,23 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt) {
   if (!I.bbuf) return set_error("cudaMalloc(fast boundary buffer)"), ICA_ERR_NOMEM;
   I.seam_list = fast.seam_list, I.seam_id = fast.seam_id, I.ns = fast.ns;
   I.sflux = (double *)buf("fast_sflux", (size_t)sz.kall * fast.ns * sizeof(double));
-  I.sval = (float *)buf("fast_sval", (size_t)ntr * sz.kall * fast.ns * sizeof(float));
-  if (!I.sflux || !I.sval) return set_error("cudaMalloc(fast seam buffers)"), ICA_ERR_NOMEM;
-  I.vco = (float4 *)buf("fast_vco", (size_t)sz.lall * sz.kall * sz.gall * sizeof(float4));
-  if (!I.vco) return set_error("cudaMalloc(fast vertical coefficients)"), ICA_ERR_NOMEM;
+  const size_t nsv = (size_t)ntr * sz.kall * fast.ns;
+  if (f64) I.sval64 = (double *)buf("fast_sval64", nsv * sizeof(double));
+  else I.sval = (float *)buf("fast_sval", nsv * sizeof(float));
+  if (!I.sflux || (f64 ? !I.sval64 : !I.sval)) return set_error("cudaMalloc(fast seam buffers)"), ICA_ERR_NOMEM;
+  const size_t n3v = (size_t)sz.lall * sz.kall * sz.gall;
+  if (f64) {
+    I.vco64 = (double4 *)buf("fast_vco64", n3v * sizeof(double4));
+    if (!I.vco64) return set_error("cudaMalloc(fast vertical coefficients)"), ICA_ERR_NOMEM;
+  } else {
+    I.vco = (float4 *)buf("fast_vco", n3v * sizeof(float4));
+    if (!I.vco) return set_error("cudaMalloc(fast vertical coefficients)"), ICA_ERR_NOMEM;
+  }
   const size_t n3 = (size_t)sz.lall * sz.kall * sz.gall;
   I.Fg = (double *)buf("fast_Fg", 3 * n3 * sizeof(double));
-  I.Dg = (float *)buf("fast_Dg", 9 * n3 * sizeof(float));
-  if (!I.Fg || !I.Dg) return set_error("cudaMalloc(fast face fluxes)"), ICA_ERR_NOMEM;
+  if (f64) I.Dg64 = (double *)buf("fast_Dg64", 9 * n3 * sizeof(double));
+  else I.Dg = (float *)buf("fast_Dg", 9 * n3 * sizeof(float));
+  if (!I.Fg || (f64 ? !I.Dg64 : !I.Dg)) return set_error("cudaMalloc(fast face fluxes)"), ICA_ERR_NOMEM;
   I.work_next = (unsigned long long *)buf("fast_work_next", sizeof(unsigned long long));
   if (!I.work_next) return set_error("cudaMalloc(fast work counter)"), ICA_ERR_NOMEM;
   return ICA_OK;
@@ -988,11 +1011,26 @@ int ica_fast_timing(ica_ctx *c, int enable, double *ms_total, long long *count) 
   return ICA_OK;
 }
 
-int ica_advect_fast_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, const double *rhog_in_pl,
-                        const double *rhogq_in, const double *rhogq_in_pl, double *rhog_out, double *rhog_out_pl,
-                        double *rhogq_out, double *rhogq_out_pl, const float *vx, const float *vx_pl, const float *vy,
-                        const float *vy_pl, const float *vz, const float *vz_pl, const float *w, const float *w_pl) {
-  CTX_OK(c);
+}  // extern "C"
+
+namespace icoadv {
+
+// fields of one instance: FP32 (float) or FP64 (double, the FP64 variant)
+static void set_fields(FastInst &I, const float *vx, const float *vx_pl, const float *vy, const float *vy_pl,
+                       const float *vz, const float *vz_pl, const float *w, const float *w_pl) {
+  I.vx = vx, I.vy = vy, I.vz = vz, I.w = w, I.vx_pl = vx_pl, I.vy_pl = vy_pl, I.vz_pl = vz_pl, I.w_pl = w_pl;
+}
+static void set_fields(FastInst &I, const double *vx, const double *vx_pl, const double *vy, const double *vy_pl,
+                       const double *vz, const double *vz_pl, const double *w, const double *w_pl) {
+  I.vx64 = vx, I.vy64 = vy, I.vz64 = vz, I.w64 = w, I.vx64_pl = vx_pl, I.vy64_pl = vy_pl, I.vz64_pl = vz_pl;
+  I.w64_pl = w_pl;
+}
+
+template <typename F>
+static int advect_fast_impl(Ctx *c, int ntr, double dt, const double *rhog_in, const double *rhog_in_pl,
+                            const double *rhogq_in, const double *rhogq_in_pl, double *rhog_out, double *rhog_out_pl,
+                            double *rhogq_out, double *rhogq_out_pl, const F *vx, const F *vx_pl, const F *vy,
+                            const F *vy_pl, const F *vz, const F *vz_pl, const F *w, const F *w_pl) {
   if (ntr < 1 || !rhog_in || !rhog_in_pl || !rhogq_in || !rhogq_in_pl || !rhog_out || !rhog_out_pl || !rhogq_out ||
       !rhogq_out_pl || !vx || !vx_pl || !vy || !vy_pl || !vz || !vz_pl || !w || !w_pl)
     return set_error("ica_advect_fast: NULL argument"), ICA_ERR_ARG;
@@ -1000,9 +1038,9 @@ int ica_advect_fast_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, c
     return set_error("ica_advect_fast: input and output state must be different buffers"), ICA_ERR_ARG;
   cudaSetDevice(c->device);
   FastInst I;
-  int rc = c->fast_inst(I, ntr, dt);
+  int rc = c->fast_inst(I, ntr, dt, sizeof(F) == 8);
   if (rc) return rc;
-  I.vx = vx, I.vy = vy, I.vz = vz, I.w = w, I.vx_pl = vx_pl, I.vy_pl = vy_pl, I.vz_pl = vz_pl, I.w_pl = w_pl;
+  set_fields(I, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl);
   I.rho_in = rhog_in, I.rho_in_pl = rhog_in_pl, I.Q_in = rhogq_in, I.Q_in_pl = rhogq_in_pl;
   I.rho_out = rhog_out, I.rho_out_pl = rhog_out_pl, I.Q_out = rhogq_out, I.Q_out_pl = rhogq_out_pl;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1020,6 +1058,29 @@ int ica_advect_fast_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, c
   return c->check_launch("ica_advect_fast");
 }
 
+}  // namespace icoadv
+
+extern "C" {
+
+int ica_advect_fast_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, const double *rhog_in_pl,
+                        const double *rhogq_in, const double *rhogq_in_pl, double *rhog_out, double *rhog_out_pl,
+                        double *rhogq_out, double *rhogq_out_pl, const float *vx, const float *vx_pl, const float *vy,
+                        const float *vy_pl, const float *vz, const float *vz_pl, const float *w, const float *w_pl) {
+  CTX_OK(c);
+  return advect_fast_impl<float>(c, ntr, dt, rhog_in, rhog_in_pl, rhogq_in, rhogq_in_pl, rhog_out, rhog_out_pl,
+                                 rhogq_out, rhogq_out_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl);
+}
+
+int ica_advect_fast64_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, const double *rhog_in_pl,
+                          const double *rhogq_in, const double *rhogq_in_pl, double *rhog_out, double *rhog_out_pl,
+                          double *rhogq_out, double *rhogq_out_pl, const double *vx, const double *vx_pl,
+                          const double *vy, const double *vy_pl, const double *vz, const double *vz_pl,
+                          const double *w, const double *w_pl) {
+  CTX_OK(c);
+  return advect_fast_impl<double>(c, ntr, dt, rhog_in, rhog_in_pl, rhogq_in, rhogq_in_pl, rhog_out, rhog_out_pl,
+                                  rhogq_out, rhogq_out_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl);
+}
+
 }  // extern "C"
 
 struct ica_batch {
@@ -1031,32 +1092,35 @@ struct ica_batch {
 
 namespace icoadv {
 
-static int fast_args_ok(const ica_fast_args &a) {
+template <typename Args>
+static int fast_args_ok(const Args &a) {
   return a.ntr >= 1 && a.rhog_in && a.rhog_in_pl && a.rhogq_in && a.rhogq_in_pl && a.rhog_out && a.rhog_out_pl &&
          a.rhogq_out && a.rhogq_out_pl && a.rhogvx && a.rhogvx_pl && a.rhogvy && a.rhogvy_pl && a.rhogvz &&
          a.rhogvz_pl && a.rhogw && a.rhogw_pl && a.rhogq_in != a.rhogq_out && a.rhog_in != a.rhog_out;
 }
 
 // instance table of a batch step (device buffers of every instance set up here)
-static int batch_insts(ica_batch *b, const ica_fast_args *args, MultiInst &M) {
+template <typename Args>
+static int batch_insts(ica_batch *b, const Args *args, MultiInst &M) {
+  constexpr bool f64 = sizeof(*args->rhogvx) == 8;
   M.n = (int)b->ctx.size();
   for (int i = 0; i < M.n; ++i) {
     Ctx *c = b->ctx[i];
-    const ica_fast_args &a = args[i];
+    const Args &a = args[i];
     if (!fast_args_ok(a)) return set_error("ica_batch: bad arguments of instance " + std::to_string(i)), ICA_ERR_ARG;
     c->fast.shape = b->shape;
     FastInst &I = M.inst[i];
-    const int rc = c->fast_inst(I, a.ntr, a.dt);
+    const int rc = c->fast_inst(I, a.ntr, a.dt, f64);
     if (rc) return rc;
-    I.vx = a.rhogvx, I.vy = a.rhogvy, I.vz = a.rhogvz, I.w = a.rhogw;
-    I.vx_pl = a.rhogvx_pl, I.vy_pl = a.rhogvy_pl, I.vz_pl = a.rhogvz_pl, I.w_pl = a.rhogw_pl;
+    set_fields(I, a.rhogvx, a.rhogvx_pl, a.rhogvy, a.rhogvy_pl, a.rhogvz, a.rhogvz_pl, a.rhogw, a.rhogw_pl);
     I.rho_in = a.rhog_in, I.rho_in_pl = a.rhog_in_pl, I.Q_in = a.rhogq_in, I.Q_in_pl = a.rhogq_in_pl;
     I.rho_out = a.rhog_out, I.rho_out_pl = a.rhog_out_pl, I.Q_out = a.rhogq_out, I.Q_out_pl = a.rhogq_out_pl;
   }
   return ICA_OK;
 }
 
-static int batch_enqueue(ica_batch *b, const MultiInst &M, const ica_fast_args *args) {
+template <typename Args>
+static int batch_enqueue(ica_batch *b, const MultiInst &M, const Args *args) {
   Ctx *c0 = b->ctx[0];
   long long launches = 0;
   cudaError_t e = fast_step_multi(M, b->shape, c0->stream, nullptr, nullptr, launches);
@@ -1109,7 +1173,12 @@ int ica_batch_set_shape(ica_batch *b, int shape) {
   return ICA_OK;
 }
 
-int ica_batch_step_dev(ica_batch *b, const ica_fast_args *args) {
+}  // extern "C"
+
+namespace icoadv {
+
+template <typename Args>
+static int batch_step_impl(ica_batch *b, const Args *args) {
   if (!b || !args) return set_error("ica_batch_step_dev: NULL argument"), ICA_ERR_ARG;
   cudaSetDevice(b->ctx[0]->device);
   MultiInst M;
@@ -1118,7 +1187,8 @@ int ica_batch_step_dev(ica_batch *b, const ica_fast_args *args) {
   return batch_enqueue(b, M, args);
 }
 
-int ica_batch_capture(ica_batch *b, const ica_fast_args *args, int slot) {
+template <typename Args>
+static int batch_capture_impl(ica_batch *b, const Args *args, int slot) {
   if (!b || !args || slot < 0 || slot > 1) return set_error("ica_batch_capture: bad arguments"), ICA_ERR_ARG;
   cudaSetDevice(b->ctx[0]->device);
   MultiInst M;
@@ -1144,6 +1214,17 @@ int ica_batch_capture(ica_batch *b, const ica_fast_args *args, int slot) {
   e = cudaGraphInstantiate(&b->exec[slot], g, 0);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
   return ICA_OK;
+}
+
+}  // namespace icoadv
+
+extern "C" {
+
+int ica_batch_step_dev(ica_batch *b, const ica_fast_args *args) { return batch_step_impl(b, args); }
+int ica_batch_step64_dev(ica_batch *b, const ica_fast_args64 *args) { return batch_step_impl(b, args); }
+int ica_batch_capture(ica_batch *b, const ica_fast_args *args, int slot) { return batch_capture_impl(b, args, slot); }
+int ica_batch_capture64(ica_batch *b, const ica_fast_args64 *args, int slot) {
+  return batch_capture_impl(b, args, slot);
 }
 
 int ica_batch_replay(ica_batch *b, int slot) {

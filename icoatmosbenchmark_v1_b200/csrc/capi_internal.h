@@ -33,6 +33,8 @@ struct FastState {  // fused path: boundary tables, tile shape, kernel timing
   float *cg32 = nullptr;
   float *off32 = nullptr;  // per-face remap offsets, rebuilt when the geometry changes
   bool off_ready = false;
+  double *off64 = nullptr;  // the same in FP64 (FP64 variant)
+  bool off64_ready = false;
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
 };
@@ -71,7 +73,7 @@ struct Ctx {
   int step_ctx(StepCtx &S);
   FastState fast;
   int build_fast_tables();
-  int fast_inst(FastInst &I, int ntr, double dt);
+  int fast_inst(FastInst &I, int ntr, double dt, bool f64 = false);
   AdjTape tape;
 };
 

@@ -22,7 +22,12 @@ struct FastInst {
   const float *cg32;   // coef_grad in FP32, (lall, 3, 7, gall)
   const float *off32;  // remap offsets GRD_xr - GRD_x per face, FP32, (lall, 18, gall)
   const double *rdgz, *afact, *bfact;
+  // fields: FP32 (the FP32 variant) or, when f64 is set, FP64 (the FP64 variant: every face
+  // value, bound and limiter in FP64, so the batched step follows the plain FP64 step)
+  int f64;
   const float *vx, *vy, *vz, *w, *vx_pl, *vy_pl, *vz_pl, *w_pl;
+  const double *vx64, *vy64, *vz64, *w64, *vx64_pl, *vy64_pl, *vz64_pl, *w64_pl;
+  const double *off64;  // remap offsets in FP64 (FP64 variant), layout of off32
   const double *rho_in, *rho_in_pl, *Q_in, *Q_in_pl;
   double *rho_out, *rho_out_pl, *Q_out, *Q_out_pl;
   // region-boundary / pole values of grad and Qout, computed once per step
@@ -38,10 +43,13 @@ struct FastInst {
   int ns;
   double *sflux;  // (K, ns): 0.5 (rhov . HN) of the seam faces
   float *sval;    // (ntr, K, ns): limited face values of the seam faces
+  double *sval64;  // the same in FP64 (FP64 variant)
   double *bbuf;  // (ntr, K, nb, 5): grad x, y, z, Qout min, Qout max
   double *Fg;    // (3, lall, K, gall): face flux 0.5 (rhov . HN) of the 3 faces of each owner, per step
   float *Dg;     // (9, lall, K, gall): face a, component c at a*3+c: -rhov rr dt / 2 (GRD_xc - GRD_xr)
   float4 *vco;   // (lall, K, gall): ck(k,1), ck(k,2), 1/rhog, rhogw(k) after the horizontal sub-step
+  double4 *vco64;  // the same in FP64 (FP64 variant)
+  double *Dg64;    // centroid displacements in FP64 (FP64 variant), layout of Dg
   unsigned long long *work_next;  // work-item counter of the persistent horizontal kernel
 };
 
@@ -72,6 +80,35 @@ __device__ __forceinline__ double mx64(double a, double b) { return (b > a) ? b 
 // Operands here are never NaN; for them the two agree except for the sign of a zero result.
 __device__ __forceinline__ float mn32(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ float mx32(float a, float b) { return fmaxf(a, b); }
+
+// field readers at flat offset o: var 0..3 = rhogvx, rhogvy, rhogvz, rhogw (FP64 of either variant)
+__device__ __forceinline__ double fld(const FastInst &I, int var, size_t o) {
+  if (I.f64) return (var == 0 ? I.vx64 : var == 1 ? I.vy64 : var == 2 ? I.vz64 : I.w64)[o];
+  return (double)(var == 0 ? I.vx : var == 1 ? I.vy : var == 2 ? I.vz : I.w)[o];
+}
+__device__ __forceinline__ double fld_pl(const FastInst &I, int var, size_t o) {
+  if (I.f64) return (var == 0 ? I.vx64_pl : var == 1 ? I.vy64_pl : var == 2 ? I.vz64_pl : I.w64_pl)[o];
+  return (double)(var == 0 ? I.vx_pl : var == 1 ? I.vy_pl : var == 2 ? I.vz_pl : I.w_pl)[o];
+}
+
+// arithmetic of the tile and column kernels: FP32 (float) or FP64 (double)
+template <typename R> struct Arith;
+template <> struct Arith<float> {
+  using V2 = float2;
+  static constexpr float BIG = FLT_MAX, RR_EPS = FLT_EPSILON;
+  static __device__ __forceinline__ float mn(float a, float b) { return fminf(a, b); }
+  static __device__ __forceinline__ float mx(float a, float b) { return fmaxf(a, b); }
+  static __device__ __forceinline__ float sgn(float a, float b) { return copysignf(a, b); }
+  static __device__ __forceinline__ V2 v2(float a, float b) { return make_float2(a, b); }
+};
+template <> struct Arith<double> {
+  using V2 = double2;
+  static constexpr double BIG = DBL_MAX, RR_EPS = DBL_EPSILON;
+  static __device__ __forceinline__ double mn(double a, double b) { return (b < a) ? b : a; }
+  static __device__ __forceinline__ double mx(double a, double b) { return (b > a) ? b : a; }
+  static __device__ __forceinline__ double sgn(double a, double b) { return copysign(a, b); }
+  static __device__ __forceinline__ V2 v2(double a, double b) { return make_double2(a, b); }
+};
 
 // geometry readers (region coords i,j 1-based)
 __device__ __forceinline__ double gt(const FastInst &I, int l, int i, int j, int t, int w) {

@@ -31,6 +31,7 @@
 
 #include <cfloat>
 #include <cstdint>
+#include <type_traits>
 
 #include "fast_common.cuh"
 #include "fast_kernels.cuh"
@@ -44,8 +45,7 @@ struct GFields {
   __device__ double operator()(int var, int i, int j) const {
     const size_t off = ((size_t)l * I->K + k) * I->gall + (size_t)(j - 1) * I->G + (i - 1);
     if (var == 0) return I->rho_in[off];
-    const float *p = var == 1 ? I->vx : (var == 2 ? I->vy : I->vz);
-    return (double)p[off];
+    return fld(*I, var - 1, off);
   }
 };
 // ---- poles: the 5 ring faces of pole p at level k (mod_src_tracer.f90:326-374), FP64
@@ -54,9 +54,9 @@ __device__ void pole_faces(const FastInst &I, int p, int k, double flux[7], doub
   auto GT = [&](int v, int w) { return I.GMTR_t_pl[((size_t)(w - 1) * kLallPl + p) * kGallPl + (v - 1)]; };
   auto GA = [&](int v, int h) { return I.GMTR_a_pl[((size_t)(h - 1) * kLallPl + p) * kGallPl + (v - 1)]; };
   auto R = [&](int v) { return I.rho_in_pl[off + v - 1]; };
-  auto X = [&](int v) { return (double)I.vx_pl[off + v - 1]; };
-  auto Y = [&](int v) { return (double)I.vy_pl[off + v - 1]; };
-  auto Z = [&](int v) { return (double)I.vz_pl[off + v - 1]; };
+  auto X = [&](int v) { return fld_pl(I, 0, off + v - 1); };
+  auto Y = [&](int v) { return fld_pl(I, 1, off + v - 1); };
+  auto Z = [&](int v) { return fld_pl(I, 2, off + v - 1); };
   double rt[7], xt[7], yt[7], zt[7];
   for (int v = 2; v <= 6; ++v) {
     const int vp = (v == 6) ? 2 : v + 1;
@@ -286,14 +286,16 @@ __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
     const double nb_min = cm * BIG + (1.0 - cm) * lo, nb_max = cm * (-BIG) + (1.0 - cm) * hi;
     v = cm * mn64(mx64(v, own_min), own_max) + (1.0 - cm) * mn64(mx64(v, nb_min), nb_max);
     v = cm * mx64(mn64(v, gn[4]), gn[3]) + (1.0 - cm) * mx64(mn64(v, go[4]), go[3]);
-    I.sval[((size_t)t * I.K + k) * I.ns + sidx] = (float)v;
+    if (I.f64) I.sval64[((size_t)t * I.K + k) * I.ns + sidx] = v;
+    else I.sval[((size_t)t * I.K + k) * I.ns + sidx] = (float)v;
   }
 }
 
 // ---- per-face remap offsets GRD_xr - GRD_x of the owner and of the neighbour (FP32),
 // fixed per face, so an interior face value does not depend on the tile that computes it.
 // off32 (lall, 18, gall): [a*6 + x] owner side, [a*6 + 3 + x] neighbour side, a = face 0..2
-__global__ void k_fast_offsets(FastInst I, float *off) {
+template <typename T>
+__global__ void k_fast_offsets(FastInst I, T *off) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= (long long)I.lall * I.gall) return;
   const int l = (int)(tid / I.gall), c = (int)(tid % I.gall);
@@ -303,8 +305,8 @@ __global__ void k_fast_offsets(FastInst I, float *off) {
     const bool nok = ni <= G && nj <= G;
     for (int x = 0; x < 3; ++x) {
       const double xr = gxr(I, l, i, j, a, x + 1);
-      off[((size_t)l * 18 + (a - 1) * 6 + x) * I.gall + c] = (float)(xr - gx(I, l, i, j, x));
-      off[((size_t)l * 18 + (a - 1) * 6 + 3 + x) * I.gall + c] = nok ? (float)(xr - gx(I, l, ni, nj, x)) : 0.0f;
+      off[((size_t)l * 18 + (a - 1) * 6 + x) * I.gall + c] = (T)(xr - gx(I, l, i, j, x));
+      off[((size_t)l * 18 + (a - 1) * 6 + 3 + x) * I.gall + c] = nok ? (T)(xr - gx(I, l, ni, nj, x)) : T(0);
     }
   }
 }
@@ -314,7 +316,9 @@ __global__ void k_fast_offsets(FastInst I, float *off) {
 // between interior cells, the FP64 value of k_fast_seam on seam faces, zero where the
 // reference has no face.  One thread per (owner cell, level); every tile that needs a
 // face reads this one value, so its two cells see the same flux.
+template <typename R>
 __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
+  using A = Arith<R>;
   long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int ii = find_inst(M, w, [](const FastInst &I) { return (long long)I.lall * (I.K - 2) * I.gall; });
   if (ii < 0) return;
@@ -323,52 +327,53 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
   const int lk = (int)(w / I.gall), k = 1 + lk % (I.K - 2), l = lk / (I.K - 2);
   const int i = c % G + 1, j = c / G + 1;
   const size_t n3 = (size_t)I.lall * I.K * I.gall, o = ((size_t)l * I.K + k) * I.gall + c;
-  const float dtf = (float)I.dt;
+  const R dtf = (R)I.dt;
   auto interior = [&](int a, int b) { return a >= I.gmin && a <= I.gmax && b >= I.gmin && b <= I.gmax; };
-  // rho, rhovx, rhovy, rhovz (FP32) of cell (a, b) of this slab
-  auto fld = [&](int a, int b, float f[4]) {
+  // rho, rhovx, rhovy, rhovz of cell (a, b) of this slab, in the arithmetic type
+  auto cellf = [&](int a, int b, R f[4]) {
     const size_t q = ((size_t)l * I.K + k) * I.gall + (size_t)(b - 1) * G + (a - 1);
-    f[0] = (float)I.rho_in[q], f[1] = I.vx[q], f[2] = I.vy[q], f[3] = I.vz[q];
+    f[0] = (R)I.rho_in[q], f[1] = (R)fld(I, 0, q), f[2] = (R)fld(I, 1, q), f[3] = (R)fld(I, 2, q);
   };
   // triangle TI (t = 0: cells (a,b), (a+1,b), (a+1,b+1)) or TJ (t = 1: (a,b), (a+1,b+1), (a,b+1))
-  auto tri = [&](int a, int b, int t, float v[4]) {
-    const float w1 = (float)gt(I, l, a, b, t + 1, W1), w2 = (float)gt(I, l, a, b, t + 1, W2),
-                w3 = (float)gt(I, l, a, b, t + 1, W3);
-    float f0[4], f1[4], f2[4];
-    fld(a, b, f0);
-    fld(a + 1, b + 1, t == 0 ? f2 : f1);
-    if (t == 0) fld(a + 1, b, f1);
-    else fld(a, b + 1, f2);
+  auto tri = [&](int a, int b, int t, R v[4]) {
+    const R w1 = (R)gt(I, l, a, b, t + 1, W1), w2 = (R)gt(I, l, a, b, t + 1, W2),
+                w3 = (R)gt(I, l, a, b, t + 1, W3);
+    R f0[4], f1[4], f2[4];
+    cellf(a, b, f0);
+    cellf(a + 1, b + 1, t == 0 ? f2 : f1);
+    if (t == 0) cellf(a + 1, b, f1);
+    else cellf(a, b + 1, f2);
 #pragma unroll
     for (int x = 0; x < 4; ++x) v[x] = f0[x] * w1 + f1[x] * w2 + f2[x] * w3;
   };
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     double F = 0.0;
-    float d[3] = {0.0f, 0.0f, 0.0f};
+    R d[3] = {R(0.0), R(0.0), R(0.0)};
     if (i < G && j < G && face_exists(I, i, j, a + 1)) {
       const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
       if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64 flux of k_fast_seam
         const int sid = I.seam_id[((size_t)l * I.gall + c) * 3 + a];
         F = I.sflux[(size_t)k * I.ns + sid];
       } else {  // AI = TJ(i,j-1) + TI(i,j); AIJ = TI(i,j) + TJ(i,j); AJ = TJ(i,j) + TI(i-1,j)
-        float p[4], q[4];
+        R p[4], q[4];
         if (a == 0) tri(i, j - 1, 1, p), tri(i, j, 0, q);
         else if (a == 1) tri(i, j, 0, p), tri(i, j, 1, q);
         else tri(i, j, 1, p), tri(i - 1, j, 0, q);
-        const float vx = p[1] + q[1], vy = p[2] + q[2], vz = p[3] + q[3];
-        const float rr = 1.0f / mx32(p[0] + q[0], FLT_EPSILON);
-        const float Ff = 0.5f * (vx * (float)ga(I, l, i, j, a + 1, HNX) + vy * (float)ga(I, l, i, j, a + 1, HNY) +
-                                 vz * (float)ga(I, l, i, j, a + 1, HNZ));
+        const R vx = p[1] + q[1], vy = p[2] + q[2], vz = p[3] + q[3];
+        const R rr = R(1.0) / A::mx(p[0] + q[0], A::RR_EPS);
+        const R Ff = R(0.5) * (vx * (R)ga(I, l, i, j, a + 1, HNX) + vy * (R)ga(I, l, i, j, a + 1, HNY) +
+                                 vz * (R)ga(I, l, i, j, a + 1, HNZ));
         F = (double)Ff;
-        d[0] = -(vx * rr * dtf * 0.5f);
-        d[1] = -(vy * rr * dtf * 0.5f);
-        d[2] = -(vz * rr * dtf * 0.5f);
+        d[0] = -(vx * rr * dtf * R(0.5));
+        d[1] = -(vy * rr * dtf * R(0.5));
+        d[2] = -(vz * rr * dtf * R(0.5));
       }
     }
     I.Fg[(size_t)a * n3 + o] = F;
 #pragma unroll
-    for (int x = 0; x < 3; ++x) I.Dg[(size_t)(a * 3 + x) * n3 + o] = d[x];
+    for (int x = 0; x < 3; ++x) if (sizeof(R) == 8) I.Dg64[(size_t)(a * 3 + x) * n3 + o] = d[x];
+    else I.Dg[(size_t)(a * 3 + x) * n3 + o] = (float)d[x];
   }
 }
 
@@ -383,29 +388,34 @@ constexpr float kEpsThr = (float)DBL_EPSILON;
 
 // ---- vertical Thuburn limiter (dyn_vert_adv_limiter/src/mod_src_tracer.f90:107-186), d = 0, FP32:
 // the tracer-independent part of a level (upwind flags, Courant sums) and the per-tracer bounds
+template <typename R>
 struct VLim {
-  float infl, a1, a2, bl, bu, icm, rden, zsw;
+  R infl, a1, a2, bl, bu, icm, rden, zsw;
 };
-__device__ __forceinline__ VLim vlim_params(float c1, float c2, float c1p) {
-  VLim v;
-  v.infl = 0.5f - copysignf(0.5f, c1);
-  const float infu = 0.5f + copysignf(0.5f, c1p);
-  v.bl = (1.0f - v.infl) * FLT_MAX;
-  v.bu = (1.0f - infu) * FLT_MAX;
+template <typename R>
+__device__ __forceinline__ VLim<R> vlim_params(R c1, R c2, R c1p) {
+  using A = Arith<R>;
+  VLim<R> v;
+  v.infl = R(0.5) - A::sgn(R(0.5), c1);
+  const R infu = R(0.5) + A::sgn(R(0.5), c1p);
+  v.bl = (R(1.0) - v.infl) * A::BIG;
+  v.bu = (R(1.0) - infu) * A::BIG;
   v.a1 = v.infl * c1;
   v.a2 = infu * c2;
-  const float Cin = v.a1 + v.a2;
-  const float Cout = (1.0f - v.infl) * c1 + (1.0f - infu) * c2;
+  const R Cin = v.a1 + v.a2;
+  const R Cout = (R(1.0) - v.infl) * c1 + (R(1.0) - infu) * c2;
   v.icm = Cin + Cout;
-  v.zsw = 0.5f - copysignf(0.5f, fabsf(Cout) - kEpsThr);
-  v.rden = (1.0f - v.zsw) / (Cout + v.zsw);
+  v.zsw = R(0.5) - A::sgn(R(0.5), fabs(Cout) - R(DBL_EPSILON));
+  v.rden = (R(1.0) - v.zsw) / (Cout + v.zsw);
   return v;
 }
-__device__ __forceinline__ void vlim_qout(const VLim &v, float qm, float qk, float qp, float &Qmin, float &Qmax) {
-  const float minL = mn32(qk, qm) + v.bl, minU = mn32(qk, qp) + v.bu;
-  const float maxL = mx32(qk, qm) - v.bl, maxU = mx32(qk, qp) - v.bu;
-  const float qnmin = mn32(mn32(minL, minU), qk), qnmax = mx32(mx32(maxL, maxU), qk);
-  const float CQmin = v.a1 * minL + v.a2 * minU, CQmax = v.a1 * maxL + v.a2 * maxU;
+template <typename R>
+__device__ __forceinline__ void vlim_qout(const VLim<R> &v, R qm, R qk, R qp, R &Qmin, R &Qmax) {
+  using A = Arith<R>;
+  const R minL = A::mn(qk, qm) + v.bl, minU = A::mn(qk, qp) + v.bu;
+  const R maxL = A::mx(qk, qm) - v.bl, maxU = A::mx(qk, qp) - v.bu;
+  const R qnmin = A::mn(A::mn(minL, minU), qk), qnmax = A::mx(A::mx(maxL, maxU), qk);
+  const R CQmin = v.a1 * minL + v.a2 * minU, CQmax = v.a1 * maxL + v.a2 * maxU;
   Qmin = ((qk - qnmax) + qnmax * v.icm - CQmax) * v.rden + qk * v.zsw;
   Qmax = ((qk - qnmin) + qnmin * v.icm - CQmin) * v.rden + qk * v.zsw;
 }
@@ -422,26 +432,30 @@ struct TileGeo {
   static constexpr int WW = TX + 5, WH = TY + 5, NW = WW * WH;
 };
 
-template <int TX, int TY, int TB>
+template <int TX, int TY, int TB, typename R>
 struct TileSmem {
+  using V2 = typename Arith<R>::V2;
   static constexpr int NT = TileGeo<TX, TY>::NT, NW = TileGeo<TX, TY>::NW;
   double rinv[NW];  // 1 / rho
   double F[3][NW];  // face flux 0.5 (rhov . HN) by owner, from k_fast_faces
   double stage[2][TB][NW];  // rhogq of the window, FP64, two batches in flight (cp.async)
   // tracer pairs (x: tracer 2p, y: tracer 2p+1): one 8-byte access serves both, and a
   // half-warp (one ring row) touches consecutive slots, so no padding is needed for banks
-  float2 q2[TB / 2][NW];
+  V2 q2[TB / 2][NW];
   struct {
-    float2 gq[TB / 2][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
-    float2 qa[TB / 2][3][NT];  // limited face values of the faces owned by ring cells
+    V2 gq[TB / 2][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
+    V2 qa[TB / 2][3][NT];  // limited face values of the faces owned by ring cells
   } t;
 };
 
 // one work item (tile, level) of instance I.  I is taken by value and the body inlined once
 // per call site, so every field of I stays a constant-bank operand (a reference to the
 // parameter measured 9% more instructions: fields reloaded around the global stores).
-template <int TX, int TY, int TB>
-__device__ __forceinline__ void horiz_item(const FastInst I, const int tile, const int k, TileSmem<TX, TY, TB> &s) {
+template <int TX, int TY, int TB, typename R>
+__device__ __forceinline__ void horiz_item(const FastInst I, const int tile, const int k,
+                                           TileSmem<TX, TY, TB, R> &s) {
+  using A = Arith<R>;
+  using V2 = typename A::V2;
   using Gm = TileGeo<TX, TY>;
   constexpr int RW = Gm::RW, NR = Gm::NR, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW;
   const int tiles_per_rgn = I.ntx * I.nty;
@@ -454,8 +468,8 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   const size_t slab = (size_t)I.gall, lk = (size_t)K * I.gall, tstride = (size_t)I.lall * K * I.gall;
   const size_t base = (size_t)l * lk + (size_t)k * slab;
   const double dt = I.dt;
-  const float dtf = (float)dt;
-  const float BIGf = FLT_MAX, EPSf = kEpsThr;
+  const R dtf = (R)dt;
+  const R BIGf = A::BIG, EPSf = R(DBL_EPSILON);
 
   // this thread's ring cell
   const bool ring = tid < NR;
@@ -466,12 +480,12 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   auto interior = [&](int i, int j) { return i >= I.gmin && i <= I.gmax && j >= I.gmin && j <= I.gmax; };
   const bool c_int = in_arr && interior(ci, cj);
   const int bs = in_arr ? I.bsrc[(size_t)l * I.gall + (cj - 1) * G + (ci - 1)] : -3;
-  const bool fp32_cell = c_int && bs == -1;                          // gradient / Qout in FP32 here
+  const bool tile_cell = c_int && bs == -1;                          // gradient / Qout formed in the tile
   const bool active = x >= 0 && x < TX && y >= 0 && y < TY && c_int;  // updated by this thread
   const bool owner = x < TX && y < TY && in_arr;                     // face values of its 3 faces
   const size_t ccell = in_arr ? (size_t)(cj - 1) * G + (ci - 1) : 0;
   const double ra64 = c_int ? rarea(I, l, ci, cj) : 1.0;
-  const float ra32 = (float)ra64;
+  const R ra32 = (R)ra64;
 
   // ---- (0a) 1/rho and the face fluxes (k_fast_faces) of this level in the window
   for (int e = tid; e < NW; e += NT) {
@@ -489,50 +503,55 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   // ---- (0d) per ring cell: Courant numbers, masks, outflow sums, gradient coefficients;
   // per owner: upwind offsets; per tile cell: flx_h (FP64), rho after the horizontal
   // sub-step and the tracer-independent inputs of the vertical sub-step
-  float chm[7], omc = 0.0f, rden = 0.0f, zsw = 1.0f, cgr[21];
+  R chm[7], omc = R(0.0), rden = R(0.0), zsw = R(1.0), cgr[21];
   unsigned inmask = 0, cmown = 0;
-  float dup[3][3];
+  R dup[3][3];
   const int nbe[7] = {0, ec, ec, ec, ec - 1, ec - WW - 1, ec - WW};  // owner slot of face m
 #pragma unroll
-  for (int m = 0; m < 7; ++m) chm[m] = 0.0f;
+  for (int m = 0; m < 7; ++m) chm[m] = R(0.0);
 #pragma unroll
-  for (int n = 0; n < 21; ++n) cgr[n] = fp32_cell ? I.cg32[((size_t)l * 21 + n) * I.gall + ccell] : 0.0f;
-  if (fp32_cell) {
-    const float rcinv = (float)s.rinv[ec];  // Courant numbers by the reciprocal of rho (one division per cell)
-    float ch[7];
+  for (int n = 0; n < 21; ++n) cgr[n] = tile_cell ? (sizeof(R) == 8 ? (R)I.cg[((size_t)l * 21 + n) * I.gall + ccell]
+                                             : (R)I.cg32[((size_t)l * 21 + n) * I.gall + ccell])
+                            : R(0);
+  if (tile_cell) {
+    const R rcinv = (R)s.rinv[ec];  // Courant numbers by the reciprocal of rho (one division per cell)
+    R ch[7];
 #pragma unroll
     for (int m = 1; m <= 6; ++m) {
-      const float Fm = (float)s.F[(m - 1) % 3][nbe[m]];
+      const R Fm = (R)s.F[(m - 1) % 3][nbe[m]];
       ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) * rcinv;
-      chm[m] = mn32(ch[m], 0.0f);
-      float chown = ch[m];
+      chm[m] = A::mn(ch[m], R(0.0));
+      R chown = ch[m];
       if (m >= 4) {  // the owner's own Courant number of this face, as the owner forms it
         const int oi = (m == 6) ? ci : ci - 1, oj = (m == 4) ? cj : cj - 1;
-        chown = (Fm * (float)rarea(I, l, oi, oj) * dtf) * (float)s.rinv[nbe[m]];
+        chown = (Fm * (R)rarea(I, l, oi, oj) * dtf) * (R)s.rinv[nbe[m]];
       }
-      const float cm = 0.5f - copysignf(0.5f, chown - EPSf);
-      const bool in = (m <= 3) ? (cm != 0.0f) : (cm == 0.0f);
+      const R cm = R(0.5) - A::sgn(R(0.5), chown - EPSf);
+      const bool in = (m <= 3) ? (cm != R(0.0)) : (cm == R(0.0));
       inmask |= in ? (1u << m) : 0u;
     }
-    const float Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
-    const float Cout =
+    const R Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
+    const R Cout =
         ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
-    zsw = 0.5f - copysignf(0.5f, fabsf(Cout) - EPSf);
-    omc = 1.0f - Cin - Cout;
-    rden = (1.0f - zsw) / (Cout + zsw);
+    zsw = R(0.5) - A::sgn(R(0.5), fabs(Cout) - EPSf);
+    omc = R(1.0) - Cin - Cout;
+    rden = (R(1.0) - zsw) / (Cout + zsw);
   }
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    dup[a][0] = dup[a][1] = dup[a][2] = 0.0f;
+    dup[a][0] = dup[a][1] = dup[a][2] = R(0.0);
     if (owner && c_int) {
-      const float Fa = (float)s.F[a][ec];
-      const float chown = (Fa * ra32 * dtf) * (float)s.rinv[ec];
-      const bool cm = (0.5f - copysignf(0.5f, chown - EPSf)) != 0.0f;
+      const R Fa = (R)s.F[a][ec];
+      const R chown = (Fa * ra32 * dtf) * (R)s.rinv[ec];
+      const bool cm = (R(0.5) - A::sgn(R(0.5), chown - EPSf)) != R(0.0);
       cmown |= cm ? (1u << a) : 0u;
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        dup[a][c] = I.off32[((size_t)l * 18 + a * 6 + (cm ? 3 : 0) + c) * I.gall + ccell] +
-                    I.Dg[(size_t)(a * 3 + c) * tstride + base + ccell];
+        dup[a][c] = (sizeof(R) == 8)
+                        ? (R)(I.off64[((size_t)l * 18 + a * 6 + (cm ? 3 : 0) + c) * I.gall + ccell] +
+                              I.Dg64[(size_t)(a * 3 + c) * tstride + base + ccell])
+                        : (R)(I.off32[((size_t)l * 18 + a * 6 + (cm ? 3 : 0) + c) * I.gall + ccell] +
+                              I.Dg[(size_t)(a * 3 + c) * tstride + base + ccell]);
     }
   }
   double flx[7];
@@ -547,15 +566,18 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     }
     const double rho_h = I.rho_in[base + ccell] - sum;
     I.rho_out[base + ccell] = rho_h;
-    const float wk = I.w[base + ccell], wk1 = I.w[base + slab + ccell];
+    const double wk = fld(I, 3, base + ccell), wk1 = fld(I, 3, base + slab + ccell);
     const double rhinv = 1.0 / rho_h;
-    I.vco[base + ccell] = make_float4((float)(-(double)wk * dt * I.rdgz[k] * rhinv),
-                                      (float)((double)wk1 * dt * I.rdgz[k] * rhinv), (float)rhinv, wk);
+    if (sizeof(R) == 8)
+      I.vco64[base + ccell] = make_double4(-wk * dt * I.rdgz[k] * rhinv, wk1 * dt * I.rdgz[k] * rhinv, rhinv, wk);
+    else
+      I.vco[base + ccell] = make_float4((float)(-wk * dt * I.rdgz[k] * rhinv), (float)(wk1 * dt * I.rdgz[k] * rhinv),
+                                        (float)rhinv, (float)wk);
   }
 
   // the window slots of this thread (e = tid + r*NT): global offset in the level
   constexpr int NSLOT = (NW + NT - 1) / NT;
-  constexpr int TP = TB / 2;  // tracer pairs of a batch: one float2 holds tracers 2p and 2p+1
+  constexpr int TP = TB / 2;  // tracer pairs of a batch: one V2 holds tracers 2p and 2p+1
   int sofs[NSLOT];
   bool sok[NSLOT];
 #pragma unroll
@@ -591,45 +613,45 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
       for (int r = 0; r < NSLOT; ++r) {
         const int e = tid + r * NT;
         if (e < NW) {
-          float2 v = make_float2(0.0f, 0.0f);
+          V2 v = A::v2(R(0.0), R(0.0));
           if (sok[r]) {
             const double ri = s.rinv[e];
-            if (2 * pp < nb) v.x = (float)(s.stage[buf][2 * pp][e] * ri);
-            if (2 * pp + 1 < nb) v.y = (float)(s.stage[buf][2 * pp + 1][e] * ri);
+            if (2 * pp < nb) v.x = (R)(s.stage[buf][2 * pp][e] * ri);
+            if (2 * pp + 1 < nb) v.y = (R)(s.stage[buf][2 * pp + 1][e] * ri);
           }
           s.q2[pp][e] = v;
         }
       }
   };
-  auto cx = [](const float2 &v, int h) { return h ? v.y : v.x; };
+  auto cx = [](const V2 &v, int h) { return h ? v.y : v.x; };
   // gradient and Qout of this (FP32) cell from q at the cell and its 6 neighbours
-  auto cell_gq = [&](const float qs[7], float out[5]) {
+  auto cell_gq = [&](const R qs[7], R out[5]) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      float g = cgr[c * 7] * qs[0];
+      R g = cgr[c * 7] * qs[0];
 #pragma unroll
       for (int n = 1; n < 7; ++n) g = g + cgr[c * 7 + n] * qs[n];
       out[c] = g;
     }
     // 4-point bounds of the 6 faces (mod_src_tracer.f90:152-214): face m is the cell and
     // the neighbours m-1, m, m+1 (cyclic, n0 = n6)
-    const float c0 = qs[0], n1 = qs[1], n2 = qs[2], n3 = qs[3], n4 = qs[4], n5 = qs[5], n6 = qs[6];
-    float lo[7], hi[7];
-    const float l12 = mn32(n1, n2), l34 = mn32(n3, n4), l56 = mn32(n5, n6);
-    const float h12 = mx32(n1, n2), h34 = mx32(n3, n4), h56 = mx32(n5, n6);
-    lo[1] = mn32(c0, mn32(n6, l12)), hi[1] = mx32(c0, mx32(n6, h12));
-    lo[2] = mn32(c0, mn32(l12, n3)), hi[2] = mx32(c0, mx32(h12, n3));
-    lo[3] = mn32(c0, mn32(n2, l34)), hi[3] = mx32(c0, mx32(n2, h34));
-    lo[4] = mn32(c0, mn32(l34, n5)), hi[4] = mx32(c0, mx32(h34, n5));
-    lo[5] = mn32(c0, mn32(n4, l56)), hi[5] = mx32(c0, mx32(n4, h56));
-    lo[6] = mn32(c0, mn32(l56, n1)), hi[6] = mx32(c0, mx32(h56, n1));
-    float qnmin = c0, qnmax = c0, CQmin = 0.0f, CQmax = 0.0f;
+    const R c0 = qs[0], n1 = qs[1], n2 = qs[2], n3 = qs[3], n4 = qs[4], n5 = qs[5], n6 = qs[6];
+    R lo[7], hi[7];
+    const R l12 = A::mn(n1, n2), l34 = A::mn(n3, n4), l56 = A::mn(n5, n6);
+    const R h12 = A::mx(n1, n2), h34 = A::mx(n3, n4), h56 = A::mx(n5, n6);
+    lo[1] = A::mn(c0, A::mn(n6, l12)), hi[1] = A::mx(c0, A::mx(n6, h12));
+    lo[2] = A::mn(c0, A::mn(l12, n3)), hi[2] = A::mx(c0, A::mx(h12, n3));
+    lo[3] = A::mn(c0, A::mn(n2, l34)), hi[3] = A::mx(c0, A::mx(n2, h34));
+    lo[4] = A::mn(c0, A::mn(l34, n5)), hi[4] = A::mx(c0, A::mx(h34, n5));
+    lo[5] = A::mn(c0, A::mn(n4, l56)), hi[5] = A::mx(c0, A::mx(n4, h56));
+    lo[6] = A::mn(c0, A::mn(l56, n1)), hi[6] = A::mx(c0, A::mx(h56, n1));
+    R qnmin = c0, qnmax = c0, CQmin = R(0.0), CQmax = R(0.0);
 #pragma unroll
     for (int m = 1; m <= 6; ++m) {
       const bool in = (inmask >> m) & 1u;
-      const float qmn = in ? lo[m] : BIGf, qmx = in ? hi[m] : -BIGf;
-      qnmin = mn32(qnmin, qmn);
-      qnmax = mx32(qnmax, qmx);
+      const R qmn = in ? lo[m] : BIGf, qmx = in ? hi[m] : -BIGf;
+      qnmin = A::mn(qnmin, qmn);
+      qnmax = A::mx(qnmax, qmx);
       CQmin = (m == 1) ? chm[1] * qmn : CQmin + chm[m] * qmn;
       CQmax = (m == 1) ? chm[1] * qmx : CQmax + chm[m] * qmx;
     }
@@ -653,41 +675,41 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
       if (bs >= 0) {  // region-boundary cell or halo cell: the FP64 boundary values
 #pragma unroll
         for (int pp = 0; pp < TP; ++pp) {
-          float o[2][5];
+          R o[2][5];
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const bool ok = 2 * pp + h < ntg;
             const double *bv = bval(I, ok ? t0 + 2 * pp + h : t0, k, bs);
 #pragma unroll
-            for (int c = 0; c < 5; ++c) o[h][c] = ok ? (float)bv[c] : 0.0f;
+            for (int c = 0; c < 5; ++c) o[h][c] = ok ? (R)bv[c] : R(0.0);
           }
 #pragma unroll
-          for (int c = 0; c < 5; ++c) s.t.gq[pp][c][tid] = make_float2(o[0][c], o[1][c]);
+          for (int c = 0; c < 5; ++c) s.t.gq[pp][c][tid] = A::v2(o[0][c], o[1][c]);
         }
-      } else if (!fp32_cell) {  // halo point no list reaches: grad 0, Qout = q
+      } else if (!tile_cell) {  // halo point no list reaches: grad 0, Qout = q
 #pragma unroll
         for (int pp = 0; pp < TP; ++pp) {
-          const float2 qc = s.q2[pp][ec];
-          s.t.gq[pp][0][tid] = s.t.gq[pp][1][tid] = s.t.gq[pp][2][tid] = make_float2(0.0f, 0.0f);
+          const V2 qc = s.q2[pp][ec];
+          s.t.gq[pp][0][tid] = s.t.gq[pp][1][tid] = s.t.gq[pp][2][tid] = A::v2(R(0.0), R(0.0));
           s.t.gq[pp][3][tid] = s.t.gq[pp][4][tid] = qc;
         }
       } else {
         const int st7[7] = {ec, ec + 1, ec + WW + 1, ec + WW, ec - 1, ec - WW - 1, ec - WW};
 #pragma unroll
         for (int pp = 0; pp < TP; ++pp) {
-          float2 q2[7];
+          V2 q2[7];
 #pragma unroll
           for (int n = 0; n < 7; ++n) q2[n] = s.q2[pp][st7[n]];
-          float o[2][5];
+          R o[2][5];
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            float qs[7];
+            R qs[7];
 #pragma unroll
             for (int n = 0; n < 7; ++n) qs[n] = cx(q2[n], h);
             cell_gq(qs, o[h]);
           }
 #pragma unroll
-          for (int c = 0; c < 5; ++c) s.t.gq[pp][c][tid] = make_float2(o[0][c], o[1][c]);
+          for (int c = 0; c < 5; ++c) s.t.gq[pp][c][tid] = A::v2(o[0][c], o[1][c]);
         }
       }
     }
@@ -703,18 +725,20 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
         const bool need = (x >= 0 && y >= 0) || (ni - i0 >= 0 && nj - j0 >= 0 && ni - i0 < TX && nj - j0 < TY);
         if (!need || !face_exists(I, ci, cj, a + 1)) {
 #pragma unroll
-          for (int pp = 0; pp < TP; ++pp) s.t.qa[pp][a][tid] = make_float2(0.0f, 0.0f);
+          for (int pp = 0; pp < TP; ++pp) s.t.qa[pp][a][tid] = A::v2(R(0.0), R(0.0));
           continue;
         }
         if (!c_int || !interior(ni, nj)) {  // seam face: value of k_fast_seam
           const int sid = I.seam_id[((size_t)l * I.gall + ccell) * 3 + a];
 #pragma unroll
           for (int pp = 0; pp < TP; ++pp) {
-            float v[2];
+            R v[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h)
-              v[h] = (2 * pp + h < ntg) ? I.sval[((size_t)(t0 + 2 * pp + h) * K + k) * I.ns + sid] : 0.0f;
-            s.t.qa[pp][a][tid] = make_float2(v[0], v[1]);
+              v[h] = (2 * pp + h < ntg) ? (sizeof(R) == 8 ? (R)I.sval64[((size_t)(t0 + 2 * pp + h) * K + k) * I.ns + sid]
+                                                          : (R)I.sval[((size_t)(t0 + 2 * pp + h) * K + k) * I.ns + sid])
+                                          : R(0.0);
+            s.t.qa[pp][a][tid] = A::v2(v[0], v[1]);
           }
           continue;
         }
@@ -727,22 +751,22 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
         const int p3 = (a == 0) ? ec + WW + 1 : (a == 1 ? ec + WW : ec - 1);
 #pragma unroll
         for (int pp = 0; pp < TP; ++pp) {
-          const float2 qu = s.q2[pp][us], g0 = s.t.gq[pp][0][ut], g1 = s.t.gq[pp][1][ut], g2 = s.t.gq[pp][2][ut];
-          const float2 on = s.t.gq[pp][3][ut], ox = s.t.gq[pp][4][ut];
-          const float2 c0 = s.q2[pp][ec], b1 = s.q2[pp][p1], b2 = s.q2[pp][p2], b3 = s.q2[pp][p3];
-          float v[2];
+          const V2 qu = s.q2[pp][us], g0 = s.t.gq[pp][0][ut], g1 = s.t.gq[pp][1][ut], g2 = s.t.gq[pp][2][ut];
+          const V2 on = s.t.gq[pp][3][ut], ox = s.t.gq[pp][4][ut];
+          const V2 c0 = s.q2[pp][ec], b1 = s.q2[pp][p1], b2 = s.q2[pp][p2], b3 = s.q2[pp][p3];
+          R v[2];
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            float w = cx(qu, h);
+            R w = cx(qu, h);
             w = w + cx(g0, h) * dup[a][0];
             w = w + cx(g1, h) * dup[a][1];
             w = w + cx(g2, h) * dup[a][2];
-            const float lo = mn32(mn32(mn32(cx(c0, h), cx(b1, h)), cx(b2, h)), cx(b3, h));
-            const float hi = mx32(mx32(mx32(cx(c0, h), cx(b1, h)), cx(b2, h)), cx(b3, h));
-            w = mn32(mx32(w, lo), hi);
-            v[h] = mx32(mn32(w, cx(ox, h)), cx(on, h));
+            const R lo = A::mn(A::mn(A::mn(cx(c0, h), cx(b1, h)), cx(b2, h)), cx(b3, h));
+            const R hi = A::mx(A::mx(A::mx(cx(c0, h), cx(b1, h)), cx(b2, h)), cx(b3, h));
+            w = A::mn(A::mx(w, lo), hi);
+            v[h] = A::mx(A::mn(w, cx(ox, h)), cx(on, h));
           }
-          s.t.qa[pp][a][tid] = make_float2(v[0], v[1]);
+          s.t.qa[pp][a][tid] = A::v2(v[0], v[1]);
         }
       }
     }
@@ -752,15 +776,15 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     if (active) {
 #pragma unroll
       for (int pp = 0; pp < TP; ++pp) {
-        const float2 f1 = s.t.qa[pp][0][tid], f2 = s.t.qa[pp][1][tid], f3 = s.t.qa[pp][2][tid];
-        const float2 f4 = s.t.qa[pp][0][tid - 1], f5 = s.t.qa[pp][1][tid - RW - 1], f6 = s.t.qa[pp][2][tid - RW];
+        const V2 f1 = s.t.qa[pp][0][tid], f2 = s.t.qa[pp][1][tid], f3 = s.t.qa[pp][2][tid];
+        const V2 f4 = s.t.qa[pp][0][tid - 1], f5 = s.t.qa[pp][1][tid - RW - 1], f6 = s.t.qa[pp][2][tid - RW];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int tt = 2 * pp + h;
           if (tt >= ntg) break;
           const size_t o = (size_t)(t0 + tt) * tstride + base + ccell;
           const double Qin = s.stage[b & 1][tt][ec];
-          const float qa[7] = {0.0f, cx(f1, h), cx(f2, h), cx(f3, h), cx(f4, h), cx(f5, h), cx(f6, h)};
+          const R qa[7] = {R(0.0), cx(f1, h), cx(f2, h), cx(f3, h), cx(f4, h), cx(f5, h), cx(f6, h)};
           double sum = flx[1] * (double)qa[1];
 #pragma unroll
           for (int m = 2; m <= 6; ++m) sum = sum + flx[m] * (double)qa[m];
@@ -778,10 +802,10 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
 // Batches of instances: persistent, one wave of CTAs; each takes the next work item
 // (instance, level, tile; tiles fastest) from a counter that starts at zero, so CTAs that
 // drew cheap items take more (as fast as one CTA per item; a static stride was 9% slower).
-template <int TX, int TY, int TB>
-__global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(const __grid_constant__ MultiInst M,
-                                                                       long long nwork) {
-  using S = TileSmem<TX, TY, TB>;
+template <int TX, int TY, int TB, typename R>
+__global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
+    k_fast_horiz(const __grid_constant__ MultiInst M, long long nwork) {
+  using S = TileSmem<TX, TY, TB, R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S &s = *reinterpret_cast<S *>(smem_raw);
   __shared__ long long s_item;
@@ -794,22 +818,22 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz(const __g
     const int ntl = M.inst[ii].lall * M.inst[ii].ntx * M.inst[ii].nty;
     const int tile = (int)(wi % ntl), k = 1 + (int)(wi / ntl);
     switch (ii) {
-      case 0: horiz_item<TX, TY, TB>(M.inst[0], tile, k, s); break;
-      case 1: horiz_item<TX, TY, TB>(M.inst[1], tile, k, s); break;
-      case 2: horiz_item<TX, TY, TB>(M.inst[2], tile, k, s); break;
-      default: horiz_item<TX, TY, TB>(M.inst[3], tile, k, s); break;
+      case 0: horiz_item<TX, TY, TB, R>(M.inst[0], tile, k, s); break;
+      case 1: horiz_item<TX, TY, TB, R>(M.inst[1], tile, k, s); break;
+      case 2: horiz_item<TX, TY, TB, R>(M.inst[2], tile, k, s); break;
+      default: horiz_item<TX, TY, TB, R>(M.inst[3], tile, k, s); break;
     }
     __syncthreads();  // the next item's fields overwrite this item's shared data; s_item is reread
   }
 }
 
 // one grid: one CTA per (tile, level) (grid x = tile, y = level - 1)
-template <int TX, int TY, int TB>
-__global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz1(FastInst I) {
-  using S = TileSmem<TX, TY, TB>;
+template <int TX, int TY, int TB, typename R>
+__global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2)) k_fast_horiz1(FastInst I) {
+  using S = TileSmem<TX, TY, TB, R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S &s = *reinterpret_cast<S *>(smem_raw);
-  horiz_item<TX, TY, TB>(I, (int)blockIdx.x, 1 + (int)blockIdx.y, s);
+  horiz_item<TX, TY, TB, R>(I, (int)blockIdx.x, 1 + (int)blockIdx.y, s);
 }
 
 // ---- vertical sub-step: one thread per (interior column, TV tracers), streaming the
@@ -818,8 +842,10 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, 2) k_fast_horiz1(FastInst
 // written to) Q_out; the threads of the first tracer group also finish rhog.
 // The tracer groups of a column block are consecutive blocks, so they run together and
 // share the per-level inputs (vco) in L2.
-template <int TV>
+template <int TV, typename R>
 __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
+  using A = Arith<R>;
+  using V4 = typename std::conditional<sizeof(R) == 8, double4, float4>::type;
   const int ngr = (I.ntr + TV - 1) / TV;
   const int t0 = (int)(blk % ngr) * TV;
   const int ntv = min(TV, I.ntr - t0);
@@ -832,28 +858,28 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
   const size_t slab = (size_t)I.gall, tstride = (size_t)I.lall * K * slab;
   const size_t cbase = (size_t)l * K * slab + (size_t)(j - 1) * I.G + (i - 1);
   double *Q = I.Q_out + (size_t)t0 * tstride + cbase;
-  double *R = I.rho_out + cbase;
-  const float4 *V = I.vco + cbase;
+  double *RH = I.rho_out + cbase;
+  const V4 *V = (const V4 *)(sizeof(R) == 8 ? (const void *)I.vco64 : (const void *)I.vco) + cbase;
   const bool dens = t0 == 0;
   const double dt = I.dt;
-  float ck1w[3] = {0.0f, 0.0f, 0.0f}, ck2w[3] = {0.0f, 0.0f, 0.0f}, wf[3] = {0.0f, 0.0f, 0.0f};
+  R ck1w[3] = {R(0.0), R(0.0), R(0.0)}, ck2w[3] = {R(0.0), R(0.0), R(0.0)}, wf[3] = {R(0.0), R(0.0), R(0.0)};
   double rh[3] = {0.0, 0.0, 0.0};
   double Qh[TV][3];
-  float qv[TV][3], qmn_km1[TV], qmx_km1[TV];
+  R qv[TV][3], qmn_km1[TV], qmx_km1[TV];
   double fu_last[TV];  // w qh of the face below the level being finished (the flux of the level below)
   double qnext[TV];
 #pragma unroll
   for (int tt = 0; tt < TV; ++tt) {
     Qh[tt][0] = Qh[tt][1] = Qh[tt][2] = 0.0;
-    qv[tt][0] = qv[tt][1] = qv[tt][2] = 0.0f;
-    qmn_km1[tt] = qmx_km1[tt] = 0.0f;
+    qv[tt][0] = qv[tt][1] = qv[tt][2] = R(0.0);
+    qmn_km1[tt] = qmx_km1[tt] = R(0.0);
     fu_last[tt] = 0.0;
     qnext[tt] = (tt < ntv) ? Q[tt * tstride + slab] : 0.0;
   }
-  float4 cnext = V[slab];
-  double rnext = dens ? R[slab] : 0.0;
+  V4 cnext = V[slab];
+  double rnext = dens ? RH[slab] : 0.0;
   for (int k = 1; k <= K - 2; ++k) {
-    const float4 c = cnext;
+    const V4 c = cnext;
     double Qk[TV];
 #pragma unroll
     for (int tt = 0; tt < TV; ++tt) Qk[tt] = qnext[tt];
@@ -864,7 +890,7 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
 #pragma unroll
       for (int tt = 0; tt < TV; ++tt)
         if (tt < ntv) qnext[tt] = Q[tt * tstride + o];
-      if (dens) rnext = R[o];
+      if (dens) rnext = RH[o];
     }
     ck1w[0] = ck1w[1], ck1w[1] = ck1w[2], ck1w[2] = c.x;
     ck2w[0] = ck2w[1], ck2w[1] = ck2w[2], ck2w[2] = c.y;
@@ -874,26 +900,26 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
 #pragma unroll
       for (int tt = 0; tt < TV; ++tt) {
         Qh[tt][2] = Qk[tt];
-        qv[tt][1] = qv[tt][2] = (float)(Qk[tt] * (double)c.z);
+        qv[tt][1] = qv[tt][2] = (R)(Qk[tt] * (double)c.z);
         fu_last[tt] = 0.0;  // qh(kmin) = 0 at the ground face
       }
       continue;
     }
     // Qout of level k-1 from q at k-2, k-1, k; the face k-1 between levels k-2 and k-1
-    const VLim vp = vlim_params(ck1w[1], ck2w[1], ck1w[2]);
+    const VLim<R> vp = vlim_params<R>(ck1w[1], ck2w[1], ck1w[2]);
     const int f = k - 1;
-    const float af = (float)I.afact[f], bf = (float)I.bfact[f];
+    const R af = (R)I.afact[f], bf = (R)I.bfact[f];
     const double dtrdz = dt * I.rdgz[k - 2];
 #pragma unroll
     for (int tt = 0; tt < TV; ++tt) {
       if (tt >= ntv) break;
       Qh[tt][0] = Qh[tt][1], Qh[tt][1] = Qh[tt][2], Qh[tt][2] = Qk[tt];
-      qv[tt][0] = qv[tt][1], qv[tt][1] = qv[tt][2], qv[tt][2] = (float)(Qk[tt] * (double)c.z);
-      float Qmin, Qmax;
+      qv[tt][0] = qv[tt][1], qv[tt][1] = qv[tt][2], qv[tt][2] = (R)(Qk[tt] * (double)c.z);
+      R Qmin, Qmax;
       vlim_qout(vp, qv[tt][0], qv[tt][1], qv[tt][2], Qmin, Qmax);
-      float qh = af * qv[tt][1] + bf * qv[tt][0];
+      R qh = af * qv[tt][1] + bf * qv[tt][0];
       if (f >= 2)
-        qh = vp.infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - vp.infl) * mx32(mn32(qh, Qmax), Qmin);
+        qh = vp.infl * A::mx(A::mn(qh, qmx_km1[tt]), qmn_km1[tt]) + (R(1.0) - vp.infl) * A::mx(A::mn(qh, Qmax), Qmin);
       const double fu = (double)wf[1] * (double)qh;
       if (k - 2 >= 1) {  // level k-2 is final once faces k-2 and k-1 are
         const int L = k - 2;
@@ -908,26 +934,26 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
     if (dens && k - 2 >= 1) {
       const int L = k - 2;
       const double rn = rh[0] - ((double)wf[1] - (double)wf[0]) * dtrdz;
-      R[(size_t)L * slab] = rn;
-      if (L == 1) R[0] = rn;
+      RH[(size_t)L * slab] = rn;
+      if (L == 1) RH[0] = rn;
     }
   }
   // ---- drain: levels K-3 and K-2 (faces K-2 and K-1); ghost level above: q(kmax+1) = q(kmax)
   const int kk = K - 1;
-  const float wk1 = I.w[cbase + (size_t)kk * slab];
-  const float c1top = (float)(-(double)wk1 * dt * I.rdgz[kk] / I.rho_in[cbase + (size_t)kk * slab]);
-  const VLim vd = vlim_params(ck1w[2], ck2w[2], c1top);  // level K-2 with q(K-1) := q(K-2)
+  const R wk1 = (R)fld(I, 3, cbase + (size_t)kk * slab);
+  const R c1top = (R)(-(double)wk1 * dt * I.rdgz[kk] / I.rho_in[cbase + (size_t)kk * slab]);
+  const VLim<R> vd = vlim_params<R>(ck1w[2], ck2w[2], c1top);  // level K-2 with q(K-1) := q(K-2)
   const int f = K - 2;
-  const float af = (float)I.afact[f], bf = (float)I.bfact[f];
-  const float ak = (float)I.afact[kk], bk = (float)I.bfact[kk];
+  const R af = (R)I.afact[f], bf = (R)I.bfact[f];
+  const R ak = (R)I.afact[kk], bk = (R)I.bfact[kk];
 #pragma unroll
   for (int tt = 0; tt < TV; ++tt) {
     if (tt >= ntv) break;
-    float Qmin, Qmax;
+    R Qmin, Qmax;
     vlim_qout(vd, qv[tt][1], qv[tt][2], qv[tt][2], Qmin, Qmax);
-    float qh = af * qv[tt][2] + bf * qv[tt][1];
+    R qh = af * qv[tt][2] + bf * qv[tt][1];
     if (f >= 2)
-      qh = vd.infl * mx32(mn32(qh, qmx_km1[tt]), qmn_km1[tt]) + (1.0f - vd.infl) * mx32(mn32(qh, Qmax), Qmin);
+      qh = vd.infl * A::mx(A::mn(qh, qmx_km1[tt]), qmn_km1[tt]) + (R(1.0) - vd.infl) * A::mx(A::mn(qh, Qmax), Qmin);
     double *Qt = Q + tt * tstride;
     const double fm = (double)wf[2] * (double)qh;  // face K-2
     if (K - 3 >= 1) {
@@ -937,7 +963,7 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
       if (L == 1) Qt[0] = Qn;
     }
     // top face K-1: unlimited
-    const float qtop = ak * qv[tt][2] + bk * qv[tt][2];
+    const R qtop = ak * qv[tt][2] + bk * qv[tt][2];
     const double fu = (double)wk1 * (double)qtop;
     const double Qn = Qh[tt][2] - (fu - fm) * (dt * I.rdgz[K - 2]);
     Qt[(size_t)(K - 2) * slab] = Qn;
@@ -948,22 +974,22 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
     if (K - 3 >= 1) {
       const int L = K - 3;
       const double rn = rh[1] - ((double)wf[2] - (double)wf[1]) * (dt * I.rdgz[L]);
-      R[(size_t)L * slab] = rn;
-      if (L == 1) R[0] = rn;
+      RH[(size_t)L * slab] = rn;
+      if (L == 1) RH[0] = rn;
     }
     const double rn = rh[2] - ((double)wk1 - (double)wf[2]) * (dt * I.rdgz[K - 2]);
-    R[(size_t)(K - 2) * slab] = rn;
-    R[(size_t)(K - 1) * slab] = rn;
-    if (K - 2 == 1) R[0] = rn;
+    RH[(size_t)(K - 2) * slab] = rn;
+    RH[(size_t)(K - 1) * slab] = rn;
+    if (K - 2 == 1) RH[0] = rn;
   }
 }
 
-template <int TV>
+template <int TV, typename R>
 __global__ void __launch_bounds__(256, 2) k_fast_vert1(FastInst I) {
-  vert_block<TV>(I, blockIdx.x);
+  vert_block<TV, R>(I, blockIdx.x);
 }
 
-template <int TV>
+template <int TV, typename R>
 __global__ void __launch_bounds__(256, 2) k_fast_vert(const __grid_constant__ MultiInst M) {
   // blocks of an instance: (tracer group fastest, column block)
   long long blk = blockIdx.x;
@@ -972,10 +998,10 @@ __global__ void __launch_bounds__(256, 2) k_fast_vert(const __grid_constant__ Mu
     return (long long)((J.ntr + TV - 1) / TV) * ((nc + 255) / 256);
   });
   switch (ii) {
-    case 0: vert_block<TV>(M.inst[0], blk); break;
-    case 1: vert_block<TV>(M.inst[1], blk); break;
-    case 2: vert_block<TV>(M.inst[2], blk); break;
-    case 3: vert_block<TV>(M.inst[3], blk); break;
+    case 0: vert_block<TV, R>(M.inst[0], blk); break;
+    case 1: vert_block<TV, R>(M.inst[1], blk); break;
+    case 2: vert_block<TV, R>(M.inst[2], blk); break;
+    case 3: vert_block<TV, R>(M.inst[3], blk); break;
     default: break;
   }
 }
@@ -1033,7 +1059,7 @@ __global__ void k_fast_pole(const __grid_constant__ MultiInst M) {
   // vertical sub-step of the pole column (FP64, region form, as the plain path)
   const int kmin = 1, kmax = K - 2;
   double ck1[KMAX], ck2[KMAX], q[KMAX], qh[KMAX];
-  auto W = [&](int k) { return (double)I.w_pl[((size_t)p * K + k) * kGallPl]; };
+  auto W = [&](int k) { return fld_pl(I, 3, ((size_t)p * K + k) * kGallPl); };
   for (int k = 0; k < K; ++k) ck1[k] = ck2[k] = 0.0;
   for (int k = kmin; k <= kmax; ++k) {
     ck1[k] = -W(k) * I.dt * I.rdgz[k] / rh[k];
@@ -1097,9 +1123,9 @@ __global__ void k_fast_carry(const __grid_constant__ MultiInst M) {
 }
 
 // ---------------------------------------------------------------------------------------
-template <int TX, int TY, int TB, bool ONE>
+template <int TX, int TY, int TB, bool ONE, typename R>
 static cudaError_t launch_tile_n(const MultiInst &M, cudaStream_t st) {
-  const int smem = (int)sizeof(TileSmem<TX, TY, TB>);
+  const int smem = (int)sizeof(TileSmem<TX, TY, TB, R>);
   constexpr int NT = TileGeo<TX, TY>::NT;
   static int per_sm[64] = {};  // resident CTAs per SM, per device (set up once, outside any capture)
   int dev = 0;
@@ -1109,11 +1135,11 @@ static cudaError_t launch_tile_n(const MultiInst &M, cudaStream_t st) {
   if (!per_sm[dev]) {
     int occ = 0;
     if (ONE) {
-      e = cudaFuncSetAttribute(k_fast_horiz1<TX, TY, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fast_horiz1<TX, TY, TB>, NT, smem);
+      e = cudaFuncSetAttribute(k_fast_horiz1<TX, TY, TB, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fast_horiz1<TX, TY, TB, R>, NT, smem);
     } else {
-      e = cudaFuncSetAttribute(k_fast_horiz<TX, TY, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fast_horiz<TX, TY, TB>, NT, smem);
+      e = cudaFuncSetAttribute(k_fast_horiz<TX, TY, TB, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fast_horiz<TX, TY, TB, R>, NT, smem);
     }
     if (e != cudaSuccess) return e;
     per_sm[dev] = occ > 0 ? occ : 1;
@@ -1125,19 +1151,19 @@ static cudaError_t launch_tile_n(const MultiInst &M, cudaStream_t st) {
   for (int i = 0; i < M.n; ++i) nwork += (long long)M.inst[i].lall * M.inst[i].ntx * M.inst[i].nty * (M.inst[i].K - 2);
   if (ONE) {
     const FastInst &I = M.inst[0];
-    k_fast_horiz1<TX, TY, TB><<<dim3((unsigned)(I.lall * I.ntx * I.nty), (unsigned)(I.K - 2)), NT, smem, st>>>(I);
+    k_fast_horiz1<TX, TY, TB, R><<<dim3((unsigned)(I.lall * I.ntx * I.nty), (unsigned)(I.K - 2)), NT, smem, st>>>(I);
   } else {
     const long long grid = nwork < (long long)nsm * per_sm[dev] ? nwork : (long long)nsm * per_sm[dev];
     e = cudaMemsetAsync(M.inst[0].work_next, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    k_fast_horiz<TX, TY, TB><<<(unsigned)grid, NT, smem, st>>>(M, nwork);
+    k_fast_horiz<TX, TY, TB, R><<<(unsigned)grid, NT, smem, st>>>(M, nwork);
   }
   return cudaGetLastError();
 }
 
-template <int TX, int TY, int TB>
+template <int TX, int TY, int TB, typename R>
 static cudaError_t launch_tile(const MultiInst &M, cudaStream_t st) {
-  return M.n == 1 ? launch_tile_n<TX, TY, TB, true>(M, st) : launch_tile_n<TX, TY, TB, false>(M, st);
+  return M.n == 1 ? launch_tile_n<TX, TY, TB, true, R>(M, st) : launch_tile_n<TX, TY, TB, false, R>(M, st);
 }
 
 int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax) {
@@ -1151,16 +1177,21 @@ int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax) {
 
 cudaError_t fast_build_offsets(const FastInst &I, float *off, cudaStream_t st) {
   const long long n = (long long)I.lall * I.gall;
-  k_fast_offsets<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(I, off);
+  k_fast_offsets<float><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(I, off);
+  return cudaGetLastError();
+}
+cudaError_t fast_build_offsets64(const FastInst &I, double *off, cudaStream_t st) {
+  const long long n = (long long)I.lall * I.gall;
+  k_fast_offsets<double><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(I, off);
   return cudaGetLastError();
 }
 
 cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
                             long long &launches) {
   if (M.n < 1 || M.n > kMaxInst) return cudaErrorInvalidValue;
-  long long nbk = 0, nsk = 0, npl = 0, nc = 0, nvb = 0, nfk = 0;
+  long long nbk = 0, nsk = 0, npl = 0, nc = 0, nvb = 0, nvb64 = 0, nfk = 0;
   int kmax = 0;
-  constexpr int TV = 4;
+  constexpr int TV = 4, TV64 = 2;  // tracers per column thread: FP32, FP64 variant
   for (int i = 0; i < M.n; ++i) {
     const FastInst &I = M.inst[i];
     const long long n = I.gmax - I.gmin + 1, ncol = (long long)I.lall * n * n;
@@ -1170,6 +1201,7 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
     npl += (long long)kLallPl * I.ntr;
     nc += (long long)I.ncarry * I.K;
     nvb += (long long)((I.ntr + TV - 1) / TV) * ((ncol + 255) / 256);
+    nvb64 += (long long)((I.ntr + TV64 - 1) / TV64) * ((ncol + 255) / 256);
     kmax = I.K > kmax ? I.K : kmax;
   }
   k_fast_boundary<<<(unsigned)((nbk + 127) / 128), 128, 0, st>>>(M);
@@ -1178,20 +1210,38 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
   else if (kmax <= 128) k_fast_pole<128><<<(unsigned)((npl + 63) / 64), 64, 0, st>>>(M);
   else return cudaErrorInvalidValue;
   if (ev0) cudaEventRecord(ev0, st);
-  k_fast_faces<<<(unsigned)((nfk + 127) / 128), 128, 0, st>>>(M);
+  const bool f64 = M.inst[0].f64 != 0;
+  for (int i = 1; i < M.n; ++i)
+    if ((M.inst[i].f64 != 0) != f64) return cudaErrorInvalidValue;  // one precision per batch
   cudaError_t e;
-  switch (shape) {
-    case 0: e = launch_tile<16, 16, 4>(M, st); break;
-    case 1: e = launch_tile<16, 16, 8>(M, st); break;
-    case 2: e = launch_tile<16, 16, 2>(M, st); break;
-    case 3: e = launch_tile<14, 14, 4>(M, st); break;
-    case 4: e = launch_tile<32, 8, 4>(M, st); break;
-    default: return cudaErrorInvalidValue;
+  if (!f64) {
+    k_fast_faces<float><<<(unsigned)((nfk + 127) / 128), 128, 0, st>>>(M);
+    switch (shape) {
+      case 0: e = launch_tile<16, 16, 4, float>(M, st); break;
+      case 1: e = launch_tile<16, 16, 8, float>(M, st); break;
+      case 2: e = launch_tile<16, 16, 2, float>(M, st); break;
+      case 3: e = launch_tile<14, 14, 4, float>(M, st); break;
+      case 4: e = launch_tile<32, 8, 4, float>(M, st); break;
+      default: return cudaErrorInvalidValue;
+    }
+  } else {  // FP64 variant: the same tiles, 2 tracers per batch (FP64 shared data and registers)
+    k_fast_faces<double><<<(unsigned)((nfk + 127) / 128), 128, 0, st>>>(M);
+    switch (shape) {
+      case 0: case 1: case 2: e = launch_tile<16, 16, 2, double>(M, st); break;
+      case 3: e = launch_tile<14, 14, 2, double>(M, st); break;
+      case 4: e = launch_tile<32, 8, 2, double>(M, st); break;
+      default: return cudaErrorInvalidValue;
+    }
   }
   if (ev1) cudaEventRecord(ev1, st);
   if (e != cudaSuccess) return e;
-  if (M.n == 1) k_fast_vert1<TV><<<(unsigned)nvb, 256, 0, st>>>(M.inst[0]);
-  else k_fast_vert<TV><<<(unsigned)nvb, 256, 0, st>>>(M);
+  if (!f64) {
+    if (M.n == 1) k_fast_vert1<TV, float><<<(unsigned)nvb, 256, 0, st>>>(M.inst[0]);
+    else k_fast_vert<TV, float><<<(unsigned)nvb, 256, 0, st>>>(M);
+  } else {
+    if (M.n == 1) k_fast_vert1<TV64, double><<<(unsigned)nvb64, 256, 0, st>>>(M.inst[0]);
+    else k_fast_vert<TV64, double><<<(unsigned)nvb64, 256, 0, st>>>(M);
+  }
   k_fast_carry<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(M);
   launches += 7;
   return cudaGetLastError();

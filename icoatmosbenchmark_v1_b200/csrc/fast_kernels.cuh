@@ -12,11 +12,13 @@ int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax);
 // Per-face remap offsets (GRD_xr - GRD_x of the owner and of the neighbour, FP32) into
 // off (lall, 18, gall); needs I's geometry pointers only.
 cudaError_t fast_build_offsets(const FastInst &I, float *off, cudaStream_t st);
+cudaError_t fast_build_offsets64(const FastInst &I, double *off, cudaStream_t st);  // the same in FP64
 // One step of instance I on stream st with tile shape `shape` (of k_fast_horiz); ev0/ev1
 // (optional) are recorded around k_fast_horiz, the dominant launch.
 cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
                       long long &launches);
-// The same step for M.n grid instances (uneven grid levels) together: each kernel is one
+// The same step for M.n grid instances (uneven grid levels) together, all of one precision
+// (FastInst::f64: the FP32 or the FP64 variant): each kernel is one
 // launch over the work of every instance; the horizontal kernel is persistent (one wave of
 // CTAs striding over all (instance, level, tile) items).  Launches nothing that allocates,
 // so it can be captured in a CUDA graph once every instance has run one step uncaptured.

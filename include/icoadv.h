@@ -325,6 +325,18 @@ int ica_advect_fast(ica_ctx *ctx, int ntr, double dt,
                     const float *rhogvy, const float *rhogvy_pl,
                     const float *rhogvz, const float *rhogvz_pl,
                     const float *rhogw, const float *rhogw_pl);
+/* FP64 variant of the batched step: the same kernels with every face value, bound,
+ * Courant number and limiter in FP64 and FP64 fields, so the result follows the plain
+ * FP64 step to FP64 rounding (the FP32 variant differs from it at FP32 rounding). */
+int ica_advect_fast64_dev(ica_ctx *ctx, int ntr, double dt,
+                          const double *rhog_in, const double *rhog_in_pl,
+                          const double *rhogq_in, const double *rhogq_in_pl,
+                          double *rhog_out, double *rhog_out_pl,
+                          double *rhogq_out, double *rhogq_out_pl,
+                          const double *rhogvx, const double *rhogvx_pl,
+                          const double *rhogvy, const double *rhogvy_pl,
+                          const double *rhogvz, const double *rhogvz_pl,
+                          const double *rhogw, const double *rhogw_pl);
 /* Tile shapes of the horizontal kernel (TX x TY cells, TG tracers per batch): *n shapes;
  * tx/ty/tg (may be NULL) receive them.  ica_fast_set_shape selects one (the
  * autotuner in the Python layer times them and keeps the fastest). */
@@ -358,8 +370,19 @@ int ica_batch_destroy(ica_batch *b);
 int ica_batch_set_shape(ica_batch *b, int shape);
 /* One step of every instance (args[i] for instance i), device pointers, asynchronous. */
 int ica_batch_step_dev(ica_batch *b, const ica_fast_args *args);
+/* The FP64 variant of a batch: FP64 fields (ica_fast_args64); all instances of a step
+ * use one variant. */
+typedef struct {
+  int ntr;
+  double dt;
+  const double *rhog_in, *rhog_in_pl, *rhogq_in, *rhogq_in_pl;
+  double *rhog_out, *rhog_out_pl, *rhogq_out, *rhogq_out_pl;
+  const double *rhogvx, *rhogvx_pl, *rhogvy, *rhogvy_pl, *rhogvz, *rhogvz_pl, *rhogw, *rhogw_pl;
+} ica_fast_args64;
+int ica_batch_step64_dev(ica_batch *b, const ica_fast_args64 *args);
 /* Capture the step with these arguments into graph slot 0 or 1 (replacing what was there). */
 int ica_batch_capture(ica_batch *b, const ica_fast_args *args, int slot);
+int ica_batch_capture64(ica_batch *b, const ica_fast_args64 *args, int slot);
 /* Launch the graph in slot 0 or 1 on the batch stream. */
 int ica_batch_replay(ica_batch *b, int slot);
 

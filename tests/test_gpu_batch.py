@@ -135,3 +135,58 @@ def test_batch_mass_conservation_uneven():
     finally:
         for ctx in ctxs:
             ctx.close()
+
+
+def test_fp64_variant_batch_against_oracle(O):
+    """The FP64 variant of the batched step (FP64 fields, faces and limiters in the same
+    persistent launches, replayed from the captured CUDA graph): uneven pair, 3 steps, within
+    1e-11 of the FP64 oracle (the operation order differs from the plain step's)."""
+    import torch
+    from icoatmosbenchmark_v1_b200 import api
+    cs = [case(*p) for p in PAIRS[1]]
+    ctxs = [_ctx(c["grid"]) for c in cs]
+    try:
+        refs = []
+        for c in cs:
+            S = {k: v.copy() for k, v in c["state"].items()}
+            for _ in range(3):
+                O.step(c["dims"], c["grid"].have_sgp, c["topo"], c["dt"], S, c["fields"], c["grid"].arrays,
+                       nthreads=8)
+            refs.append(S)
+        br = api.BatchRunner(ctxs, [_dev(c["state"]) for c in cs], [_dev(c["fields"]) for c in cs],
+                             [c["dt"] for c in cs], shape=3, f64=True)
+        br.step()
+        br.use_graph()
+        br.step()
+        br.step()
+        torch.cuda.synchronize()
+        for got, ref in zip(br.states, refs):
+            for k in ref:
+                assert rel_err(got[k].cpu().numpy(), ref[k]) <= 1e-11, k
+        br.close()
+    finally:
+        for ctx in ctxs:
+            ctx.close()
+
+
+@pytest.mark.parametrize("glevel,rlevel,kall,ntr", [(5, 0, 42, 3), (4, 1, 10, 2)])
+def test_fp64_variant_single_grid_against_plain_step(glevel, rlevel, kall, ntr):
+    """ica_advect_fast64_dev against the plain FP64 step on the same inputs, 3 steps: 1e-11."""
+    import torch
+    c = case(glevel, rlevel, kall, ntr)
+    g, f = c["grid"], c["fields"]
+    ctx = _ctx(g)
+    try:
+        P = _dev(c["state"])
+        A, B = _dev(c["state"]), {k: torch.empty_like(v) for k, v in _dev(c["state"]).items()}
+        fd = _dev(f)
+        for _ in range(3):
+            ctx.advect_step(c["dt"], P["rhog"], P["rhog_pl"], P["rhogq"], P["rhogq_pl"], fd["rhogvx"], fd["rhogvx_pl"],
+                            fd["rhogvy"], fd["rhogvy_pl"], fd["rhogvz"], fd["rhogvz_pl"], fd["rhogw"], fd["rhogw_pl"])
+            ctx.advect_fast64_dev(c["dt"], A, B, fd)
+            A, B = B, A
+        torch.cuda.synchronize()
+        for k in P:
+            assert rel_err(A[k].cpu().numpy(), P[k].cpu().numpy()) <= 1e-11, k
+    finally:
+        ctx.close()
