@@ -333,10 +333,10 @@ def tracer_mass(g, S):
 
 def run_uneven(args, world, rank, local):
     """Batch of two uneven grid instances (glevel 7 / kall 96 / 40 tracers and glevel 6 / kall 42 /
-    12 tracers) advanced by the same launches and replayed from a CUDA graph (FP32 variant);
-    the FP64 variant is the plain per-tracer path of each instance.  Reports the FP32 variant's
-    max relative error against the FP64 path after one step and the relative mass drift over the
-    timed steps."""
+    12 tracers) advanced by the same launches and replayed from a CUDA graph, in the FP32 variant
+    (the line's value) and the FP64 variant (`fp64_variant`).  Each reports its max relative
+    error against the plain FP64 step after one step and the relative mass drift over the
+    timed steps; the plain FP64 step of both instances is timed beside them."""
     import torch
 
     from icoatmosbenchmark_v1_b200 import api
@@ -365,6 +365,7 @@ def run_uneven(args, world, rank, local):
                         f["rhogvy"], f["rhogvy_pl"], f["rhogvz"], f["rhogvz_pl"], f["rhogw"], f["rhogw_pl"])
         del S
     ref = [{k: v.clone() for k, v in st.items()} for st in sts]
+    init = [{k: v.clone() for k, v in st.items()} for st in sts]  # the FP32 runner advances sts in place
     torch.cuda.synchronize()
     t64 = time.perf_counter()
     for ctx, S, f, dt in zip(ctxs, ref, fs, dts):
@@ -410,6 +411,29 @@ def run_uneven(args, world, rank, local):
     ms = e0.elapsed_time(e1) / args.steps
     m1 = masses(br.states)
     drift = max(float(((b - a).abs() / a.abs()).max().item()) for a, b in zip(m0, m1))
+    br.close()
+    del br
+    torch.cuda.empty_cache()
+    # FP64 variant of the same batch: the same launches in FP64 (fields, faces, limiters)
+    b64 = api.BatchRunner(ctxs, init, fs, dts, shape=best[0], f64=True)
+    m0 = masses(b64.states)
+    b64.step()
+    torch.cuda.synchronize()
+    err64 = max(float(((a["rhogq"] - b["rhogq"]).abs().max() / b["rhogq"].abs().max()).item())
+                for a, b in zip(b64.states, ref))
+    b64.use_graph()
+    for _ in range(args.warmup):
+        b64.step()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        b64.step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_f64 = e0.elapsed_time(e1) / args.steps
+    m1 = masses(b64.states)
+    drift64 = max(float(((b - a).abs() / a.abs()).max().item()) for a, b in zip(m0, m1))
+    b64.close()
     if rank == 0:
         shape = list(ctxs[0].fast_shapes()[best[0]])
         line = {"metric": METRIC, "value": upd / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -421,9 +445,11 @@ def run_uneven(args, world, rank, local):
                            "tile": {"shape_txtytg": shape, "autotune_ms": tuning}},
                 "fp64_plain_ms_per_step": ms64, "max_rel_err_vs_fp64": err,
                 "mass_drift": {"value": drift, "steps": args.steps + args.warmup},
+                "fp64_variant": {"ms_per_step": ms_f64, "value": upd / (ms_f64 * 1e-3),
+                                 "max_rel_err_vs_fp64_plain": err64,
+                                 "mass_drift": {"value": drift64, "steps": 1 + args.steps + args.warmup}},
                 "gpu_launches": None, "clocks": clocks}
         print(json.dumps(line), flush=True)
-    br.close()
     for c in ctxs:
         c.close()
 
