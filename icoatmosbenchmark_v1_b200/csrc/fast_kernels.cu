@@ -372,19 +372,22 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
     }
     I.Fg[(size_t)a * n3 + o] = F;
 #pragma unroll
-    for (int x = 0; x < 3; ++x) if (sizeof(R) == 8) I.Dg64[(size_t)(a * 3 + x) * n3 + o] = d[x];
-    else I.Dg[(size_t)(a * 3 + x) * n3 + o] = (float)d[x];
+    for (int x = 0; x < 3; ++x) {
+      if (sizeof(R) == 8) I.Dg64[(size_t)(a * 3 + x) * n3 + o] = d[x];
+      else I.Dg[(size_t)(a * 3 + x) * n3 + o] = (float)d[x];
+    }
   }
 }
 
 // Threshold of the upwind masks (0.5 - sign(0.5, ch - EPS)) and of the zero-outflow guards
-// (zerosw) in the FP32 arithmetic: the FP64 EPS, not epsilon(1.0).  These are switches, not
+// (zerosw) in either arithmetic: the FP64 EPS, also in FP32, not epsilon(1.0).  These are switches, not
 // roundings: with FP32's own EPS a face whose Courant number lies in (2.2e-16, 1.2e-7) is
 // taken from the other side than in FP64, which moves its 4-point bounds into or out of the
 // cell's qnext; at a slotted-cylinder edge (glevel 7, kall 96) that gave 9e-4 relative error
 // against the FP64 oracle in 10 cells.  With the FP64 threshold the same run is at 1.6e-7.
 // (The standalone *_f32 kernel entry points keep the reference's RP = SP semantics.)
-constexpr float kEpsThr = (float)DBL_EPSILON;
+template <typename R>
+__device__ __forceinline__ R eps_thr() { return (R)DBL_EPSILON; }
 
 // ---- vertical Thuburn limiter (dyn_vert_adv_limiter/src/mod_src_tracer.f90:107-186), d = 0, FP32:
 // the tracer-independent part of a level (upwind flags, Courant sums) and the per-tracer bounds
@@ -405,7 +408,7 @@ __device__ __forceinline__ VLim<R> vlim_params(R c1, R c2, R c1p) {
   const R Cin = v.a1 + v.a2;
   const R Cout = (R(1.0) - v.infl) * c1 + (R(1.0) - infu) * c2;
   v.icm = Cin + Cout;
-  v.zsw = R(0.5) - A::sgn(R(0.5), fabs(Cout) - R(DBL_EPSILON));
+  v.zsw = R(0.5) - A::sgn(R(0.5), fabs(Cout) - eps_thr<R>());
   v.rden = (R(1.0) - v.zsw) / (Cout + v.zsw);
   return v;
 }
@@ -469,7 +472,7 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   const size_t base = (size_t)l * lk + (size_t)k * slab;
   const double dt = I.dt;
   const R dtf = (R)dt;
-  const R BIGf = A::BIG, EPSf = R(DBL_EPSILON);
+  const R BIGf = A::BIG, EPSf = eps_thr<R>();
 
   // this thread's ring cell
   const bool ring = tid < NR;
