@@ -1,0 +1,195 @@
+"""Kernel snapshots in the reference drivers' binary format (dumpio.c): the reader and writer
+on CPU, and, on the GPU, the library run on snapshots whose expected outputs the oracle
+wrote.  The snapshots are synthetic: region 0 of a glevel-4 grid (gall_1d 18) with the poles,
+the form of the drivers' one-region-per-process snapshots at a small size."""
+import numpy as np
+import pytest
+
+from cases import case
+from icoatmosbenchmark_v1_b200 import snapshot as S
+
+DIMS = S.SnapshotDims(gall_1d=18, kall=8)
+
+
+def _one_region(a):
+    """Region 0 of a [..., L, K, G] array."""
+    return np.ascontiguousarray(np.asarray(a)[..., :1, :, :])
+
+
+def _geo_one_region(a, pole):
+    """A library geometry array ([..., L, G] or pole [..., LP, P]) in the driver's form with
+    the K0 axis: [..., L, 1, G]."""
+    a = np.asarray(a)
+    if not pole:
+        a = a[..., :1, :]
+    return np.ascontiguousarray(a[..., None, :])
+
+
+def synthetic_snapshots(tmp_path, O):
+    """Writes the three drivers' snapshots from oracle outputs; returns {kernel: path}."""
+    c = case(4, 0, 8, 1)
+    g, d, f = c["grid"], c["dims"], c["fields"]
+    paths = {}
+
+    arr = dict(flx_h=_one_region(c["flx"]), flx_h_pl=c["flx_pl"], GRD_xc=_one_region(c["xc"]), GRD_xc_pl=c["xc_pl"],
+               rho=_one_region(f["rhog"]), rho_pl=f["rhog_pl"])
+    for v in ("x", "y", "z"):
+        arr[f"rhov{v}"] = _one_region(f[f"rhogv{v}"])
+        arr[f"rhov{v}_pl"] = f[f"rhogv{v}_pl"]
+    for k, v in c["geo"].items():
+        arr[k] = _geo_one_region(v, k.endswith("_pl"))
+    paths["dyn_horiz_adv_flux"] = tmp_path / S.file_name("dyn_horiz_adv_flux")
+    S.write_snapshot("dyn_horiz_adv_flux", paths["dyn_horiz_adv_flux"], arr, DIMS)
+
+    args = (d, g.have_sgp, c["qa"], c["qa_pl"], c["q"], c["q_pl"], c["d"], c["d_pl"], c["ch"], c["ch_pl"],
+            c["cm"], c["cm_pl"])
+    qa, qa_pl, qo, qo_pl = O.horizontal_limiter(*args, topo=c["topo"])
+    post, post_pl = qo.copy(), qo_pl.copy()
+    c["topo"].data_transfer([post], [post_pl])
+    arr = dict(q_a_prev=_one_region(c["qa"]), q_a_prev_pl=c["qa_pl"], q_a=_one_region(qa), q_a_pl=qa_pl,
+               q=_one_region(c["q"]), q_pl=c["q_pl"], d=_one_region(c["d"]), d_pl=c["d_pl"],
+               ch=_one_region(c["ch"]), ch_pl=c["ch_pl"], cmask=_one_region(c["cm"]), cmask_pl=c["cm_pl"],
+               Qout_prev=_one_region(qo), Qout_prev_pl=qo_pl, Qout_post=_one_region(post), Qout_post_pl=post_pl)
+    paths["dyn_horiz_adv_limiter"] = tmp_path / S.file_name("dyn_horiz_adv_limiter")
+    S.write_snapshot("dyn_horiz_adv_limiter", paths["dyn_horiz_adv_limiter"], arr, DIMS)
+
+    from cases import vertical_inputs
+    qh, qh_pl, ck, ck_pl = vertical_inputs(c)
+    rqh, rqh_pl = O.vertical_limiter(d, qh, qh_pl, c["q"], c["q_pl"], c["d"], c["d_pl"], ck, ck_pl)
+    arr = dict(q_h_prev=_one_region(qh), q_h_prev_pl=qh_pl, q_h=_one_region(rqh), q_h_pl=rqh_pl,
+               q=_one_region(c["q"]), q_pl=c["q_pl"], d=_one_region(c["d"]), d_pl=c["d_pl"],
+               ck=_one_region(ck), ck_pl=ck_pl)
+    paths["dyn_vert_adv_limiter"] = tmp_path / S.file_name("dyn_vert_adv_limiter")
+    S.write_snapshot("dyn_vert_adv_limiter", paths["dyn_vert_adv_limiter"], arr, DIMS)
+    return paths, c["dt"]
+
+
+@pytest.fixture(scope="module")
+def O(built):
+    from oracle import oracle
+    return oracle
+
+
+def test_reference_snapshot_sizes():
+    """The reference's snapshots (gall_1d 130, kall 42, one region and the poles) hold these
+    many 8-byte reals: the sums of the drivers' array extents."""
+    def nbytes(kernel):
+        return 8 * sum(int(np.prod(e)) for _, e, _ in S.layout(kernel))
+    G, K, P = 130 * 130, 42, 6
+    assert nbytes("dyn_vert_adv_limiter") == 8 * (G * K * (4 + 2) + P * K * 2 * (4 + 2))
+    assert nbytes("dyn_horiz_adv_limiter") == 8 * (G * K * (6 * 4 + 1 + 1 + 2 * 2)
+                                                   + P * K * 2 * (4 + 1 + 1 + 2 * 2))
+    assert nbytes("dyn_horiz_adv_flux") == 8 * (G * K * (6 + 9 + 4) + P * K * 2 * (1 + 3 + 4)
+                                                + G * (9 + 8 + 10 + 36) + P * 2 * (3 + 8 + 5 + 18))
+    assert S.file_name("dyn_horiz_adv_flux", 3) == "snapshot.dyn_horiz_adv_flux.pe000003"
+
+
+def test_snapshot_round_trip_big_endian(tmp_path):
+    """Arrays come back as written; the file is big-endian float64 in Fortran (column-major)
+    order, one array after the other with no record markers."""
+    rng = np.random.default_rng(3)
+    lay = S.layout("dyn_vert_adv_limiter", DIMS)
+    arr = {n: rng.standard_normal(e[::-1]) for n, e, _ in lay}
+    p = tmp_path / "snap"
+    S.write_snapshot("dyn_vert_adv_limiter", p, arr, DIMS)
+    raw = p.read_bytes()
+    assert len(raw) == 8 * sum(a.size for a in arr.values())
+    # first array, Fortran order: q_h_prev(ij, k, l) with ij fastest
+    first = arr["q_h_prev"]
+    assert np.frombuffer(raw[:8], ">f8")[0] == first[0, 0, 0]
+    assert np.frombuffer(raw[8:16], ">f8")[0] == first[0, 0, 1]
+    assert np.frombuffer(raw[8 * DIMS.gall:8 * DIMS.gall + 8], ">f8")[0] == first[0, 1, 0]
+    back = S.read_snapshot("dyn_vert_adv_limiter", p, DIMS)
+    assert list(back) == [n for n, _, _ in lay]
+    for n in arr:
+        np.testing.assert_array_equal(back[n], arr[n])
+    with pytest.raises(ValueError):
+        S.read_snapshot("dyn_horiz_adv_limiter", p, DIMS)
+    with pytest.raises(ValueError):
+        S.write_snapshot("dyn_vert_adv_limiter", p, {**arr, "ck": arr["ck"][:1]}, DIMS)
+
+
+def test_value_check_format():
+    line = S.value_check("check_q_h", np.array([1.0, -2.0, 0.5]))
+    assert line.startswith(" +check[check_q_h       ] max=  1.0000000000000000E+00,min= -2.0000000000000000E+00")
+    assert line.endswith("sum= -5.0000000000000000E-01")
+
+
+def test_synthetic_snapshots_read_back(tmp_path, O):
+    paths, _ = synthetic_snapshots(tmp_path, O)
+    for kernel, p in paths.items():
+        s = S.read_snapshot(kernel, p, DIMS)
+        assert all(np.isfinite(v).all() for v in s.values())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", S.KERNELS)
+def test_run_snapshot_matches_expected(tmp_path, O, cuda, kernel):
+    """The library on a snapshot reproduces the snapshot's expected outputs: bit-exact for the
+    flux and the two limiters (FP64 kernels built without contraction)."""
+    paths, dt = synthetic_snapshots(tmp_path, O)
+    got, diffs = S.run_snapshot(kernel, paths[kernel], DIMS, dt=dt)
+    assert list(diffs) == [n for n, _, out in S.layout(kernel, DIMS) if out]
+    for name, dv in diffs.items():
+        assert np.isfinite(got[name]).all()
+        assert np.abs(dv).max() == 0.0, (name, np.abs(dv).max())
+
+
+class _OracleCtx:
+    """Stands in for api.IcoAdv on CPU (same methods, in-place outputs), computing with the
+    oracle, so that the snapshot plumbing (region embedding, geometry without the K0 axis,
+    the driver's initial output values) is checked without a GPU."""
+
+    def __init__(self, glevel, rlevel, vlayer, device=0):
+        from icoatmosbenchmark_v1_b200.grid import Grid
+        from oracle import oracle
+        self.O, self.g = oracle, Grid(glevel, rlevel, vlayer + 2)
+        self.d = oracle.make_dims(glevel, rlevel, vlayer + 2)
+        self.sizes = type("Sizes", (), {"lall": self.g.lall})()
+
+    def set_geometry(self, *geo):
+        names = ("GRD_xr", "GRD_xr_pl", "GMTR_p", "GMTR_p_pl", "GMTR_t", "GMTR_t_pl", "GMTR_a", "GMTR_a_pl")
+        ref = self.g.geometry()
+        for n, a in zip(names, geo):
+            assert a.shape == ref[n].shape, (n, a.shape, ref[n].shape)
+        self.geo = dict(zip(names, geo))
+
+    def horizontal_flux(self, flx, flx_pl, xc, xc_pl, rho, rho_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, dt):
+        a, ap, x, xp = self.O.horizontal_flux(self.d, self.g.have_sgp, rho, rho_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl,
+                                              dt, self.geo)
+        flx[...], xc[...] = a, x
+        flx_pl[:, :, 1:], xc_pl[..., 1:] = ap[:, :, 1:], xp[..., 1:]  # pole centre not written
+
+    def horizontal_limiter_thuburn(self, qa, qa_pl, q, q_pl, d, d_pl, ch, ch_pl, cm, cm_pl, qo, qo_pl, post, post_pl):
+        a, ap, o, op = self.O.horizontal_limiter(self.d, self.g.have_sgp, qa, qa_pl, q, q_pl, d, d_pl, ch, ch_pl, cm,
+                                                 cm_pl, Qout_post=post, Qout_post_pl=post_pl)
+        qa[...], qa_pl[...], qo[...], qo_pl[...] = a, ap, o, op
+
+    def vertical_limiter_thuburn(self, qh, qh_pl, q, q_pl, d, d_pl, ck, ck_pl):
+        a, ap = self.O.vertical_limiter(self.d, qh, qh_pl, q, q_pl, d, d_pl, ck, ck_pl)
+        qh[...], qh_pl[...] = a, ap
+
+    def close(self):
+        pass
+
+
+@pytest.mark.parametrize("kernel", S.KERNELS)
+def test_run_snapshot_plumbing_with_oracle(tmp_path, O, monkeypatch, kernel):
+    """run_snapshot's embedding of the snapshot's region in a whole grid, with the oracle in
+    place of the CUDA library: the region's outputs come back equal to the expected ones."""
+    from icoatmosbenchmark_v1_b200 import api
+    monkeypatch.setattr(api, "IcoAdv", _OracleCtx)
+    paths, dt = synthetic_snapshots(tmp_path, O)
+    got, diffs = S.run_snapshot(kernel, paths[kernel], DIMS, dt=dt)
+    for name, dv in diffs.items():
+        assert got[name].shape == S.read_snapshot(kernel, paths[kernel], DIMS)[name].shape
+        assert np.abs(dv).max() == 0.0, (name, np.abs(dv).max())
+
+
+def test_cli_check_prints_driver_summaries(tmp_path, O, capsys):
+    paths, _ = synthetic_snapshots(tmp_path, O)
+    S.main(["check", "dyn_vert_adv_limiter", str(paths["dyn_vert_adv_limiter"]), "--gall-1d", "18", "--kall", "8"])
+    out = capsys.readouterr().out.splitlines()
+    assert out[0].strip() == "### Input ###"
+    assert [ln.split("]")[0].split("[")[1].strip() for ln in out[1:]] == \
+        [n for n, _, _ in S.layout("dyn_vert_adv_limiter", DIMS)]
