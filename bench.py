@@ -547,6 +547,8 @@ def measure_e2e(args, ctx, g, st, f, dt, upd, world):
         v.numel() * v.element_size() for v in hf.values())
     d2h = sum(v.numel() * v.element_size() for v in host.values())
     call = ctx.advect_step if args.mode == "plain" else ctx.advect_fast_host
+    if args.mode != "plain":
+        ctx.fast_set_host_chunk(args.host_chunk)
     call(dt, **_step_kwargs(hn, hfn))  # warm (allocates staging once)
     torch.cuda.synchronize()
     barrier(world)
@@ -586,6 +588,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=12, help="steps of the adjoint sweep")
     ap.add_argument("--adjoint-every", type=int, default=4, help="checkpoint interval of the adjoint sweep")
     ap.add_argument("--tile-shape", type=int, default=-1, help="tile shape index of the horizontal kernel (default: autotune)")
+    ap.add_argument("--host-chunk", type=int, default=0,
+                    help="tracers per chunk of the host-pointer step's overlapped copies (default 0: by size)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")
     args = ap.parse_args()

@@ -346,6 +346,10 @@ class IcoAdv:
     def fast_set_shape(self, shape):
         _check("ica_fast_set_shape", lib().ica_fast_set_shape(self.h, int(shape)))
 
+    def fast_set_host_chunk(self, tracers):
+        """Tracers per chunk of advect_fast_host's overlapped copies (0: by size)."""
+        _check("ica_fast_set_host_chunk", lib().ica_fast_set_host_chunk(self.h, int(tracers)))
+
     def fast_timing(self, enable):
         ms = C.c_double()
         n = C.c_longlong()

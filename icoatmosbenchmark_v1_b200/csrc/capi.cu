@@ -187,6 +187,17 @@ Ctx::~Ctx() {
     if (p) cudaFree(p);
   for (auto &ev : fast.events) cudaEventDestroy(ev.first), cudaEventDestroy(ev.second);
   if (stream) cudaStreamDestroy(stream);
+  if (copy_in) cudaStreamDestroy(copy_in);
+  if (copy_out) cudaStreamDestroy(copy_out);
+}
+
+int Ctx::copy_streams() {
+  for (cudaStream_t *s : {&copy_in, &copy_out})
+    if (!*s) {
+      cudaError_t e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate(copy)");
+    }
+  return ICA_OK;
 }
 
 int Ctx::upload_geometry(const double *const h[8], const size_t n[8]) {
@@ -990,6 +1001,13 @@ int ica_fast_set_shape(ica_ctx *c, int shape) {
   return ICA_OK;
 }
 
+int ica_fast_set_host_chunk(ica_ctx *c, int tracers) {
+  CTX_OK(c);
+  if (tracers < 0) return set_error("ica_fast_set_host_chunk: tracers must be >= 0"), ICA_ERR_ARG;
+  c->host_chunk = tracers;
+  return ICA_OK;
+}
+
 int ica_fast_timing(ica_ctx *c, int enable, double *ms_total, long long *count) {
   CTX_OK(c);
   cudaSetDevice(c->device);
@@ -1056,6 +1074,98 @@ static int advect_fast_impl(Ctx *c, int ntr, double dt, const double *rhog_in, c
   launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, ntr, rhogq_out, rhogq_out_pl, c->stream);
   c->launches += 2;
   return c->check_launch("ica_advect_fast");
+}
+
+
+// Tracers per chunk of the host-pointer step.  The state crosses the host link in chunks: the
+// copy of chunk c+1 in and of chunk c-1 out run on their own streams while the step works on
+// chunk c, so a step costs about one pass of the state over the link instead of two, plus the
+// last chunk's way out.  By size: about 1 GiB of rhogq per chunk, 1 to 4 tracers (four
+// tracers are one batch of the horizontal kernel's widest shape).  At glevel 8, kall 96 that
+// is 2 tracers: 434 ms per 32-tracer step on a B200 against 602 ms with 1 tracer per chunk,
+// whose step no longer keeps up with its copies, and 453 ms with 4.
+static int host_chunk_tracers(const Ctx *c, int ntr) {
+  if (c->host_chunk > 0) return std::min(ntr, c->host_chunk);
+  const size_t per = (size_t)c->sz.gall * c->sz.kall * c->sz.lall * sizeof(double);
+  const int t = (int)std::max<size_t>(1, std::min<size_t>(4, ((size_t)1 << 30) / per));
+  return std::min(ntr, t);
+}
+
+static int advect_fast_chunked(Ctx *c, int ntr, double dt, double *rhog, double *rhog_pl, double *rhogq,
+                               double *rhogq_pl, const float *vx, const float *vx_pl, const float *vy,
+                               const float *vy_pl, const float *vz, const float *vz_pl, const float *w,
+                               const float *w_pl) {
+  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
+  const int tc = host_chunk_tracers(c, ntr), nch = (ntr + tc - 1) / tc;
+  auto dbl = [&](const char *n, size_t k) { return (double *)c->buf(n, k * sizeof(double)); };
+  auto flt = [&](const char *n, size_t k) { return (float *)c->buf(n, k * sizeof(float)); };
+  // rho in, rho out (chunk 0; the later chunks recompute the same values into a scratch copy)
+  double *r0 = dbl("f0", n3), *r0p = dbl("f1", n3p), *r1 = dbl("f4", n3), *r1p = dbl("f5", n3p);
+  double *rs = nch > 1 ? dbl("f8", n3) : r1, *rsp = nch > 1 ? dbl("f9", n3p) : r1p;
+  double *qi[2] = {dbl("fq0", n3 * tc), nch > 1 ? dbl("fq1", n3 * tc) : nullptr};
+  double *qip[2] = {dbl("fqp0", n3p * tc), nch > 1 ? dbl("fqp1", n3p * tc) : nullptr};
+  double *qo[2] = {dbl("fr0", n3 * tc), nch > 1 ? dbl("fr1", n3 * tc) : nullptr};
+  double *qop[2] = {dbl("frp0", n3p * tc), nch > 1 ? dbl("frp1", n3p * tc) : nullptr};
+  const float *hf[8] = {vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl};
+  float *df[8];
+  static const char *fname[8] = {"g0", "g1", "g2", "g3", "g4", "g5", "g6", "g7"};
+  bool ok = r0 && r0p && r1 && r1p && rs && rsp;
+  for (int h = 0; h < (nch > 1 ? 2 : 1); ++h) ok = ok && qi[h] && qip[h] && qo[h] && qop[h];
+  for (int v = 0; v < 8; ++v) ok = ok && (df[v] = flt(fname[v], (v & 1) ? n3p : n3)) != nullptr;
+  if (!ok) return set_error("ica_advect_fast: cudaMalloc of the staging buffers"), ICA_ERR_NOMEM;
+
+  cudaEvent_t ev[7] = {};  // fields in, chunk in x2, step done x2, chunk out x2
+  for (auto &e : ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      for (auto &x : ev)
+        if (x) cudaEventDestroy(x);
+      return set_error("ica_advect_fast: cudaEventCreate"), ICA_ERR_CUDA;
+    }
+  cudaEvent_t ev_f = ev[0], *ev_in = ev + 1, *ev_step = ev + 3, *ev_out = ev + 5;
+  cudaStream_t sin = c->copy_in, sout = c->copy_out, sc = c->stream;
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+  chk(cudaMemcpyAsync(r0, rhog, n3 * sizeof(double), cudaMemcpyHostToDevice, sin));
+  chk(cudaMemcpyAsync(r0p, rhog_pl, n3p * sizeof(double), cudaMemcpyHostToDevice, sin));
+  for (int v = 0; v < 8; ++v)
+    chk(cudaMemcpyAsync(df[v], hf[v], ((v & 1) ? n3p : n3) * sizeof(float), cudaMemcpyHostToDevice, sin));
+  chk(cudaEventRecord(ev_f, sin));
+  chk(cudaStreamWaitEvent(sc, ev_f, 0));
+  int rc = ICA_OK;
+  for (int ch = 0; ch < nch && e == cudaSuccess && rc == ICA_OK; ++ch) {
+    const int b = ch & 1, t0 = ch * tc, nt = std::min(tc, ntr - t0);
+    // in: the slot is free once the step of chunk ch-2 has read it
+    if (ch >= 2) chk(cudaStreamWaitEvent(sin, ev_step[b], 0));
+    chk(cudaMemcpyAsync(qi[b], rhogq + (size_t)t0 * n3, n3 * nt * sizeof(double), cudaMemcpyHostToDevice, sin));
+    chk(cudaMemcpyAsync(qip[b], rhogq_pl + (size_t)t0 * n3p, n3p * nt * sizeof(double), cudaMemcpyHostToDevice,
+                        sin));
+    chk(cudaEventRecord(ev_in[b], sin));
+    // step: after its input landed and the output slot of chunk ch-2 went out
+    chk(cudaStreamWaitEvent(sc, ev_in[b], 0));
+    if (ch >= 2) chk(cudaStreamWaitEvent(sc, ev_out[b], 0));
+    if (e != cudaSuccess) break;
+    rc = advect_fast_impl<float>(c, nt, dt, r0, r0p, qi[b], qip[b], ch == 0 ? r1 : rs, ch == 0 ? r1p : rsp, qo[b],
+                                 qop[b], df[0], df[1], df[2], df[3], df[4], df[5], df[6], df[7]);
+    if (rc) break;
+    chk(cudaEventRecord(ev_step[b], sc));
+    // out
+    chk(cudaStreamWaitEvent(sout, ev_step[b], 0));
+    if (ch == 0) {
+      chk(cudaMemcpyAsync(rhog, r1, n3 * sizeof(double), cudaMemcpyDeviceToHost, sout));
+      chk(cudaMemcpyAsync(rhog_pl, r1p, n3p * sizeof(double), cudaMemcpyDeviceToHost, sout));
+    }
+    chk(cudaMemcpyAsync(rhogq + (size_t)t0 * n3, qo[b], n3 * nt * sizeof(double), cudaMemcpyDeviceToHost, sout));
+    chk(cudaMemcpyAsync(rhogq_pl + (size_t)t0 * n3p, qop[b], n3p * nt * sizeof(double), cudaMemcpyDeviceToHost,
+                        sout));
+    chk(cudaEventRecord(ev_out[b], sout));
+  }
+  // all three streams drain before the buffers can be reused or the host reads the state
+  const cudaError_t s1 = cudaStreamSynchronize(sin), s2 = cudaStreamSynchronize(sc), s3 = cudaStreamSynchronize(sout);
+  for (auto &x : ev) cudaEventDestroy(x);
+  if (rc) return rc;
+  chk(s1), chk(s2), chk(s3);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_advect_fast");
+  return ICA_OK;
 }
 
 }  // namespace icoadv
@@ -1243,26 +1353,9 @@ int ica_advect_fast(ica_ctx *c, int ntr, double dt, double *rhog, double *rhog_p
       !w_pl)
     return set_error("ica_advect_fast: NULL argument"), ICA_ERR_ARG;
   cudaSetDevice(c->device);
-  const size_t n3 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall, n3p = (size_t)kGallPl * c->sz.kall * kLallPl;
-  Stage<double> s(c);
-  double *r0 = s.in("f0", rhog, n3), *r0p = s.in("f1", rhog_pl, n3p);
-  double *q0 = s.in("f2", rhogq, n3 * ntr), *q0p = s.in("f3", rhogq_pl, n3p * ntr);
-  double *r1 = s.in("f4", nullptr, n3), *r1p = s.in("f5", nullptr, n3p);
-  double *q1 = s.in("f6", nullptr, n3 * ntr), *q1p = s.in("f7", nullptr, n3p * ntr);
-  Stage<float> sf(c);
-  float *dx = sf.in("g0", vx, n3), *dxp = sf.in("g1", vx_pl, n3p);
-  float *dy = sf.in("g2", vy, n3), *dyp = sf.in("g3", vy_pl, n3p);
-  float *dz = sf.in("g4", vz, n3), *dzp = sf.in("g5", vz_pl, n3p);
-  float *dw = sf.in("g6", w, n3), *dwp = sf.in("g7", w_pl, n3p);
-  if (s.rc) return s.rc;
-  if (sf.rc) return sf.rc;
-  int rc = ica_advect_fast_dev(c, ntr, dt, r0, r0p, q0, q0p, r1, r1p, q1, q1p, dx, dxp, dy, dyp, dz, dzp, dw, dwp);
+  int rc = c->copy_streams();
   if (rc) return rc;
-  s.out(rhog, r1, n3);
-  s.out(rhog_pl, r1p, n3p);
-  s.out(rhogq, q1, n3 * ntr);
-  s.out(rhogq_pl, q1p, n3p * ntr);
-  return s.sync();
+  return advect_fast_chunked(c, ntr, dt, rhog, rhog_pl, rhogq, rhogq_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl);
 }
 
 }  // extern "C"

@@ -53,6 +53,8 @@ struct Ctx {
   Dims D{};
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;  // host-link copies of the chunked host path
+  int host_chunk = 0;                                   // tracers per chunk of that path, 0: by size
   Plan plan[2];               // [0] COMM_data_transfer, [1] COMM_var
   int *d_have_sgp = nullptr;
   void *geo64[8] = {};        // GRD_xr, _pl, GMTR_p, _pl, GMTR_t, _pl, GMTR_a, _pl
@@ -68,6 +70,7 @@ struct Ctx {
   void *buf(const char *name, size_t bytes);
   void release(const char *name);
   int check_launch(const char *what);
+  int copy_streams();
   int upload_geometry(const double *const h[8], const size_t n[8]);
   template <typename T> Geo<T> geo() const;
   int step_ctx(StepCtx &S);

@@ -318,7 +318,9 @@ int ica_advect_fast_dev(ica_ctx *ctx, int ntr, double dt,
                         const float *rhogvy, const float *rhogvy_pl,
                         const float *rhogvz, const float *rhogvz_pl,
                         const float *rhogw, const float *rhogw_pl);
-/* The same step on host arrays, in place on the state (copies in and out). */
+/* The same step on host arrays, in place on the state (copies in and out).  The state
+ * moves in chunks of tracers on two copy streams, overlapped with the step on the chunk
+ * before; from page-locked host memory the copies in and out run at the same time. */
 int ica_advect_fast(ica_ctx *ctx, int ntr, double dt,
                     double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
                     const float *rhogvx, const float *rhogvx_pl,
@@ -342,6 +344,9 @@ int ica_advect_fast64_dev(ica_ctx *ctx, int ntr, double dt,
  * autotuner in the Python layer times them and keeps the fastest). */
 int ica_fast_shapes(ica_ctx *ctx, int *n, int *tx, int *ty, int *tg);
 int ica_fast_set_shape(ica_ctx *ctx, int shape);
+/* Tracers per chunk of ica_advect_fast's copies; 0 (the default) sizes chunks at about
+ * 1 GiB of rhogq, 1 to 4 tracers.  The result does not depend on it. */
+int ica_fast_set_host_chunk(ica_ctx *ctx, int tracers);
 /* CUDA-event timing of the horizontal kernel: returns the total milliseconds and
  * the number of launches recorded since the last call, then enables (1) or
  * disables (0) recording for the following calls.  Synchronises the stream. */

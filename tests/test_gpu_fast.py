@@ -71,16 +71,26 @@ def test_fast_every_tile_shape(O):
         ctx.close()
 
 
-def test_fast_host_entry_equals_device_entry():
+@pytest.mark.parametrize("ntr,chunk,pinned", [(3, 0, False), (9, 0, False), (9, 0, True), (9, 2, True),
+                                               (5, 1, False)])
+def test_fast_host_entry_equals_device_entry(ntr, chunk, pinned):
+    """The host-pointer step moves the state in chunks of tracers, overlapping the copies with
+    the step (9 tracers by size at this grid: chunks 4, 4, 1, both staging slots reused); its
+    result is the device step's, bit for bit, whatever the chunk, from pageable or pinned
+    host memory."""
     import torch
-    c = case(4, 0, 8, 3)
+    c = case(4, 0, 8, ntr)
     g, f = c["grid"], c["fields"]
     ctx = _ctx(g)
     try:
+        ctx.fast_set_host_chunk(chunk)
         r = ctx.fast_runner(g, _dev(c["state"]), _dev(f), c["dt"], autotune=False)
         r.step()
         torch.cuda.synchronize()
-        H = {k: v.copy() for k, v in c["state"].items()}
+        if pinned:
+            H = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in c["state"].items()}
+        else:
+            H = {k: v.copy() for k, v in c["state"].items()}
         f32 = {k: np.ascontiguousarray(f[k], np.float32) for k in ("rhogvx", "rhogvx_pl", "rhogvy", "rhogvy_pl",
                                                                   "rhogvz", "rhogvz_pl", "rhogw", "rhogw_pl")}
         ctx.advect_fast_host(c["dt"], H["rhog"], H["rhog_pl"], H["rhogq"], H["rhogq_pl"], **f32)
