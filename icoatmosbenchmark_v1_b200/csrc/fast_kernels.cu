@@ -176,34 +176,52 @@ __global__ void k_fast_boundary(const __grid_constant__ MultiInst M) {
   for (int x = 0; x < 3; ++x)
     for (int n = 0; n < 7; ++n) cgr[x][n] = I.cg[(((size_t)l * 3 + x) * 7 + n) * I.gall + c];
   const int di7[7] = {0, 1, 1, 0, -1, -1, 0}, dj7[7] = {0, 0, 1, 1, 0, -1, -1};
+  // The 4 points of each face's bounds (bounds64 for the face's owner), as offsets in the 3x3
+  // block: a region-boundary cell lies in [gmin, gmax]^2, so every point is in the block and
+  // no index clamp applies.  Face 5's owner is the singular corner (gmin-1, gmin-1) when the
+  // cell is (gmin, gmin) of a region with the singular point: then its points shift.
+  const bool sgp5 = sgp && i == I.gmin && j == I.gmin;
   for (int t = 0; t < I.ntr; ++t) {
     const double *Qt = I.Q_in + t * tstride + ((size_t)l * I.K + k) * I.gall;
     double q9[3][3];
+#pragma unroll
     for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
       for (int di = 0; di < 3; ++di) q9[dj][di] = Qt[(size_t)(j - 2 + dj) * G + (i - 2 + di)] * rinv[dj][di];
-    // q at (ii,jj): the 3x3 block around the cell, else directly
-    auto q = [&](int ii, int jj) -> double {
-      const int a = ii - i + 1, bb = jj - j + 1;
-      if (a >= 0 && a < 3 && bb >= 0 && bb < 3) return q9[bb][a];
-      return Qt[(size_t)(jj - 1) * G + (ii - 1)] / f(0, ii, jj);
-    };
+    auto Q = [&](int di, int dj) { return q9[dj + 1][di + 1]; };
     double out[5];
+#pragma unroll
     for (int x = 0; x < 3; ++x) {
       double s = cgr[x][0] * q9[1][1];
+#pragma unroll
       for (int n = 1; n <= 6; ++n) s = s + cgr[x][n] * q9[1 + dj7[n]][1 + di7[n]];
       out[x] = s;
     }
+    // (q0, b, c, d) of bounds64, in its order
+    double lo[7], hi[7];
+    auto b4 = [&](int m, double q0, double b, double c, double d) {
+      lo[m] = mn64(mn64(mn64(q0, b), c), d);
+      hi[m] = mx64(mx64(mx64(q0, b), c), d);
+    };
+    b4(1, Q(0, 0), Q(0, -1), Q(1, 0), Q(1, 1));     // AI of (i, j)
+    b4(2, Q(0, 0), Q(1, 0), Q(1, 1), Q(0, 1));      // AIJ of (i, j)
+    b4(3, Q(0, 0), Q(1, 1), Q(0, 1), Q(-1, 0));     // AJ of (i, j)
+    b4(4, Q(-1, 0), Q(-1, -1), Q(0, 0), Q(0, 1));   // AI of (i-1, j)
+    if (sgp5) b4(5, Q(-1, -1), Q(0, 0), Q(1, 0), Q(-1, 0));  // AIJ of the singular corner
+    else b4(5, Q(-1, -1), Q(0, -1), Q(0, 0), Q(-1, 0));      // AIJ of (i-1, j-1)
+    b4(6, Q(0, -1), Q(1, 0), Q(0, 0), Q(-1, -1));   // AJ of (i, j-1)
     double qmn[7], qmx[7];
+#pragma unroll
     for (int m = 1; m <= 6; ++m) {
-      double lo, hi;
-      bounds64(I, oi[m], oj[m], fa[m], sgp, q, lo, hi);
       const double cm = cmk[m];
-      if (m <= 3) qmn[m] = cm * lo + (1.0 - cm) * BIG, qmx[m] = cm * hi + (1.0 - cm) * (-BIG);
-      else qmn[m] = cm * BIG + (1.0 - cm) * lo, qmx[m] = cm * (-BIG) + (1.0 - cm) * hi;
+      if (m <= 3) qmn[m] = cm * lo[m] + (1.0 - cm) * BIG, qmx[m] = cm * hi[m] + (1.0 - cm) * (-BIG);
+      else qmn[m] = cm * BIG + (1.0 - cm) * lo[m], qmx[m] = cm * (-BIG) + (1.0 - cm) * hi[m];
     }
     const double q0 = q9[1][1];
     double qnmin = q0, qnmax = q0;
+#pragma unroll
     for (int m = 1; m <= 6; ++m) qnmin = mn64(qnmin, qmn[m]);
+#pragma unroll
     for (int m = 1; m <= 6; ++m) qnmax = mx64(qnmax, qmx[m]);
     const double CQmin = chm[1] * qmn[1] + chm[2] * qmn[2] + chm[3] * qmn[3] + chm[4] * qmn[4] + chm[5] * qmn[5] +
                          chm[6] * qmn[6];
@@ -212,6 +230,7 @@ __global__ void k_fast_boundary(const __grid_constant__ MultiInst M) {
     out[3] = (q0 - CQmax - qnmax * omc) * rden + q0 * zerosw;
     out[4] = (q0 - CQmin - qnmin * omc) * rden + q0 * zerosw;
     double *dst = dst0 + t * dstride;
+#pragma unroll
     for (int x = 0; x < 5; ++x) dst[x] = out[x];
   }
 }
