@@ -916,6 +916,8 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt, bool f64) {
   I = FastInst{};
   if (!geo_set || !stepgeo_set) return set_error("advect_fast: geometry not registered"), ICA_ERR_STATE;
   if (sz.kall < 4 || sz.kall > 128) return set_error("advect_fast: kall must be in [4, 128]"), ICA_ERR_ARG;
+  if ((long long)sz.lall * (sz.kall - 2) * sz.gall >= (1LL << 31))  // 32-bit cell-level indices in the kernels
+    return set_error("advect_fast: grid too large (lall * (kall - 2) * gall >= 2^31)"), ICA_ERR_ARG;
   int rc = build_fast_tables();
   if (rc) return rc;
   int tx[16], ty[16], tg[16];

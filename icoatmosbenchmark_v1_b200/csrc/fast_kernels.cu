@@ -342,9 +342,13 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
   const int ii = find_inst(M, w, [](const FastInst &I) { return (long long)I.lall * (I.K - 2) * I.gall; });
   if (ii < 0) return;
   const FastInst &I = M.inst[ii];
-  const int G = I.G, c = (int)(w % I.gall);
-  const int lk = (int)(w / I.gall), k = 1 + lk % (I.K - 2), l = lk / (I.K - 2);
-  const int i = c % G + 1, j = c / G + 1;
+  // 32-bit index arithmetic (a 64-bit division is several times the cost of this thread's
+  // work); the host keeps lall * (K - 2) * gall below 2^31
+  const unsigned wu = (unsigned)w, gall = (unsigned)I.gall, kin = (unsigned)(I.K - 2), Gu = (unsigned)I.G;
+  const int G = I.G, c = (int)(wu % gall);
+  const unsigned lk = wu / gall;
+  const int k = 1 + (int)(lk % kin), l = (int)(lk / kin);
+  const int i = (int)((unsigned)c % Gu) + 1, j = (int)((unsigned)c / Gu) + 1;
   const size_t n3 = (size_t)I.lall * I.K * I.gall, o = ((size_t)l * I.K + k) * I.gall + c;
   const R dtf = (R)I.dt;
   auto interior = [&](int a, int b) { return a >= I.gmin && a <= I.gmax && b >= I.gmin && b <= I.gmax; };
