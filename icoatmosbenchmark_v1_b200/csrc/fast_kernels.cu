@@ -513,94 +513,6 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   const double ra64 = c_int ? rarea(I, l, ci, cj) : 1.0;
   const R ra32 = (R)ra64;
 
-  // ---- (0a) 1/rho and the face fluxes (k_fast_faces) of this level in the window
-  for (int e = tid; e < NW; e += NT) {
-    const int lx = e % WW, ly = e / WW;  // local slot: x = lx - 3
-    const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-    const bool in = i >= 1 && i <= G && j >= 1 && j <= G;
-    const size_t o = base + (size_t)(j - 1) * G + (i - 1);
-    s.rinv[e] = in ? 1.0 / I.rho_in[o] : 1.0;
-    // owners x, y in [-2, T] are read by the Courant numbers of the ring cells
-    const bool own = in && lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) s.F[a][e] = own ? I.Fg[(size_t)a * tstride + o] : 0.0;
-  }
-  __syncthreads();
-  // ---- (0d) per ring cell: Courant numbers, masks, outflow sums, gradient coefficients;
-  // per owner: upwind offsets; per tile cell: flx_h (FP64), rho after the horizontal
-  // sub-step and the tracer-independent inputs of the vertical sub-step
-  R chm[7], omc = R(0.0), rden = R(0.0), zsw = R(1.0), cgr[21];
-  unsigned inmask = 0, cmown = 0;
-  R dup[3][3];
-  const int nbe[7] = {0, ec, ec, ec, ec - 1, ec - WW - 1, ec - WW};  // owner slot of face m
-#pragma unroll
-  for (int m = 0; m < 7; ++m) chm[m] = R(0.0);
-#pragma unroll
-  for (int n = 0; n < 21; ++n) cgr[n] = tile_cell ? (sizeof(R) == 8 ? (R)I.cg[((size_t)l * 21 + n) * I.gall + ccell]
-                                             : (R)I.cg32[((size_t)l * 21 + n) * I.gall + ccell])
-                            : R(0);
-  if (tile_cell) {
-    const R rcinv = (R)s.rinv[ec];  // Courant numbers by the reciprocal of rho (one division per cell)
-    R ch[7];
-#pragma unroll
-    for (int m = 1; m <= 6; ++m) {
-      const R Fm = (R)s.F[(m - 1) % 3][nbe[m]];
-      ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) * rcinv;
-      chm[m] = A::mn(ch[m], R(0.0));
-      R chown = ch[m];
-      if (m >= 4) {  // the owner's own Courant number of this face, as the owner forms it
-        const int oi = (m == 6) ? ci : ci - 1, oj = (m == 4) ? cj : cj - 1;
-        chown = (Fm * (R)rarea(I, l, oi, oj) * dtf) * (R)s.rinv[nbe[m]];
-      }
-      const R cm = R(0.5) - A::sgn(R(0.5), chown - EPSf);
-      const bool in = (m <= 3) ? (cm != R(0.0)) : (cm == R(0.0));
-      inmask |= in ? (1u << m) : 0u;
-    }
-    const R Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
-    const R Cout =
-        ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
-    zsw = R(0.5) - A::sgn(R(0.5), fabs(Cout) - EPSf);
-    omc = R(1.0) - Cin - Cout;
-    rden = (R(1.0) - zsw) / (Cout + zsw);
-  }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    dup[a][0] = dup[a][1] = dup[a][2] = R(0.0);
-    if (owner && c_int) {
-      const R Fa = (R)s.F[a][ec];
-      const R chown = (Fa * ra32 * dtf) * (R)s.rinv[ec];
-      const bool cm = (R(0.5) - A::sgn(R(0.5), chown - EPSf)) != R(0.0);
-      cmown |= cm ? (1u << a) : 0u;
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        dup[a][c] = (sizeof(R) == 8)
-                        ? (R)(I.off64[((size_t)l * 18 + a * 6 + (cm ? 3 : 0) + c) * I.gall + ccell] +
-                              I.Dg64[(size_t)(a * 3 + c) * tstride + base + ccell])
-                        : (R)(I.off32[((size_t)l * 18 + a * 6 + (cm ? 3 : 0) + c) * I.gall + ccell] +
-                              I.Dg[(size_t)(a * 3 + c) * tstride + base + ccell]);
-    }
-  }
-  double flx[7];
-#pragma unroll
-  for (int m = 0; m < 7; ++m) flx[m] = 0.0;
-  if (active) {
-    double sum = 0.0;
-#pragma unroll
-    for (int m = 1; m <= 6; ++m) {
-      flx[m] = cell_flx(I, l, ci, cj, m, sgp, s.F[(m - 1) % 3][nbe[m]], ra64);
-      sum = (m == 1) ? flx[m] : sum + flx[m];
-    }
-    const double rho_h = I.rho_in[base + ccell] - sum;
-    I.rho_out[base + ccell] = rho_h;
-    const double wk = fld(I, 3, base + ccell), wk1 = fld(I, 3, base + slab + ccell);
-    const double rhinv = 1.0 / rho_h;
-    if (sizeof(R) == 8)
-      I.vco64[base + ccell] = make_double4(-wk * dt * I.rdgz[k] * rhinv, wk1 * dt * I.rdgz[k] * rhinv, rhinv, wk);
-    else
-      I.vco[base + ccell] = make_float4((float)(-wk * dt * I.rdgz[k] * rhinv), (float)(wk1 * dt * I.rdgz[k] * rhinv),
-                                        (float)rhinv, (float)wk);
-  }
-
   // the window slots of this thread (e = tid + r*NT): global offset in the level
   constexpr int NSLOT = (NW + NT - 1) / NT;
   constexpr int TP = TB / 2;  // tracer pairs of a batch: one V2 holds tracers 2p and 2p+1
@@ -630,6 +542,108 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     }
     asm volatile("cp.async.commit_group;\n" ::);
   };
+  // the first two batches' windows stream in during the tracer-independent part
+  issue(0, 0);
+  if (TB < ntr) issue(TB, 1);
+  // that part's per-cell inputs from global memory, in flight together: gradient
+  // coefficients, remap offsets of both sides of the owner's faces, centroid displacements,
+  // rho and rhogw of the tile cell
+  R cgr[21], offr[18], dgr[9];
+  const bool own_int = owner && c_int;
+#pragma unroll
+  for (int n = 0; n < 21; ++n) cgr[n] = tile_cell ? (sizeof(R) == 8 ? (R)I.cg[((size_t)l * 21 + n) * I.gall + ccell]
+                                             : (R)I.cg32[((size_t)l * 21 + n) * I.gall + ccell])
+                            : R(0);
+#pragma unroll
+  for (int n = 0; n < 18; ++n)
+    offr[n] = !own_int ? R(0)
+              : (sizeof(R) == 8) ? (R)I.off64[((size_t)l * 18 + n) * I.gall + ccell]
+                                 : (R)I.off32[((size_t)l * 18 + n) * I.gall + ccell];
+#pragma unroll
+  for (int n = 0; n < 9; ++n)
+    dgr[n] = !own_int ? R(0)
+             : (sizeof(R) == 8) ? (R)I.Dg64[(size_t)n * tstride + base + ccell]
+                                : (R)I.Dg[(size_t)n * tstride + base + ccell];
+  double rho_c = 0.0, wk = 0.0, wk1 = 0.0;
+  if (active) rho_c = I.rho_in[base + ccell], wk = fld(I, 3, base + ccell), wk1 = fld(I, 3, base + slab + ccell);
+  // ---- (0a) 1/rho and the face fluxes (k_fast_faces) of this level in the window
+  for (int e = tid; e < NW; e += NT) {
+    const int lx = e % WW, ly = e / WW;  // local slot: x = lx - 3
+    const int i = i0 - 3 + lx, j = j0 - 3 + ly;
+    const bool in = i >= 1 && i <= G && j >= 1 && j <= G;
+    const size_t o = base + (size_t)(j - 1) * G + (i - 1);
+    s.rinv[e] = in ? 1.0 / I.rho_in[o] : 1.0;
+    // owners x, y in [-2, T] are read by the Courant numbers of the ring cells
+    const bool own = in && lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) s.F[a][e] = own ? I.Fg[(size_t)a * tstride + o] : 0.0;
+  }
+  __syncthreads();
+  // ---- (0d) per ring cell: Courant numbers, masks, outflow sums, gradient coefficients;
+  // per owner: upwind offsets; per tile cell: flx_h (FP64), rho after the horizontal
+  // sub-step and the tracer-independent inputs of the vertical sub-step
+  R chm[7], omc = R(0.0), rden = R(0.0), zsw = R(1.0);
+  unsigned inmask = 0, cmown = 0;
+  R dup[3][3];
+  const int nbe[7] = {0, ec, ec, ec, ec - 1, ec - WW - 1, ec - WW};  // owner slot of face m
+#pragma unroll
+  for (int m = 0; m < 7; ++m) chm[m] = R(0.0);
+  if (tile_cell) {
+    const R rcinv = (R)s.rinv[ec];  // Courant numbers by the reciprocal of rho (one division per cell)
+    R ch[7];
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) {
+      const R Fm = (R)s.F[(m - 1) % 3][nbe[m]];
+      ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) * rcinv;
+      chm[m] = A::mn(ch[m], R(0.0));
+      R chown = ch[m];
+      if (m >= 4) {  // the owner's own Courant number of this face, as the owner forms it
+        const int oi = (m == 6) ? ci : ci - 1, oj = (m == 4) ? cj : cj - 1;
+        chown = (Fm * (R)rarea(I, l, oi, oj) * dtf) * (R)s.rinv[nbe[m]];
+      }
+      const R cm = R(0.5) - A::sgn(R(0.5), chown - EPSf);
+      const bool in = (m <= 3) ? (cm != R(0.0)) : (cm == R(0.0));
+      inmask |= in ? (1u << m) : 0u;
+    }
+    const R Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
+    const R Cout =
+        ch[1] - chm[1] + ch[2] - chm[2] + ch[3] - chm[3] + ch[4] - chm[4] + ch[5] - chm[5] + ch[6] - chm[6];
+    zsw = R(0.5) - A::sgn(R(0.5), fabs(Cout) - EPSf);
+    omc = R(1.0) - Cin - Cout;
+    rden = (R(1.0) - zsw) / (Cout + zsw);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    dup[a][0] = dup[a][1] = dup[a][2] = R(0.0);
+    if (own_int) {
+      const R Fa = (R)s.F[a][ec];
+      const R chown = (Fa * ra32 * dtf) * (R)s.rinv[ec];
+      const bool cm = (R(0.5) - A::sgn(R(0.5), chown - EPSf)) != R(0.0);
+      cmown |= cm ? (1u << a) : 0u;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dup[a][c] = (cm ? offr[a * 6 + 3 + c] : offr[a * 6 + c]) + dgr[a * 3 + c];
+    }
+  }
+  double flx[7];
+#pragma unroll
+  for (int m = 0; m < 7; ++m) flx[m] = 0.0;
+  if (active) {
+    double sum = 0.0;
+#pragma unroll
+    for (int m = 1; m <= 6; ++m) {
+      flx[m] = cell_flx(I, l, ci, cj, m, sgp, s.F[(m - 1) % 3][nbe[m]], ra64);
+      sum = (m == 1) ? flx[m] : sum + flx[m];
+    }
+    const double rho_h = rho_c - sum;
+    I.rho_out[base + ccell] = rho_h;
+    const double rhinv = 1.0 / rho_h;
+    if (sizeof(R) == 8)
+      I.vco64[base + ccell] = make_double4(-wk * dt * I.rdgz[k] * rhinv, wk1 * dt * I.rdgz[k] * rhinv, rhinv, wk);
+    else
+      I.vco[base + ccell] = make_float4((float)(-wk * dt * I.rdgz[k] * rhinv), (float)(wk1 * dt * I.rdgz[k] * rhinv),
+                                        (float)rhinv, (float)wk);
+  }
+
   // q of the batch starting at tracer tb from stage[buf] (window x, y in [-2, T+1]), by pairs
   auto load_q = [&](int tb, int buf) {
     const int nb = min(TB, ntr - tb);
@@ -687,13 +701,13 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
   // Per batch b: (B) gradient + Qout, (C) face values, then (D) the update of batch b
   // together with (A) q of batch b+1, whose rhogq window streamed in during B and C.
   // Three barriers per batch.
-  issue(0, 0);
-  asm volatile("cp.async.wait_group 0;\n" ::);
+  // the first batch's window has landed (the second may still be in flight)
+  if (TB < ntr) asm volatile("cp.async.wait_group 1;\n" ::);
+  else asm volatile("cp.async.wait_group 0;\n" ::);
   __syncthreads();
   // ---- (A) q of the first batch
   load_q(0, 0);
   __syncthreads();
-  if (TB < ntr) issue(TB, 1);
   for (int t0 = 0, b = 0; t0 < ntr; t0 += TB, ++b) {
     const int ntg = min(TB, ntr - t0);
     // ---- (B) gradient and Qout of the ring cells
