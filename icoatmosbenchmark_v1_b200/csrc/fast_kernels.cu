@@ -369,35 +369,50 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
 #pragma unroll
     for (int x = 0; x < 4; ++x) v[x] = f0[x] * w1 + f1[x] * w2 + f2[x] * w3;
   };
+  // faces between interior cells take the FP32 triangle form, seam faces the FP64 value of
+  // k_fast_seam; AI = TJ(i,j-1) + TI(i,j), AIJ = TI(i,j) + TJ(i,j), AJ = TJ(i,j) + TI(i-1,j),
+  // so the four triangles are formed once each, before any store
+  bool ex[3], inner[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    double F = 0.0;
-    R d[3] = {R(0.0), R(0.0), R(0.0)};
-    if (i < G && j < G && face_exists(I, i, j, a + 1)) {
-      const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
-      if (!interior(i, j) || !interior(ni, nj)) {  // seam face: FP64 flux of k_fast_seam
-        const int sid = I.seam_id[((size_t)l * I.gall + c) * 3 + a];
-        F = I.sflux[(size_t)k * I.ns + sid];
-      } else {  // AI = TJ(i,j-1) + TI(i,j); AIJ = TI(i,j) + TJ(i,j); AJ = TJ(i,j) + TI(i-1,j)
-        R p[4], q[4];
-        if (a == 0) tri(i, j - 1, 1, p), tri(i, j, 0, q);
-        else if (a == 1) tri(i, j, 0, p), tri(i, j, 1, q);
-        else tri(i, j, 1, p), tri(i - 1, j, 0, q);
-        const R vx = p[1] + q[1], vy = p[2] + q[2], vz = p[3] + q[3];
-        const R rr = R(1.0) / A::mx(p[0] + q[0], A::RR_EPS);
-        const R Ff = R(0.5) * (vx * (R)ga(I, l, i, j, a + 1, HNX) + vy * (R)ga(I, l, i, j, a + 1, HNY) +
-                                 vz * (R)ga(I, l, i, j, a + 1, HNZ));
-        F = (double)Ff;
-        d[0] = -(vx * rr * dtf * R(0.5));
-        d[1] = -(vy * rr * dtf * R(0.5));
-        d[2] = -(vz * rr * dtf * R(0.5));
-      }
+    const int ni = (a < 2) ? i + 1 : i, nj = (a > 0) ? j + 1 : j;
+    ex[a] = i < G && j < G && face_exists(I, i, j, a + 1);
+    inner[a] = ex[a] && interior(i, j) && interior(ni, nj);
+  }
+  R tIij[4] = {}, tJij[4] = {}, tJm[4] = {}, tIm[4] = {};
+  if (inner[0] || inner[1]) tri(i, j, 0, tIij);
+  if (inner[1] || inner[2]) tri(i, j, 1, tJij);
+  if (inner[0]) tri(i, j - 1, 1, tJm);
+  if (inner[2]) tri(i - 1, j, 0, tIm);
+  double F[3];
+  R d[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    F[a] = 0.0;
+    d[a][0] = d[a][1] = d[a][2] = R(0.0);
+    if (inner[a]) {
+      const R *p = (a == 0) ? tJm : (a == 1 ? tIij : tJij);
+      const R *q = (a == 0) ? tIij : (a == 1 ? tJij : tIm);
+      const R vx = p[1] + q[1], vy = p[2] + q[2], vz = p[3] + q[3];
+      const R rr = R(1.0) / A::mx(p[0] + q[0], A::RR_EPS);
+      const R Ff = R(0.5) * (vx * (R)ga(I, l, i, j, a + 1, HNX) + vy * (R)ga(I, l, i, j, a + 1, HNY) +
+                               vz * (R)ga(I, l, i, j, a + 1, HNZ));
+      F[a] = (double)Ff;
+      d[a][0] = -(vx * rr * dtf * R(0.5));
+      d[a][1] = -(vy * rr * dtf * R(0.5));
+      d[a][2] = -(vz * rr * dtf * R(0.5));
+    } else if (ex[a]) {  // seam face
+      const int sid = I.seam_id[((size_t)l * I.gall + c) * 3 + a];
+      F[a] = I.sflux[(size_t)k * I.ns + sid];
     }
-    I.Fg[(size_t)a * n3 + o] = F;
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    I.Fg[(size_t)a * n3 + o] = F[a];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-      if (sizeof(R) == 8) I.Dg64[(size_t)(a * 3 + x) * n3 + o] = d[x];
-      else I.Dg[(size_t)(a * 3 + x) * n3 + o] = (float)d[x];
+      if (sizeof(R) == 8) I.Dg64[(size_t)(a * 3 + x) * n3 + o] = d[a][x];
+      else I.Dg[(size_t)(a * 3 + x) * n3 + o] = (float)d[a][x];
     }
   }
 }
