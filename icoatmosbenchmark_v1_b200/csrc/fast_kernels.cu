@@ -181,13 +181,27 @@ __global__ void k_fast_boundary(const __grid_constant__ MultiInst M) {
   // no index clamp applies.  Face 5's owner is the singular corner (gmin-1, gmin-1) when the
   // cell is (gmin, gmin) of a region with the singular point: then its points shift.
   const bool sgp5 = sgp && i == I.gmin && j == I.gmin;
+  // rhogq of the 3x3 block, one tracer ahead: the next tracer's loads are issued before this
+  // tracer's stores (which the compiler may not move them across)
+  const double *Q0 = I.Q_in + ((size_t)l * I.K + k) * I.gall + (size_t)(j - 2) * G + (i - 2);
+  double raw[3][3];
+#pragma unroll
+  for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+    for (int di = 0; di < 3; ++di) raw[dj][di] = Q0[(size_t)dj * G + di];
   for (int t = 0; t < I.ntr; ++t) {
-    const double *Qt = I.Q_in + t * tstride + ((size_t)l * I.K + k) * I.gall;
     double q9[3][3];
 #pragma unroll
     for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
-      for (int di = 0; di < 3; ++di) q9[dj][di] = Qt[(size_t)(j - 2 + dj) * G + (i - 2 + di)] * rinv[dj][di];
+      for (int di = 0; di < 3; ++di) q9[dj][di] = raw[dj][di] * rinv[dj][di];
+    if (t + 1 < I.ntr) {
+      const double *Qn = Q0 + (size_t)(t + 1) * tstride;
+#pragma unroll
+      for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+        for (int di = 0; di < 3; ++di) raw[dj][di] = Qn[(size_t)dj * G + di];
+    }
     auto Q = [&](int di, int dj) { return q9[dj + 1][di + 1]; };
     double out[5];
 #pragma unroll
@@ -284,17 +298,30 @@ __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
   for (int n = 0; n < 4; ++n) rv[n] = 1.0 / I.rho_in[slab + pc[n] - 1];
   const double rn = 1.0 / I.rho_in[slab + on];
   const double BIG = DBL_MAX;
-  for (int t = 0; t < I.ntr; ++t) {
+  // the tracer's inputs one tracer ahead: the next tracer's loads are issued before this
+  // tracer's store (which the compiler may not move them across)
+  double rq[5], rgo[5], rgn[5];
+  auto fetch = [&](int t) {
     const double *Qt = I.Q_in + t * tstride + slab;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) rq[n] = Qt[pc[n] - 1];
+    rq[4] = Qt[on];
+#pragma unroll
+    for (int x = 0; x < 5; ++x) rgo[x] = bo >= 0 ? bval(I, t, k, bo)[x] : 0.0, rgn[x] = bn >= 0 ? bval(I, t, k, bn)[x] : 0.0;
+  };
+  fetch(0);
+  for (int t = 0; t < I.ntr; ++t) {
     double qv[4];
-    for (int n = 0; n < 4; ++n) qv[n] = Qt[pc[n] - 1] * rv[n];
-    const double qo = qv[0], qn = Qt[on] * rn;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) qv[n] = rq[n] * rv[n];
+    const double qo = qv[0], qn = rq[4] * rn;
     // gradient and Qout of both cells (boundary or halo cells of this region)
     double go[5] = {0, 0, 0, 0, 0}, gn[5] = {0, 0, 0, 0, 0};
-    if (bo >= 0) for (int x = 0; x < 5; ++x) go[x] = bval(I, t, k, bo)[x];
+    if (bo >= 0) for (int x = 0; x < 5; ++x) go[x] = rgo[x];
     else go[3] = go[4] = qo;  // halo point no list reaches: Qout = q, grad = 0 (as after the reference fill)
-    if (bn >= 0) for (int x = 0; x < 5; ++x) gn[x] = bval(I, t, k, bn)[x];
+    if (bn >= 0) for (int x = 0; x < 5; ++x) gn[x] = rgn[x];
     else gn[3] = gn[4] = qn;
+    if (t + 1 < I.ntr) fetch(t + 1);
     double vu = qn, vs = qo;
     for (int x = 0; x < 3; ++x) vu = vu + gn[x] * dxn[x];
     for (int x = 0; x < 3; ++x) vs = vs + go[x] * dxo[x];
