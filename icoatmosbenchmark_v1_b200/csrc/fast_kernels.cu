@@ -1088,20 +1088,27 @@ __global__ void __launch_bounds__(256, 2) k_fast_vert(const __grid_constant__ Mu
   }
 }
 
-// ---- the two pole centres, all levels, one thread per (pole, tracer), FP64 -----------
+// ---- the two pole centres, FP64: one CTA per (pole, tracer), one thread per level ----------
+// The horizontal sub-step of every level, then the vertical one of the column: its Qout of a
+// level needs only q and the Courant numbers, so every stage is level-parallel, with the
+// arithmetic of each value as in the column form of the plain path.
 template <int KMAX>
-__global__ void k_fast_pole(const __grid_constant__ MultiInst M) {
-  long long tl = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(KMAX) k_fast_pole(const __grid_constant__ MultiInst M) {
+  long long tl = blockIdx.x;
   const int ii = find_inst(M, tl, [](const FastInst &J) { return (long long)kLallPl * J.ntr; });
-  if (ii < 0) return;
+  if (ii < 0) return;  // whole CTA
   const FastInst &I = M.inst[ii];
   const int t = (int)tl;
   const int p = t % kLallPl, tr = t / kLallPl;
-  const int K = I.K;
+  const int K = I.K, k = threadIdx.x;
+  const int kmin = 1, kmax = K - 2;
   const size_t toff = (size_t)tr * kLallPl * K * kGallPl;
   const double rarea = I.GMTR_p_pl[((size_t)(P_RAREA - 1) * kLallPl + p) * kGallPl];
-  double Qh[KMAX], rh[KMAX];
-  for (int k = 1; k <= K - 2; ++k) {
+  const double BIG = DBL_MAX, EPS = DBL_EPSILON;
+  __shared__ double sQh[KMAX], srh[KMAX], sq[KMAX], sqh[KMAX], sck1[KMAX], sck2[KMAX], sQmn[KMAX], sQmx[KMAX],
+      sinfl[KMAX];
+  // ---- horizontal sub-step of level k
+  if (k >= kmin && k <= kmax) {
     const size_t off = ((size_t)p * K + k) * kGallPl;
     double flux[7], xc[7][3];
     pole_faces(I, p, k, flux, xc);
@@ -1116,7 +1123,6 @@ __global__ void k_fast_pole(const __grid_constant__ MultiInst M) {
       Qmn[v] = br[3], Qmx[v] = br[4];
     }
     double sum = 0.0, rsum = 0.0;
-    const double BIG = DBL_MAX, EPS = DBL_EPSILON;
     for (int v = 2; v <= 6; ++v) {
       const double flx = flux[v] * rarea * I.dt;
       const double ch = flx / I.rho_in_pl[off];
@@ -1135,58 +1141,66 @@ __global__ void k_fast_pole(const __grid_constant__ MultiInst M) {
       if (v == 2) sum = flx * a, rsum = flx;
       else sum = sum + flx * a, rsum = rsum + flx;
     }
-    Qh[k] = I.Q_in_pl[toff + off] - sum;
-    rh[k] = I.rho_in_pl[off] - rsum;
+    sQh[k] = I.Q_in_pl[toff + off] - sum;
+    srh[k] = I.rho_in_pl[off] - rsum;
   }
-  // vertical sub-step of the pole column (FP64, region form, as the plain path)
-  const int kmin = 1, kmax = K - 2;
-  double ck1[KMAX], ck2[KMAX], q[KMAX], qh[KMAX];
-  auto W = [&](int k) { return fld_pl(I, 3, ((size_t)p * K + k) * kGallPl); };
-  for (int k = 0; k < K; ++k) ck1[k] = ck2[k] = 0.0;
-  for (int k = kmin; k <= kmax; ++k) {
-    ck1[k] = -W(k) * I.dt * I.rdgz[k] / rh[k];
-    ck2[k] = W(k + 1) * I.dt * I.rdgz[k] / rh[k];
+  __syncthreads();
+  // ---- vertical sub-step of the pole column (FP64, region form, as the plain path)
+  auto W = [&](int kk) { return fld_pl(I, 3, ((size_t)p * K + kk) * kGallPl); };
+  if (k < K) {
+    double c1 = 0.0, c2 = 0.0;
+    if (k >= kmin && k <= kmax) {
+      c1 = -W(k) * I.dt * I.rdgz[k] / srh[k];
+      c2 = W(k + 1) * I.dt * I.rdgz[k] / srh[k];
+      sq[k] = sQh[k] / srh[k];
+    }
+    if (k == K - 1) c1 = -W(K - 1) * I.dt * I.rdgz[K - 1] / I.rho_in_pl[((size_t)p * K + K - 1) * kGallPl];
+    sck1[k] = c1, sck2[k] = c2;
   }
-  ck1[K - 1] = -W(K - 1) * I.dt * I.rdgz[K - 1] / I.rho_in_pl[((size_t)p * K + K - 1) * kGallPl];
-  for (int k = kmin; k <= kmax; ++k) q[k] = Qh[k] / rh[k];
-  q[0] = q[kmin];
-  q[K - 1] = q[kmax];
-  for (int k = kmin; k <= kmax + 1 && k < K; ++k) qh[k] = I.afact[k] * q[k] + I.bfact[k] * q[k - 1];
-  const double BIG = DBL_MAX, EPS = DBL_EPSILON;
-  auto vq = [&](int k, double &infl, double &Qmin, double &Qmax) {
-    infl = 0.5 - fsg(0.5, ck1[k]);
-    const double infu = 0.5 + fsg(0.5, ck1[k + 1]);
-    const double qk = q[k], qm = q[k - 1], qp = q[k + 1];
+  __syncthreads();
+  if (k == 0) sq[0] = sq[kmin];
+  if (k == K - 1) sq[K - 1] = sq[kmax];
+  __syncthreads();
+  if (k >= kmin && k <= kmax + 1 && k < K) sqh[k] = I.afact[k] * sq[k] + I.bfact[k] * sq[k - 1];
+  if (k >= kmin && k <= kmax) {  // Qout of level k
+    const double infl = 0.5 - fsg(0.5, sck1[k]);
+    const double infu = 0.5 + fsg(0.5, sck1[k + 1]);
+    const double qk = sq[k], qm = sq[k - 1], qp = sq[k + 1];
     const double minL = mn64(qk, qm) + (1.0 - infl) * BIG, minU = mn64(qk, qp) + (1.0 - infu) * BIG;
     const double maxL = mx64(qk, qm) - (1.0 - infl) * BIG, maxU = mx64(qk, qp) - (1.0 - infu) * BIG;
     const double qnmin = mn64(mn64(minL, minU), qk), qnmax = mx64(mx64(maxL, maxU), qk);
-    const double Cin = infl * ck1[k] + infu * ck2[k], Cout = (1.0 - infl) * ck1[k] + (1.0 - infu) * ck2[k];
-    const double CQmax = infl * ck1[k] * maxL + infu * ck2[k] * maxU;
-    const double CQmin = infl * ck1[k] * minL + infu * ck2[k] * minU;
+    const double Cin = infl * sck1[k] + infu * sck2[k], Cout = (1.0 - infl) * sck1[k] + (1.0 - infu) * sck2[k];
+    const double CQmax = infl * sck1[k] * maxL + infu * sck2[k] * maxU;
+    const double CQmin = infl * sck1[k] * minL + infu * sck2[k] * minU;
     const double zerosw = 0.5 - fsg(0.5, fabs(Cout) - EPS);
-    Qmin = ((qk - qnmax) + qnmax * (Cin + Cout) - CQmax) / (Cout + zerosw) * (1.0 - zerosw) + qk * zerosw;
-    Qmax = ((qk - qnmin) + qnmin * (Cin + Cout) - CQmin) / (Cout + zerosw) * (1.0 - zerosw) + qk * zerosw;
-  };
-  double fl0, Qmin_km1, Qmax_km1;
-  vq(kmin, fl0, Qmin_km1, Qmax_km1);
-  for (int k = kmin + 1; k <= kmax; ++k) {
-    double infl, Qmin, Qmax;
-    vq(k, infl, Qmin, Qmax);
-    const double h = qh[k];
-    qh[k] = infl * mx64(mn64(h, Qmax_km1), Qmin_km1) + (1.0 - infl) * mx64(mn64(h, Qmax), Qmin);
-    Qmin_km1 = Qmin, Qmax_km1 = Qmax;
+    sQmn[k] = ((qk - qnmax) + qnmax * (Cin + Cout) - CQmax) / (Cout + zerosw) * (1.0 - zerosw) + qk * zerosw;
+    sQmx[k] = ((qk - qnmin) + qnmin * (Cin + Cout) - CQmin) / (Cout + zerosw) * (1.0 - zerosw) + qk * zerosw;
+    sinfl[k] = infl;
   }
-  for (int k = kmin; k <= kmax; ++k) {
-    const double Qn = Qh[k] - (W(k + 1) * qh[k + 1] - W(k) * qh[k]) * I.dt * I.rdgz[k];
-    I.Q_out_pl[toff + ((size_t)p * K + k) * kGallPl] = Qn;
+  __syncthreads();
+  // limited face values of faces kmin+1 .. kmax (bounds of the levels on both sides)
+  double hk = 0.0;
+  const bool lim = k >= kmin + 1 && k <= kmax;
+  if (lim) {
+    const double h = sqh[k], infl = sinfl[k];
+    hk = infl * mx64(mn64(h, sQmx[k - 1]), sQmn[k - 1]) + (1.0 - infl) * mx64(mn64(h, sQmx[k]), sQmn[k]);
   }
-  I.Q_out_pl[toff + ((size_t)p * K + 0) * kGallPl] = I.Q_out_pl[toff + ((size_t)p * K + kmin) * kGallPl];
-  I.Q_out_pl[toff + ((size_t)p * K + K - 1) * kGallPl] = I.Q_out_pl[toff + ((size_t)p * K + kmax) * kGallPl];
-  if (tr == 0) {
-    for (int k = kmin; k <= kmax; ++k)
-      I.rho_out_pl[((size_t)p * K + k) * kGallPl] = rh[k] - (W(k + 1) - W(k)) * I.dt * I.rdgz[k];
-    I.rho_out_pl[((size_t)p * K) * kGallPl] = I.rho_out_pl[((size_t)p * K + kmin) * kGallPl];
-    I.rho_out_pl[((size_t)p * K + K - 1) * kGallPl] = I.rho_out_pl[((size_t)p * K + kmax) * kGallPl];
+  __syncthreads();
+  if (lim) sqh[k] = hk;
+  __syncthreads();
+  if (k >= kmin && k <= kmax) {
+    const double Qn = sQh[k] - (W(k + 1) * sqh[k + 1] - W(k) * sqh[k]) * I.dt * I.rdgz[k];
+    double *Qo = I.Q_out_pl + toff + (size_t)p * K * kGallPl;
+    Qo[(size_t)k * kGallPl] = Qn;
+    if (k == kmin) Qo[0] = Qn;
+    if (k == kmax) Qo[(size_t)(K - 1) * kGallPl] = Qn;
+    if (tr == 0) {
+      const double rn = srh[k] - (W(k + 1) - W(k)) * I.dt * I.rdgz[k];
+      double *Ro = I.rho_out_pl + (size_t)p * K * kGallPl;
+      Ro[(size_t)k * kGallPl] = rn;
+      if (k == kmin) Ro[0] = rn;
+      if (k == kmax) Ro[(size_t)(K - 1) * kGallPl] = rn;
+    }
   }
 }
 
@@ -1288,8 +1302,8 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
   }
   k_fast_boundary<<<(unsigned)((nbk + 127) / 128), 128, 0, st>>>(M);
   k_fast_seam<<<(unsigned)((nsk + 127) / 128), 128, 0, st>>>(M);
-  if (kmax <= 48) k_fast_pole<48><<<(unsigned)((npl + 63) / 64), 64, 0, st>>>(M);
-  else if (kmax <= 128) k_fast_pole<128><<<(unsigned)((npl + 63) / 64), 64, 0, st>>>(M);
+  if (kmax <= 64) k_fast_pole<64><<<(unsigned)npl, 64, 0, st>>>(M);
+  else if (kmax <= 128) k_fast_pole<128><<<(unsigned)npl, 128, 0, st>>>(M);
   else return cudaErrorInvalidValue;
   if (ev0) cudaEventRecord(ev0, st);
   const bool f64 = M.inst[0].f64 != 0;
