@@ -402,10 +402,12 @@ def run_uneven(args, world, rank, local):
     sampler = ClockSampler(local)
     sampler.start()
     torch.cuda.synchronize()
+    n0 = sum(c.launch_count for c in ctxs)
     e0.record(stream)
     for _ in range(args.steps):
         br.step()
     e1.record(stream)
+    launches = sum(c.launch_count for c in ctxs) - n0
     torch.cuda.synchronize()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.steps
@@ -448,7 +450,7 @@ def run_uneven(args, world, rank, local):
                 "fp64_variant": {"ms_per_step": ms_f64, "value": upd / (ms_f64 * 1e-3),
                                  "max_rel_err_vs_fp64_plain": err64,
                                  "mass_drift": {"value": drift64, "steps": 1 + args.steps + args.warmup}},
-                "gpu_launches": None, "clocks": clocks}
+                "gpu_launches": launches, "clocks": clocks}
         print(json.dumps(line), flush=True)
     for c in ctxs:
         c.close()

@@ -1200,6 +1200,7 @@ struct ica_batch {
   int shape = 0;
   cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  long long graph_launches[2] = {0, 0};  // kernel launches a replay of the slot's graph makes
 };
 
 namespace icoadv {
@@ -1311,7 +1312,11 @@ static int batch_capture_impl(ica_batch *b, const Args *args, int slot) {
   if (e != cudaSuccess) return cuda_fail(e, "ica_batch_capture");
   e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+  long long n0 = 0;
+  for (Ctx *c : b->ctx) n0 += c->launches;
   rc = batch_enqueue(b, M, args);
+  long long n1 = 0;
+  for (Ctx *c : b->ctx) n1 += c->launches;
   cudaGraph_t g = nullptr;
   e = cudaStreamEndCapture(st, &g);
   if (rc) {
@@ -1323,6 +1328,7 @@ static int batch_capture_impl(ica_batch *b, const Args *args, int slot) {
   if (b->graph[slot]) cudaGraphDestroy(b->graph[slot]);
   b->graph[slot] = g;
   b->exec[slot] = nullptr;
+  b->graph_launches[slot] = n1 - n0;
   e = cudaGraphInstantiate(&b->exec[slot], g, 0);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
   return ICA_OK;
@@ -1344,6 +1350,7 @@ int ica_batch_replay(ica_batch *b, int slot) {
   cudaSetDevice(b->ctx[0]->device);
   cudaError_t e = cudaGraphLaunch(b->exec[slot], b->ctx[0]->stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+  b->ctx[0]->launches += b->graph_launches[slot];
   return ICA_OK;
 }
 

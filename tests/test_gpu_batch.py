@@ -47,10 +47,15 @@ def test_batch_equals_each_instance_alone_and_graph_replay(pair):
         br = api.BatchRunner(ctxs, [_dev(c["state"]) for c in cs], [_dev(c["fields"]) for c in cs],
                              [c["dt"] for c in cs], shape=0)
         br.step()  # uncaptured: sets up every buffer
-        br.use_graph()
+        n0 = sum(c.launch_count for c in ctxs)
         br.step()
+        per_step = sum(c.launch_count for c in ctxs) - n0
+        br.use_graph()
+        n0 = sum(c.launch_count for c in ctxs)
         br.step()
         torch.cuda.synchronize()
+        # a replay counts the kernels its graph launches, as an uncaptured step does
+        assert per_step > 0 and sum(c.launch_count for c in ctxs) - n0 == per_step
         for got, ref in zip(br.states, singles):
             for k in ref:
                 np.testing.assert_array_equal(got[k].cpu().numpy(), ref[k], err_msg=k)
