@@ -125,10 +125,23 @@ def write_snapshot(kernel, path, arrays, dims=SnapshotDims()):
     Path(path).write_bytes(b"".join(parts))
 
 
+def _es(v, w=24, d=16):
+    """Fortran ES<w>.<d> of a real: one digit before the point, d after, exponent of two digits
+    with its E (three digits without it past 99), right-justified in w characters."""
+    v = float(v)
+    if not math.isfinite(v):
+        return f"{'Infinity' if v > 0 else '-Infinity' if v < 0 else 'NaN':>{w}s}"
+    m, e = f"{v:.{d}E}".split("E")
+    ex = int(e)
+    t = f"{m}E{ex:+03d}" if abs(ex) <= 99 else f"{m}{ex:+04d}"
+    return f"{t:>{w}s}"
+
+
 def value_check(name, a):
-    """DEBUG_valuecheck's line: max, min and sum of an array."""
+    """DEBUG_valuecheck's line (mod_misc.f90, format (1x,A,A16,3(A,ES24.16))): max, min and sum
+    of an array, the name padded to 16 characters."""
     a = np.asarray(a)
-    return f" +check[{name:<16s}] max= {a.max(): .16E},min= {a.min(): .16E},sum= {a.sum(): .16E}"
+    return f" +check[{name[:16]:<16s}] max={_es(a.max())},min={_es(a.min())},sum={_es(a.sum())}"
 
 
 def _embed(a, lall):

@@ -110,9 +110,18 @@ def test_snapshot_round_trip_big_endian(tmp_path):
 
 
 def test_value_check_format():
+    """The driver's (1x,A,A16,3(A,ES24.16)) line: 16-character name, each value right-justified
+    in 24 characters with 16 digits after the point and a two-digit exponent (three, without
+    the E, past 99)."""
     line = S.value_check("check_q_h", np.array([1.0, -2.0, 0.5]))
-    assert line.startswith(" +check[check_q_h       ] max=  1.0000000000000000E+00,min= -2.0000000000000000E+00")
-    assert line.endswith("sum= -5.0000000000000000E-01")
+    assert line == (" +check[check_q_h       ] max=  1.0000000000000000E+00,min= -2.0000000000000000E+00,"
+                    "sum= -5.0000000000000000E-01")
+    assert S.value_check("d", np.array([-0.0])).split("] ", 1)[1] == \
+        "max= -0.0000000000000000E+00,min= -0.0000000000000000E+00,"\
+        "sum=  0.0000000000000000E+00"  # a sum starts from +0, as the Fortran SUM does
+    assert S._es(3.3842023700197510e-02) == "  3.3842023700197510E-02"
+    assert S._es(-1.5e-120) == " -1.5000000000000000-120"
+    assert len(S.value_check("a_name_longer_than_16", np.ones(2))) == len(S.value_check("x", np.ones(2)))
 
 
 def test_synthetic_snapshots_read_back(tmp_path, O):
