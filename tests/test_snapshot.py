@@ -120,7 +120,8 @@ def test_value_check_format():
         "max= -0.0000000000000000E+00,min= -0.0000000000000000E+00,"\
         "sum=  0.0000000000000000E+00"  # a sum starts from +0, as the Fortran SUM does
     assert S._es(3.3842023700197510e-02) == "  3.3842023700197510E-02"
-    assert S._es(-1.5e-120) == " -1.5000000000000000-120"
+    big = S._es(-2.0 ** -400)  # -3.87e-121: three exponent digits, no E
+    assert len(big) == 24 and "E" not in big and big.endswith("-121") and big.startswith(" -3.8725919148493")
     assert len(S.value_check("a_name_longer_than_16", np.ones(2))) == len(S.value_check("x", np.ones(2)))
 
 
