@@ -162,17 +162,23 @@ def _region1(a):
     return np.asarray(a)[..., :1, :, :]
 
 
-def run_snapshot(kernel, path, dims=SnapshotDims(), dt=360.0, device=0):
+def run_snapshot(kernel, path, dims=SnapshotDims(), dt=360.0, device=0, precision="f64"):
     """Runs the snapshot's inputs through the library and returns (outputs, diffs): the
     computed outputs of the snapshot's region and the poles, and expected - computed per
-    output (the driver's point-by-point diff)."""
+    output (the driver's point-by-point diff).  precision "f32" runs the FP32 entry points,
+    as the drivers built with RP = SP do (they read the same FP64 snapshot and convert)."""
     from icoatmosbenchmark_v1_b200 import api
     if dims.lall != 1:
         raise ValueError("the drivers' snapshots hold one region per process (ADM_lall = 1)")
+    if precision not in ("f64", "f32"):
+        raise ValueError(f"precision {precision!r}: f64 or f32")
+    rp = np.float64 if precision == "f64" else np.float32
     s = read_snapshot(kernel, path, dims)
     ctx = api.IcoAdv(dims.glevel, 0, dims.kall - 2, device)
     lall = ctx.sizes.lall
     full = {k: (_embed(v, lall) if not k.endswith("_pl") else np.ascontiguousarray(v)) for k, v in s.items()}
+    # kernel arguments in the working precision (the metrics stay FP64: the context keeps both)
+    a = {k: np.ascontiguousarray(v, dtype=rp) for k, v in full.items() if not k.startswith(("GRD_xr", "GMTR_"))}
     try:
         if kernel == "dyn_horiz_adv_flux":
             geo = []
@@ -182,26 +188,24 @@ def run_snapshot(kernel, path, dims=SnapshotDims(), dt=360.0, device=0):
             ctx.set_geometry(*geo)
             # the driver's output arrays start as the snapshot's: points the kernel does not
             # write (the pole centre of flx_h_pl and GRD_xc_pl) keep those values
-            flx, flx_pl = full["flx_h"].copy(), full["flx_h_pl"].copy()
-            xc, xc_pl = full["GRD_xc"].copy(), full["GRD_xc_pl"].copy()
-            ctx.horizontal_flux(flx, flx_pl, xc, xc_pl, full["rho"], full["rho_pl"], full["rhovx"], full["rhovx_pl"],
-                                full["rhovy"], full["rhovy_pl"], full["rhovz"], full["rhovz_pl"], float(dt))
+            flx, flx_pl = a["flx_h"].copy(), a["flx_h_pl"].copy()
+            xc, xc_pl = a["GRD_xc"].copy(), a["GRD_xc_pl"].copy()
+            ctx.horizontal_flux(flx, flx_pl, xc, xc_pl, a["rho"], a["rho_pl"], a["rhovx"], a["rhovx_pl"],
+                                a["rhovy"], a["rhovy_pl"], a["rhovz"], a["rhovz_pl"], float(dt))
             got = OrderedDict(flx_h=flx, flx_h_pl=flx_pl, GRD_xc=xc, GRD_xc_pl=xc_pl)
         elif kernel == "dyn_horiz_adv_limiter":
-            qa, qa_pl = full["q_a_prev"].copy(), full["q_a_prev_pl"].copy()
-            qo, qo_pl = np.zeros_like(full["Qout_prev"]), np.zeros_like(full["Qout_prev_pl"])
-            ctx.horizontal_limiter_thuburn(qa, qa_pl, full["q"], full["q_pl"], full["d"], full["d_pl"], full["ch"],
-                                           full["ch_pl"], full["cmask"], full["cmask_pl"], qo, qo_pl,
-                                           full["Qout_post"], full["Qout_post_pl"])
+            qa, qa_pl = a["q_a_prev"].copy(), a["q_a_prev_pl"].copy()
+            qo, qo_pl = np.zeros_like(a["Qout_prev"]), np.zeros_like(a["Qout_prev_pl"])
+            ctx.horizontal_limiter_thuburn(qa, qa_pl, a["q"], a["q_pl"], a["d"], a["d_pl"], a["ch"], a["ch_pl"],
+                                           a["cmask"], a["cmask_pl"], qo, qo_pl, a["Qout_post"], a["Qout_post_pl"])
             got = OrderedDict(q_a=qa, q_a_pl=qa_pl, Qout_prev=qo, Qout_prev_pl=qo_pl)
         else:
-            qh, qh_pl = full["q_h_prev"].copy(), full["q_h_prev_pl"].copy()
-            ctx.vertical_limiter_thuburn(qh, qh_pl, full["q"], full["q_pl"], full["d"], full["d_pl"], full["ck"],
-                                         full["ck_pl"])
+            qh, qh_pl = a["q_h_prev"].copy(), a["q_h_prev_pl"].copy()
+            ctx.vertical_limiter_thuburn(qh, qh_pl, a["q"], a["q_pl"], a["d"], a["d_pl"], a["ck"], a["ck_pl"])
             got = OrderedDict(q_h=qh, q_h_pl=qh_pl)
     finally:
         ctx.close()
-    got = OrderedDict((k, v if k.endswith("_pl") else _region1(v)) for k, v in got.items())
+    got = OrderedDict((k, (v if k.endswith("_pl") else _region1(v)).astype(np.float64)) for k, v in got.items())
     diffs = OrderedDict((k, s[k] - v) for k, v in got.items())
     return got, diffs
 
@@ -215,6 +219,8 @@ def main(argv=None):
     ap.add_argument("--gall-1d", type=int, default=130)
     ap.add_argument("--kall", type=int, default=42)
     ap.add_argument("--dt", type=float, default=360.0, help="SET_dt_large of the flux driver")
+    ap.add_argument("--precision", choices=["f64", "f32"], default="f64",
+                    help="f32: the FP32 entry points, as the drivers' single-precision (RP = SP) build")
     a = ap.parse_args(argv)
     dims = SnapshotDims(gall_1d=a.gall_1d, kall=a.kall)
     s = read_snapshot(a.kernel, a.path, dims)
@@ -222,7 +228,7 @@ def main(argv=None):
     for k, v in s.items():
         print(value_check(k, v))
     if a.action == "run":
-        got, diffs = run_snapshot(a.kernel, a.path, dims, a.dt)
+        got, diffs = run_snapshot(a.kernel, a.path, dims, a.dt, precision=a.precision)
         print(" ### Output ###")
         for k, v in got.items():
             print(value_check(k, v))

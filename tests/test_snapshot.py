@@ -25,9 +25,12 @@ def _geo_one_region(a, pole):
     return np.ascontiguousarray(a[..., None, :])
 
 
-def synthetic_snapshots(tmp_path, O):
-    """Writes the three drivers' snapshots from oracle outputs; returns {kernel: path}."""
-    c = case(4, 0, 8, 1)
+def synthetic_snapshots(tmp_path, O, zero_d=False):
+    """Writes the three drivers' snapshots from oracle outputs; returns {kernel: path}.
+    zero_d: the limiters' d = 0, as the composed step passes it."""
+    c = dict(case(4, 0, 8, 1))
+    if zero_d:
+        c["d"], c["d_pl"] = np.zeros_like(c["d"]), np.zeros_like(c["d_pl"])
     g, d, f = c["grid"], c["dims"], c["fields"]
     paths = {}
 
@@ -203,3 +206,21 @@ def test_cli_check_prints_driver_summaries(tmp_path, O, capsys):
     assert out[0].strip() == "### Input ###"
     assert [ln.split("]")[0].split("[")[1].strip() for ln in out[1:]] == \
         [n for n, _, _ in S.layout("dyn_vert_adv_limiter", DIMS)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", S.KERNELS)
+def test_run_snapshot_single_precision(tmp_path, O, cuda, kernel):
+    """The FP32 entry points on the same FP64 snapshots, as the drivers' RP = SP build reads and
+    converts them (d = 0): the flux and the limited values within FP32 rounding of the FP64
+    expected ones (normwise, the tolerances of the FP32 kernel tests).  Qout is left out: the
+    FP32 and FP64 zero-outflow switches differ on ill-conditioned cells."""
+    paths, dt = synthetic_snapshots(tmp_path, O, zero_d=True)
+    got, diffs = S.run_snapshot(kernel, paths[kernel], DIMS, dt=dt, precision="f32")
+    s = S.read_snapshot(kernel, paths[kernel], DIMS)
+    tol = 2e-5 if kernel == "dyn_horiz_adv_limiter" else 1e-5
+    for name, dv in diffs.items():
+        if name.startswith("Qout"):
+            continue
+        e = np.abs(dv).max() / max(np.abs(s[name]).max(), 1e-30)
+        assert e <= tol, (name, e)
