@@ -177,8 +177,11 @@ def run_snapshot(kernel, path, dims=SnapshotDims(), dt=360.0, device=0, precisio
     ctx = api.IcoAdv(dims.glevel, 0, dims.kall - 2, device)
     lall = ctx.sizes.lall
     full = {k: (_embed(v, lall) if not k.endswith("_pl") else np.ascontiguousarray(v)) for k, v in s.items()}
-    # kernel arguments in the working precision (the metrics stay FP64: the context keeps both)
-    a = {k: np.ascontiguousarray(v, dtype=rp) for k, v in full.items() if not k.startswith(("GRD_xr", "GMTR_"))}
+    # kernel arguments in the working precision (the metrics stay FP64: the context keeps both).
+    # In FP32 the +-HUGE-scale Qout bounds of cells without outflow become +-inf, as the
+    # single-precision drivers' conversion of the same snapshot does
+    with np.errstate(over="ignore"):
+        a = {k: np.ascontiguousarray(v, dtype=rp) for k, v in full.items() if not k.startswith(("GRD_xr", "GMTR_"))}
     try:
         if kernel == "dyn_horiz_adv_flux":
             geo = []
