@@ -224,3 +224,21 @@ def test_run_snapshot_single_precision(tmp_path, O, cuda, kernel):
             continue
         e = np.abs(dv).max() / max(np.abs(s[name]).max(), 1e-30)
         assert e <= tol, (name, e)
+
+
+def test_cli_run_prints_zero_diffs_with_oracle(tmp_path, O, monkeypatch, capsys):
+    """`run`: the input summaries, the outputs and the driver's point-by-point diff lines, here
+    with the oracle in the library's place (all diffs zero)."""
+    from icoatmosbenchmark_v1_b200 import api
+    monkeypatch.setattr(api, "IcoAdv", _OracleCtx)
+    paths, dt = synthetic_snapshots(tmp_path, O)
+    S.main(["run", "dyn_horiz_adv_flux", str(paths["dyn_horiz_adv_flux"]), "--gall-1d", "18", "--kall", "8",
+            "--dt", repr(dt)])
+    out = capsys.readouterr().out.splitlines()
+    i = out.index(" ### Validation : point-by-point diff ###")
+    diff = out[i + 1:]
+    assert [ln.split("[")[1].split("]")[0].strip() for ln in diff] == \
+        ["check_flx_h", "check_flx_h_pl", "check_GRD_xc", "check_GRD_xc_pl"]
+    zero = S._es(0.0)
+    for ln in diff:
+        assert ln.endswith(f"max={zero},min={zero},sum={zero}"), ln  # x - x is +0
