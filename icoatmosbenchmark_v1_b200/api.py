@@ -105,6 +105,21 @@ def topology_info(glevel, rlevel):
     return sgp, r4, ring
 
 
+def boundary_tables(glevel, rlevel):
+    """The batched step's boundary-value tables (ica_boundary_tables): nb, bsrc (lall*gall),
+    blist (nb), pole_ring (2, 5)."""
+    nb = C.c_int(0)
+    ip = C.POINTER(C.c_int)
+    _check("ica_boundary_tables", lib().ica_boundary_tables(glevel, rlevel, C.byref(nb), None, None, None))
+    g1 = 2 ** (glevel - rlevel) + 2
+    bsrc = np.zeros(10 * 4 ** rlevel * g1 * g1, np.int32)
+    blist = np.zeros(nb.value, np.int32)
+    ring = np.zeros((2, 5), np.int32)
+    _check("ica_boundary_tables", lib().ica_boundary_tables(glevel, rlevel, C.byref(nb), bsrc.ctypes.data_as(ip),
+                                                            blist.ctypes.data_as(ip), ring.ctypes.data_as(ip)))
+    return nb.value, bsrc, blist, ring
+
+
 def apply_plan_numpy(plan, var, var_pl):
     """Host-side application of a plan (used to fill halos of synthetic inputs)."""
     dst, src = plan

@@ -829,12 +829,17 @@ namespace icoadv {
 
 // Boundary tables of the batched path: which cells' gradient / Qout come from the
 // boundary pass (region-boundary cells, halo cells through the COMM plan, pole centres).
-int Ctx::build_fast_tables() {
-  if (fast.built) return ICA_OK;
-  const Topology &t = *topo;
+// Boundary-value tables of the batched step: bsrc (lall*gall) gives each region point its
+// boundary index (>= 0: a region-boundary cell, or the halo point's source; -1 an interior cell
+// off the region boundary; -2 a halo point no list writes), blist (nb) each boundary index's
+// point (the region-boundary cells, then the two pole centres) and ring (2*5) the boundary
+// index feeding each pole ring slot.
+static int fast_boundary_tables(const Topology &t, std::vector<int> &bsrc, std::vector<int> &blist,
+                                std::vector<int> &ring) {
   const int G = t.gall_1d, gall = t.gall, L = t.nrgn, g0 = t.gmin, g1 = t.gmax;
   const int npt = L * gall;
-  std::vector<int> bsrc((size_t)L * gall, -1), blist;
+  bsrc.assign((size_t)L * gall, -1);
+  blist.clear();
   for (int l = 0; l < L; ++l)
     for (int j = 1; j <= G; ++j)
       for (int i = 1; i <= G; ++i) {
@@ -849,7 +854,7 @@ int Ctx::build_fast_tables() {
   const int nbr = (int)blist.size();
   blist.push_back(npt + 0);
   blist.push_back(npt + kGallPl);
-  std::vector<int> ring(2 * kVlink, -1);
+  ring.assign(2 * kVlink, -1);
   std::vector<int> d, s;
   int rc = t.build_plan(false, d, s);
   if (rc) return rc;
@@ -871,6 +876,17 @@ int Ctx::build_fast_tables() {
   }
   for (int x : ring)
     if (x < 0) return set_error("fast tables: pole ring slot without a source"), ICA_ERR_INTERNAL;
+  return ICA_OK;
+}
+
+int Ctx::build_fast_tables() {
+  if (fast.built) return ICA_OK;
+  const Topology &t = *topo;
+  const int G = t.gall_1d, gall = t.gall, L = t.nrgn, g0 = t.gmin, g1 = t.gmax;
+  const int npt = L * gall;
+  std::vector<int> bsrc, blist, ring;
+  int rc = fast_boundary_tables(t, bsrc, blist, ring);
+  if (rc) return rc;
   // halo points no list writes (region corners at rlevel 0): the reference leaves them as they were
   std::vector<int> carry;
   for (int c = 0; c < npt; ++c)
@@ -1000,6 +1016,21 @@ int ica_fast_set_shape(ica_ctx *c, int shape) {
   int n = fast_tile_shapes(nullptr, nullptr, nullptr, 0);
   if (shape < 0 || shape >= n) return set_error("ica_fast_set_shape: no such tile shape"), ICA_ERR_ARG;
   c->fast.shape = shape;
+  return ICA_OK;
+}
+
+int ica_boundary_tables(int glevel, int rlevel, int *nb, int *bsrc, int *blist, int *pole_ring) {
+  if (!nb) return set_error("ica_boundary_tables: NULL count"), ICA_ERR_ARG;
+  if (glevel < 1 || rlevel < 0 || rlevel > glevel || glevel > 12)
+    return set_error("ica_boundary_tables: bad levels"), ICA_ERR_ARG;
+  Topology t(glevel, rlevel);
+  std::vector<int> bs, bl, ring;
+  const int rc = fast_boundary_tables(t, bs, bl, ring);
+  if (rc) return rc;
+  *nb = (int)bl.size();
+  if (bsrc) std::memcpy(bsrc, bs.data(), bs.size() * sizeof(int));
+  if (blist) std::memcpy(blist, bl.data(), bl.size() * sizeof(int));
+  if (pole_ring) std::memcpy(pole_ring, ring.data(), ring.size() * sizeof(int));
   return ICA_OK;
 }
 

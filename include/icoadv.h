@@ -402,6 +402,13 @@ int ica_comm_plan(int glevel, int rlevel, int pole_fill, int *n, int *dst, int *
 /* have_sgp[10*4^rl] (ADM_have_sgp), rgn4pl[2] (RGNMNG_rgn4pl),
  * pole_ring[2][5] (RGNMNG_vert_tab_pl region ids); any may be NULL. */
 int ica_topology_info(int glevel, int rlevel, int *have_sgp, int *rgn4pl, int *pole_ring);
+/* ica_boundary_tables (host only): the batched step's boundary-value tables.  bsrc[lall*gall]:
+ * a region point's boundary index (a region-boundary cell's own, a halo point's source's;
+ * -1 an interior cell off the region boundary, -2 a halo point no list writes); blist[*nb]:
+ * the point of each boundary index (region points l*gall + ij, then the two pole centres as
+ * lall*gall + 6*p); pole_ring[2][5]: the boundary index feeding each pole ring slot.  Call
+ * with NULL arrays to get *nb. */
+int ica_boundary_tables(int glevel, int rlevel, int *nb, int *bsrc, int *blist, int *pole_ring);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,169 @@
+"""The host side of region sharding (icoatmosbenchmark_v1_b200.shard): the plan's lists cover
+every value a rank reads from another rank exactly once, and two gloo ranks that exchange
+along them end with the halos of the single-process fill.  Packing and unpacking are numpy
+gathers here; on GPUs they are the library's pack/unpack step around NCCL send/recv."""
+import json
+import os
+import socket
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module")
+def plans(built):
+    from icoatmosbenchmark_v1_b200 import shard
+    return {(g, rl, n): shard.ShardPlan.build(g, rl, n) for g, rl, n in
+            [(4, 0, 1), (4, 0, 2), (4, 0, 3), (4, 1, 4), (4, 1, 7), (5, 0, 10)]}
+
+
+def test_region_blocks():
+    from icoatmosbenchmark_v1_b200.shard import region_blocks
+    assert region_blocks(10, 3) == [(0, 4), (4, 7), (7, 10)]
+    assert region_blocks(40, 8) == [(5 * r, 5 * r + 5) for r in range(8)]
+    with pytest.raises(ValueError):
+        region_blocks(10, 11)
+
+
+def test_single_rank_plan_is_local(plans):
+    from icoatmosbenchmark_v1_b200 import api
+    p = plans[(4, 0, 1)]
+    assert not p.bval_recv and not p.halo_recv
+    dst, src = api.comm_plan(4, 0)
+    np.testing.assert_array_equal(p.halo_local[0][0], dst)
+    np.testing.assert_array_equal(p.halo_local[0][1], src)
+
+
+@pytest.mark.parametrize("key", [(4, 0, 2), (4, 0, 3), (4, 1, 4), (4, 1, 7), (5, 0, 10)])
+def test_plan_covers_every_read_once(plans, key):
+    from icoatmosbenchmark_v1_b200 import api
+    p = plans[key]
+    g, rl, n = key
+    dst, src = api.comm_plan(g, rl)
+    nb, bsrc, blist, ring = api.boundary_tables(g, rl)
+    npt = p.nrgn * p.gall
+
+    def owner(pt):
+        return 0 if pt >= npt else next(r for r, (a, b) in enumerate(p.blocks) if a <= pt // p.gall < b)
+
+    # halo fill: every plan copy appears once, on the rank of its destination, local or
+    # received from the rank of its source
+    seen = {}
+    for r in range(n):
+        pairs = [p.halo_local[r]] + [v for (rr, q), v in p.halo_recv.items() if rr == r]
+        for (q_dst, q_src) in pairs:
+            for d, s in zip(q_dst.tolist(), q_src.tolist()):
+                assert owner(d) == r and d not in seen
+                seen[d] = s
+    for (r, q), (d, s) in p.halo_recv.items():
+        assert all(owner(x) == q for x in s.tolist())
+    assert seen == dict(zip(dst.tolist(), src.tolist()))
+    # boundary values: what a rank's tiles, seam and pole passes read is computed by it or
+    # received once, from the rank that computes it
+    for r, (a, b) in enumerate(p.blocks):
+        need = set(bsrc[a * p.gall:b * p.gall][bsrc[a * p.gall:b * p.gall] >= 0].tolist())
+        if r == 0:
+            need |= set(ring.ravel().tolist()) | {nb - 2, nb - 1}
+        got = {}
+        for (rr, q), lst in p.bval_recv.items():
+            if rr != r:
+                continue
+            for x in lst.tolist():
+                assert x not in got and owner(blist[x]) == q != r
+                got[x] = q
+        assert {x for x in need if owner(blist[x]) != r} == set(got)
+    v_b, v_h = p.bytes_per_step(kall=8, ntr=2)
+    assert v_b > 0 and v_h > 0
+
+
+def _port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _exchange_worker(rank, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, str(ROOT))
+    import torch
+    import torch.distributed as dist
+    from icoatmosbenchmark_v1_b200 import api, shard
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    g, rl, m, K = 4, 1, 2, 3
+    p = shard.ShardPlan.build(g, rl, 2)
+    dst, src = api.comm_plan(g, rl)
+    nb, bsrc, blist, ring = api.boundary_tables(g, rl)
+    npt = p.nrgn * p.gall + 12
+    rng = np.random.default_rng(11)
+    R = rng.standard_normal((m, K, npt))      # every point's value before the fill
+    V = rng.standard_normal((nb, 5, K))       # every boundary index's values
+    mine = np.zeros(npt, bool)
+    mine[p.owned_points(rank)] = True
+    is_dst = np.zeros(npt, bool)
+    is_dst[dst] = True
+    X = np.full((m, K, npt), np.nan)
+    X[:, :, mine & ~is_dst] = R[:, :, mine & ~is_dst]
+    comp = np.array([0 if b >= npt - 12 else next(r for r, (a, c) in enumerate(p.blocks) if a <= b // p.gall < c)
+                     for b in blist])
+    B = np.full(V.shape, np.nan)
+    B[comp == rank] = V[comp == rank]
+
+    def swap(recv_key, send_key, send_arr, shape):
+        reqs, buf = [], None
+        if send_key in send_arr:
+            reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(send_arr[send_key])), dst=1 - rank))
+        if recv_key is not None:
+            buf = torch.empty(shape, dtype=torch.float64)
+            reqs.append(dist.irecv(buf, src=1 - rank))
+        for q in reqs:
+            q.wait()
+        return None if buf is None else buf.numpy()
+
+    # (1) boundary values, then (2) the halo fill; keys are (receiver, sender)
+    other = 1 - rank
+    sends = {}
+    if (other, rank) in p.bval_recv:
+        sends[(other, rank)] = B[p.bval_recv[(other, rank)]]
+    lst = p.bval_recv.get((rank, other))
+    got = swap((rank, other) if lst is not None else None, (other, rank), sends,
+               (0 if lst is None else lst.size, 5, K))
+    if lst is not None:
+        B[lst] = got
+    sends = {}
+    if (other, rank) in p.halo_recv:
+        sends[(other, rank)] = X[:, :, p.halo_recv[(other, rank)][1]]
+    pr = p.halo_recv.get((rank, other))
+    got = swap((rank, other) if pr is not None else None, (other, rank), sends,
+               (m, K, 0 if pr is None else pr[0].size))
+    if pr is not None:
+        X[:, :, pr[0]] = got
+    ld, ls = p.halo_local[rank]
+    X[:, :, ld] = X[:, :, ls]
+    # what the rank reads after the fill equals the single-process fill
+    ref = R.copy()
+    ref[:, :, dst] = ref[:, :, src]
+    a, b = p.blocks[rank]
+    own_dst = dst[(dst < npt - 12) & (dst // p.gall >= a) & (dst // p.gall < b)] if rank else \
+        dst[((dst < npt - 12) & (dst // p.gall >= a) & (dst // p.gall < b)) | (dst >= npt - 12)]
+    ok_halo = bool(np.array_equal(X[:, :, own_dst], ref[:, :, own_dst]))
+    need = bsrc[a * p.gall:b * p.gall]
+    need = np.unique(need[need >= 0])
+    if rank == 0:
+        need = np.unique(np.concatenate([need, ring.ravel(), [nb - 2, nb - 1]]))
+    ok_bval = bool(np.array_equal(B[need], V[need]))
+    dist.destroy_process_group()
+    Path(out, f"rank{rank}.json").write_text(json.dumps({"halo": ok_halo, "bval": ok_bval,
+                                                        "nhalo": int(own_dst.size), "nneed": int(need.size)}))
+
+
+def test_two_rank_exchange_gloo(tmp_path, built):
+    import torch.multiprocessing as mp
+    os.environ["CUDA_VISIBLE_DEVICES"] = ""
+    mp.start_processes(_exchange_worker, args=(_port(), str(tmp_path)), nprocs=2, start_method="spawn", join=True)
+    for r in (0, 1):
+        d = json.loads((tmp_path / f"rank{r}.json").read_text())
+        assert d["halo"] and d["bval"] and d["nhalo"] > 0 and d["nneed"] > 0, d
