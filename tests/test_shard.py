@@ -167,3 +167,34 @@ def test_two_rank_exchange_gloo(tmp_path, built):
     for r in (0, 1):
         d = json.loads((tmp_path / f"rank{r}.json").read_text())
         assert d["halo"] and d["bval"] and d["nhalo"] > 0 and d["nneed"] > 0, d
+
+
+@pytest.mark.parametrize("glevel,rlevel", [(4, 0), (4, 1), (5, 2)])
+def test_boundary_tables(built, glevel, rlevel):
+    """ica_boundary_tables, the tables the batched step reads: boundary indices of the region
+    edge cells in order, then the two pole centres; a halo point takes its plan source's
+    index; every pole ring slot has one; interior cells off the edge -1, unwritten halo -2."""
+    from icoatmosbenchmark_v1_b200 import api
+    nb, bsrc, blist, ring = api.boundary_tables(glevel, rlevel)
+    g1 = 2 ** (glevel - rlevel) + 2
+    gall, L = g1 * g1, 10 * 4 ** rlevel
+    npt = L * gall
+    ij = np.arange(gall)
+    i, j = ij % g1 + 1, ij // g1 + 1
+    inner = (i >= 2) & (i <= g1 - 1) & (j >= 2) & (j <= g1 - 1)
+    edge = inner & ((i == 2) | (i == g1 - 1) | (j == 2) | (j == g1 - 1))
+    cells = (np.arange(L)[:, None] * gall + ij[edge][None, :]).ravel()
+    np.testing.assert_array_equal(blist, np.concatenate([cells, [npt, npt + 6]]))
+    np.testing.assert_array_equal(bsrc[cells], np.arange(cells.size))
+    b2 = bsrc.reshape(L, gall)
+    assert (b2[:, inner & ~edge] == -1).all()
+    dst, src = api.comm_plan(glevel, rlevel)
+    rd = dst < npt
+    exp = np.where(src[rd] < npt, bsrc[np.minimum(src[rd], npt - 1)], cells.size + (src[rd] - npt) // 6)
+    np.testing.assert_array_equal(bsrc[dst[rd]], exp)
+    assert ((ring >= 0) & (ring < nb)).all()
+    halo = np.ones(npt, bool)
+    halo[(np.arange(L)[:, None] * gall + ij[inner][None, :]).ravel()] = False
+    unwritten = halo.copy()
+    unwritten[dst[rd]] = False
+    assert (bsrc[unwritten] == -2).all()
