@@ -1090,8 +1090,9 @@ __global__ void __launch_bounds__(256, 2) k_fast_vert(const __grid_constant__ Mu
 
 // ---- the two pole centres, FP64: one CTA per (pole, tracer), one thread per level ----------
 // The horizontal sub-step of every level, then the vertical one of the column: its Qout of a
-// level needs only q and the Courant numbers, so every stage is level-parallel, with the
-// arithmetic of each value as in the column form of the plain path.
+// level needs only q and the Courant numbers, so every stage is level-parallel.  Each value
+// takes the operations of the column form; this file allows FMA contraction, so results
+// can differ from that form at FP64 rounding.
 template <int KMAX>
 __global__ void __launch_bounds__(KMAX) k_fast_pole(const __grid_constant__ MultiInst M) {
   long long tl = blockIdx.x;
