@@ -13,8 +13,8 @@ value : updates/s of the device-resident step loop (CUDA events on the library's
         stream, max over ranks); e2e: the same metric through the host-pointer
         C ABI call with pinned host buffers, copies inside the timed region.
 --impl reference: the CPU restatement of the reference (oracle) on all host
-        cores, on a bounded sample of the workload (glevel 6, same kall/tracers per
-        step), reported in the same unit.
+        cores, on a bounded sample of the workload (each step: the same glevel 8
+        grid and 32 tracers, 10 of the 94 physical levels), reported in the same unit.
 N > 1: one process per GPU, each running an independent replica of the workload
 (the single-GPU path does not shard), value = total updates / max time.
 """
@@ -137,13 +137,15 @@ def barrier(world):
 
 # ---------------------------------------------------------------------------------------------
 def cpu_reference(glevel, kall, ntr, steps, warmup, threads):
-    """The oracle (C restatement of the reference) on `threads` host cores; returns updates/s."""
+    """The oracle (C restatement of the reference) on `threads` host cores; returns updates/s.
+    The grid's topology and halo plan come from the oracle too (oracle.GridTables), so this
+    leg loads no part of the library under test."""
     import numpy as np
 
     from icoatmosbenchmark_v1_b200 import fields as F
     from icoatmosbenchmark_v1_b200.grid import Grid, default_dt
     from oracle import oracle as O
-    g = Grid(glevel, 0, kall)
+    g = Grid(glevel, 0, kall, tables=O.GridTables())
     f = {k: v.numpy() for k, v in F.make_fields(g).items()}
     S = {k: v.numpy().copy() for k, v in F.make_state(g, ntr, "mixed").items()}
     d = O.make_dims(glevel, 0, kall)
@@ -163,14 +165,16 @@ def run_reference_arm(args, world, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    gl = args.ref_glevel
-    val, el, upd, _ = cpu_reference(gl, args.kall, args.ntr, args.steps, args.warmup, threads)
-    sample = f"glevel {gl}, kall {args.kall}, {args.ntr} tracers, {args.steps} steps ({upd:.3e} updates)"
+    ks = args.ref_kall
+    val, el, upd, _ = cpu_reference(args.glevel, ks, args.ntr, args.steps, args.warmup, threads)
+    sample = (f"each step: glevel {args.glevel}, all {args.ntr} tracers, {ks - 2} of the {args.kall - 2} "
+              f"physical levels (kall {ks}); {args.steps} steps, {upd:.3e} updates")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(args),
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "sample_updates_per_step": upd // max(args.steps, 1),
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -221,16 +225,21 @@ def run_ours(args, world, rank, local):
         s_bytes = 32
 
     err = m0 = None
+    extra = args.mode == "fast" and world == 1 and rank == 0 and not args.no_extra and not args.no_check
+    init = ref = None
     if args.mode != "plain" and not args.no_check:
         # one FP64 plain-path step on a copy: the reference of the batched step's first step
         ref = {k: v.clone() for k, v in runner.state.items()}
+        if extra:  # the FP64 variant starts from the same state later
+            init = {k: v.clone() for k, v in runner.state.items()}
         ctx.advect_step(dt, ref["rhog"], ref["rhog_pl"], ref["rhogq"], ref["rhogq_pl"], f["rhogvx"], f["rhogvx_pl"],
                         f["rhogvy"], f["rhogvy_pl"], f["rhogvz"], f["rhogvz_pl"], f["rhogw"], f["rhogw_pl"])
         m0 = tracer_mass(g, runner.state)
         step()
         torch.cuda.synchronize()
         err = float(((runner.state["rhogq"] - ref["rhogq"]).abs().max() / ref["rhogq"].abs().max()).item())
-        del ref
+        if not extra:
+            ref = None
         torch.cuda.empty_cache()
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -286,11 +295,13 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        cval, cel, cupd, _ = cpu_reference(args.ref_glevel, args.kall, args.ntr, 1, 0, threads)
+        cval, cel, cupd, _ = cpu_reference(args.glevel, args.ref_kall, args.ntr, 1, 0, threads)
         cpu = {"value": cval, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"oracle, glevel {args.ref_glevel}, kall {args.kall}, {args.ntr} tracers, 1 step "
+               "sample": f"oracle, glevel {args.glevel}, all {args.ntr} tracers, {args.ref_kall - 2} of the "
+                         f"{args.kall - 2} physical levels (kall {args.ref_kall}), 1 step "
                          f"({cupd:.3e} updates, {cel:.1f} s)"}
     cfg = workload_config(args)
+    shape_idx = runner.shape if args.mode != "plain" else None
     if args.mode != "plain":
         cfg["tile"] = {"shape_txtytg": list(ctx.fast_shapes()[runner.shape]),
                        "autotune_ms": [round(t["ms"], 3) for t in runner.tuning] or None}
@@ -302,6 +313,16 @@ def run_ours(args, world, rank, local):
         if err is not None:
             line["max_rel_err_vs_fp64"] = err  # first step vs the FP64 plain path (bit-exact to the oracle)
             line["mass_drift"] = {"value": drift, "steps": 1 + args.warmup + args.steps}
+    if extra:  # the FP64 variant of the batched step on the same workload, from the same state
+        runner = step = None
+        st = None
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+        line["fp64_variant"] = measure_fast64(args, ctx, g, init, ref, f, dt, shape_idx, ms)
+        init = ref = None
+        gc.collect()
+        torch.cuda.empty_cache()
     ctx.close()
     if rank == 0 and world == 1 and not args.no_adjoint and args.mode == "fast":
         runner = st = f = step = None  # the bound step method holds the runner and its buffers
@@ -310,8 +331,51 @@ def run_ours(args, world, rank, local):
         torch.cuda.empty_cache()
         line["adjoint"] = measure_adjoint(args, local, fast_ms=ms, steps=args.adjoint_steps,
                                           every=args.adjoint_every)
+    if extra:
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+        line["uneven_batch"] = measure_uneven(args, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def measure_fast64(args, ctx, g, init, ref, f, dt, shape, ms32):
+    """The FP64 variant of the batched step (FP64 fields, face values, bounds and limiters) on
+    the workload of the line, from the line's initial state: its first step's max relative
+    error against the plain FP64 step, its device time per step (CUDA events on the library's
+    stream) and the relative mass drift over its steps."""
+    import torch
+
+    from icoatmosbenchmark_v1_b200 import api
+    r = api.FastRunner(ctx, g, init, f, dt, autotune=False, f64=True)
+    ctx.fast_set_shape(shape)
+    r.shape = shape
+    m0 = tracer_mass(g, r.state)
+    r.step()
+    torch.cuda.synchronize()
+    err = float(((r.state["rhogq"] - ref["rhogq"]).abs().max() / ref["rhogq"].abs().max()).item())
+    for _ in range(max(args.warmup - 1, 1)):
+        r.step()
+    n = max(1, min(args.steps, 5))
+    stream = torch.cuda.ExternalStream(ctx.stream, device=init["rhog"].device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(n):
+        r.step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    m1 = tracer_mass(g, r.state)
+    drift = float(((m1 - m0).abs() / m0.abs()).max().item())
+    upd = (10 * 4 ** args.glevel + 2) * args.kall * args.ntr
+    out = {"workload": f"gl{args.glevel}_k{args.kall}_t{args.ntr}", "dtype": "f64", "steps": n,
+           "ms_per_step": ms, "value": upd / (ms * 1e-3), "unit": UNIT,
+           "max_rel_err_vs_fp64_plain": err, "mass_drift": {"value": drift, "steps": 1 + max(args.warmup - 1, 1) + n},
+           "time_vs_fp32_variant": ms / ms32}
+    del r
+    return out
 
 
 UNEVEN = ((7, 96, 40), (6, 42, 12))  # (glevel, kall, tracers) of the two instances
@@ -332,11 +396,23 @@ def tracer_mass(g, S):
 
 
 def run_uneven(args, world, rank, local):
+    """`--mode uneven`: the uneven batch (measure_uneven) as the line's workload."""
+    out = measure_uneven(args, local)
+    if rank == 0:
+        line = {"metric": METRIC, "value": out["value"], "unit": UNIT, "n_gpus": world, "steps": out["steps"],
+                "warmup": args.warmup, "ms_per_step": out["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": out["config"]}
+        line.update({k: v for k, v in out.items() if k not in ("value", "ms_per_step", "steps", "config")})
+        print(json.dumps(line), flush=True)
+
+
+def measure_uneven(args, local):
     """Batch of two uneven grid instances (glevel 7 / kall 96 / 40 tracers and glevel 6 / kall 42 /
     12 tracers) advanced by the same launches and replayed from a CUDA graph, in the FP32 variant
-    (the line's value) and the FP64 variant (`fp64_variant`).  Each reports its max relative
-    error against the plain FP64 step after one step and the relative mass drift over the
-    timed steps; the plain FP64 step of both instances is timed beside them."""
+    (`value`) and the FP64 variant (`fp64_variant`).  Each reports its max relative error
+    against the plain FP64 step after one step and the relative mass drift over the timed
+    steps; the plain FP64 step of both instances is timed beside them."""
     import torch
 
     from icoatmosbenchmark_v1_b200 import api
@@ -436,24 +512,21 @@ def run_uneven(args, world, rank, local):
     m1 = masses(b64.states)
     drift64 = max(float(((b - a).abs() / a.abs()).max().item()) for a, b in zip(m0, m1))
     b64.close()
-    if rank == 0:
-        shape = list(ctxs[0].fast_shapes()[best[0]])
-        line = {"metric": METRIC, "value": upd / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "uneven_gl7_k96_t40+gl6_k42_t12", "instances": [list(x) for x in UNEVEN],
-                           "updates_per_step": upd, "launch": "one launch per stage over both instances, "
-                           "persistent horizontal kernel, step replayed from a CUDA graph",
-                           "tile": {"shape_txtytg": shape, "autotune_ms": tuning}},
-                "fp64_plain_ms_per_step": ms64, "max_rel_err_vs_fp64": err,
-                "mass_drift": {"value": drift, "steps": args.steps + args.warmup},
-                "fp64_variant": {"ms_per_step": ms_f64, "value": upd / (ms_f64 * 1e-3),
-                                 "max_rel_err_vs_fp64_plain": err64,
-                                 "mass_drift": {"value": drift64, "steps": 1 + args.steps + args.warmup}},
-                "gpu_launches": launches, "clocks": clocks}
-        print(json.dumps(line), flush=True)
+    shape = list(ctxs[0].fast_shapes()[best[0]])
+    out = {"value": upd / (ms * 1e-3), "unit": UNIT, "steps": args.steps, "ms_per_step": ms, "dtype": "f32",
+           "config": {"workload": "uneven_gl7_k96_t40+gl6_k42_t12", "instances": [list(x) for x in UNEVEN],
+                      "updates_per_step": upd, "launch": "one launch per stage over both instances, "
+                      "persistent horizontal kernel, step replayed from a CUDA graph",
+                      "tile": {"shape_txtytg": shape, "autotune_ms": tuning}},
+           "fp64_plain_ms_per_step": ms64, "max_rel_err_vs_fp64": err,
+           "mass_drift": {"value": drift, "steps": args.steps + args.warmup},
+           "fp64_variant": {"ms_per_step": ms_f64, "value": upd / (ms_f64 * 1e-3),
+                            "max_rel_err_vs_fp64_plain": err64,
+                            "mass_drift": {"value": drift64, "steps": 1 + args.steps + args.warmup}},
+           "gpu_launches": launches, "clocks": clocks}
     for c in ctxs:
         c.close()
+    return out
 
 
 def measure_adjoint(args, local, fast_ms=None, steps=12, every=4):
@@ -581,12 +654,15 @@ def main():
     ap.add_argument("--glevel", type=int, default=8)
     ap.add_argument("--kall", type=int, default=96)
     ap.add_argument("--ntr", type=int, default=32)
-    ap.add_argument("--ref-glevel", type=int, default=6)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-kall", type=int, default=12,
+                    help="kall of the CPU sample (same grid level and tracers, fewer levels per step)")
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true", help="skip the error / mass-drift check")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint sweep measurement")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the FP64 variant and the uneven batch (extra keys of the default line)")
     ap.add_argument("--adjoint-steps", type=int, default=12, help="steps of the adjoint sweep")
     ap.add_argument("--adjoint-every", type=int, default=4, help="checkpoint interval of the adjoint sweep")
     ap.add_argument("--tile-shape", type=int, default=-1, help="tile shape index of the horizontal kernel (default: autotune)")

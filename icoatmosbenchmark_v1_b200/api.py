@@ -122,13 +122,8 @@ def boundary_tables(glevel, rlevel):
 
 def apply_plan_numpy(plan, var, var_pl):
     """Host-side application of a plan (used to fill halos of synthetic inputs)."""
-    dst, src = plan
-    m, L, K, G = var.shape
-    flat = np.concatenate([var.transpose(0, 2, 1, 3).reshape(m, K, L * G),
-                           var_pl.transpose(0, 2, 1, 3).reshape(m, K, 12)], axis=2)
-    flat[:, :, dst] = flat[:, :, src]
-    var[...] = flat[:, :, :L * G].reshape(m, K, L, G).transpose(0, 2, 1, 3)
-    var_pl[...] = flat[:, :, L * G:].reshape(m, K, 2, 6).transpose(0, 2, 1, 3)
+    from .grid import apply_plan_numpy as apply
+    apply(plan, var, var_pl)
 
 
 # ---- the context ------------------------------------------------------------------
@@ -371,8 +366,8 @@ class IcoAdv:
         _check("ica_fast_timing", lib().ica_fast_timing(self.h, int(enable), C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
-    def fast_runner(self, grid, state, fields, dt, autotune=True):
-        return FastRunner(self, grid, state, fields, dt, autotune)
+    def fast_runner(self, grid, state, fields, dt, autotune=True, f64=False):
+        return FastRunner(self, grid, state, fields, dt, autotune, f64)
 
 
 STATE_KEYS = ("rhog", "rhog_pl", "rhogq", "rhogq_pl")
@@ -381,19 +376,22 @@ WIND_KEYS = ("rhogvx", "rhogvx_pl", "rhogvy", "rhogvy_pl", "rhogvz", "rhogvz_pl"
 
 
 class FastRunner:
-    """Device-resident loop of the batched step: double-buffered FP64 state, FP32 fields, tile
-    shape chosen by timing every available shape on the real inputs (the autotuner)."""
+    """Device-resident loop of the batched step: double-buffered FP64 state, FP32 fields (FP64
+    fields and arithmetic for the FP64 variant, f64=True), tile shape chosen by timing every
+    available shape on the real inputs (the autotuner)."""
 
-    def __init__(self, ctx, grid, state, fields, dt, autotune=True):
+    def __init__(self, ctx, grid, state, fields, dt, autotune=True, f64=False):
         import torch
         self.ctx, self.dt = ctx, dt
+        self.f64 = bool(f64)
         self.a = state
         self.b = {k: torch.empty_like(v) for k, v in state.items()}
-        self.f32 = {k: fields[k].to(torch.float32).contiguous() for k in FIELD_KEYS}
+        ft = torch.float64 if self.f64 else torch.float32
+        self.f32 = {k: fields[k].to(ft).contiguous() for k in FIELD_KEYS}
         self.updates = (10 * 4 ** grid.glevel + 2) * grid.kall * state["rhogq"].shape[0]
         # algorithmic bytes of one tracer cell-level update: rhogq read + write (FP64); per cell-level,
-        # shared by the tracers: rhog old and new (FP64) and rhogv x/y/z + rhogw (FP32)
-        self.alg_bytes = 16.0 + 32.0 / state["rhogq"].shape[0]
+        # shared by the tracers: rhog old and new (FP64) and rhogv x/y/z + rhogw (FP32, or FP64)
+        self.alg_bytes = 16.0 + (48.0 if self.f64 else 32.0) / state["rhogq"].shape[0]
         self.shape = 0
         self.tuning = []
         if autotune:
@@ -404,7 +402,10 @@ class FastRunner:
         return self.a
 
     def step(self):
-        self.ctx.advect_fast_dev(self.dt, self.a, self.b, self.f32)
+        if self.f64:
+            self.ctx.advect_fast64_dev(self.dt, self.a, self.b, self.f32)
+        else:
+            self.ctx.advect_fast_dev(self.dt, self.a, self.b, self.f32)
         self.a, self.b = self.b, self.a
 
     def autotune(self, reps=2):

@@ -126,6 +126,10 @@ int ica_init(const ica_dims *dims, ica_ctx **out) {
   c->D.kmax = s.kmax;
   c->D.lall = s.lall;
   c->D.have_sgp = c->d_have_sgp;
+  // the noalloc limiter's fixed scratch: loaded now, while the context is created, so that
+  // its first call takes no device memory (with lazy module loading the array would
+  // otherwise be set up inside that call)
+  if (noalloc_scratch_address(&c->noalloc_scratch) != ICA_OK) c->noalloc_scratch = nullptr;
   e = cudaGetLastError();
   if (e != cudaSuccess) { delete c; return cuda_fail(e, "ica_init"); }
   *out = c;
@@ -265,8 +269,10 @@ int hlim_dev(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, c
   c->launches += 2;
   const T *Qo = Qout_post, *Qo_pl = Qout_post_pl;
   if (!Qout_post) {  // NICAM: COMM_data_transfer(Qout, Qout_pl) on a copy of the pre-fill Qout
-    cudaMemcpyAsync(scratch_Qout, Qout_prev, n2 * sizeof(T), cudaMemcpyDeviceToDevice, c->stream);
-    cudaMemcpyAsync(scratch_Qout_pl, Qout_prev_pl, n2p * sizeof(T), cudaMemcpyDeviceToDevice, c->stream);
+    cudaError_t e = cudaMemcpyAsync(scratch_Qout, Qout_prev, n2 * sizeof(T), cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "horizontal_limiter_thuburn: copy of Qout");
+    e = cudaMemcpyAsync(scratch_Qout_pl, Qout_prev_pl, n2p * sizeof(T), cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "horizontal_limiter_thuburn: copy of Qout_pl");
     const Plan &p = c->plan[0];
     launch_gather<T>(c->D, p.n, p.dst, p.src, c->sz.kall, 2, scratch_Qout, scratch_Qout_pl, c->stream);
     c->launches += 1;
@@ -277,6 +283,10 @@ int hlim_dev(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, c
   c->launches += 2;
   return c->check_launch("horizontal_limiter_thuburn");
 }
+
+template int hlim_dev<double>(Ctx *, double *, double *, const double *, const double *, const double *,
+                              const double *, const double *, const double *, const double *, const double *,
+                              double *, double *, const double *, const double *, double *, double *, double *);
 
 template <typename T>
 int hlim_dev_alloc(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, const T *d_pl, const T *ch,

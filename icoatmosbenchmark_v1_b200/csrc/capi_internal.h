@@ -78,8 +78,24 @@ struct Ctx {
   int build_fast_tables();
   int fast_inst(FastInst &I, int ntr, double dt, bool f64 = false);
   AdjTape tape;
+  // device address of the fixed scratch of ica_horizontal_limiter_thuburn_noalloc on this
+  // context's device, looked up by ica_init (nullptr if that lookup failed)
+  double *noalloc_scratch = nullptr;
 };
 
 int cuda_fail(cudaError_t e, const char *what);
+
+// horizontal_limiter_thuburn on device buffers with caller-provided scratch: the Qout copy
+// the halo fill runs on (gall*kall*lall*2 and 6*kall*2*2 values) and the pole inflow bounds
+// (6*kall*2*4 values).  Instantiated for double in capi.cu.
+template <typename T>
+int hlim_dev(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, const T *d_pl, const T *ch,
+             const T *ch_pl, const T *cmask, const T *cmask_pl, T *Qout_prev, T *Qout_prev_pl, const T *Qout_post,
+             const T *Qout_post_pl, T *scratch_Qout, T *scratch_Qout_pl, T *scratch_Qin_pl);
+
+// Device address of the noalloc limiter's fixed scratch array in the current device's
+// context.  Looking it up loads the module that holds the array, so its device memory is
+// taken at that moment (ica_init calls this).
+int noalloc_scratch_address(double **out);
 
 }  // namespace icoadv

@@ -11,8 +11,8 @@ Per configuration (rl 0, R = 6.371e6 m):
           from the discrete continuity equation, so rho stays steady (see make_fields)
   tracers in [0,1]: "bell" = cosine bell of radius R/3 plus a slotted cylinder
           (per tracer the two centres rotate in longitude), "smooth" = random
-          band-limited field (plane waves with |k| <= 16 on the unit sphere,
-          standing in for spherical-harmonic degree <= 16) clipped to [0,1];
+          field of real spherical harmonics of degree <= 16 (seeded
+          coefficients) scaled about 0.5 and clipped to [0,1];
           each with a vertical profile that steps at 12 km so the vertical
           limiter is active.
 Seeds: numpy PCG64(20261203) for the noise, tracer i uses seed 20261203 + 1 + i.
@@ -216,15 +216,46 @@ def _bell_cylinder(x, lon0, lat0, R_frac=1.0 / 3.0):
     return torch.clamp(bell + cyl, 0.0, 1.0)
 
 
-def _smooth_random(x, seed, kmax=16.0, nwaves=24):
+def spherical_harmonic_field(x, seed, lmax=16):
+    """Random band-limited field on the unit sphere: sum over degrees l <= lmax and orders
+    |m| <= l of a_lm Y_lm(x), real orthonormal spherical harmonics, with seeded coefficients
+    a_lm ~ N(0, 1) / (1 + l) (a red spectrum, so the field is smooth at the grid scale).
+    x: unit vectors (3, ...).  The associated Legendre functions come from the standard
+    fully normalised three-term recurrences in l (stable to l of a few hundred)."""
     g = torch.Generator(device="cpu").manual_seed(seed)
-    f = torch.zeros(x.shape[1:], dtype=x.dtype, device=x.device)
-    for _ in range(nwaves):
-        k = torch.randn(3, generator=g, dtype=torch.float64)
-        k = k / k.norm() * (torch.rand(1, generator=g, dtype=torch.float64) * kmax)
-        ph = float(torch.rand(1, generator=g) * 2 * math.pi)
-        a = float(torch.randn(1, generator=g))
-        f = f + a * torch.cos((x * k.to(x.device).view(3, *([1] * (x.dim() - 1)))).sum(0) + ph)
+    ct = torch.clamp(x[2], -1.0, 1.0)
+    st = torch.sqrt(torch.clamp(1.0 - ct * ct, min=0.0))
+    phi = torch.atan2(x[1], x[0])
+    f = torch.zeros_like(ct)
+    pmm = torch.full_like(ct, 1.0 / math.sqrt(4.0 * math.pi))  # P_0^0
+    for m in range(lmax + 1):
+        if m > 0:
+            pmm = -math.sqrt((2.0 * m + 1.0) / (2.0 * m)) * st * pmm
+        p_lm2, p_lm1 = None, pmm  # P_{l-2}^m, P_{l-1}^m with l-1 = m
+        cm, sm = (torch.cos(m * phi), torch.sin(m * phi)) if m > 0 else (None, None)
+        for l in range(m, lmax + 1):
+            if l == m:
+                p = pmm
+            elif l == m + 1:
+                p = math.sqrt(2.0 * m + 3.0) * ct * pmm
+            else:
+                a = math.sqrt((4.0 * l * l - 1.0) / (l * l - m * m))
+                b = math.sqrt(((l - 1.0) ** 2 - m * m) / (4.0 * (l - 1.0) ** 2 - 1.0))
+                p = a * (ct * p_lm1 - b * p_lm2)
+            if l > m:
+                p_lm2, p_lm1 = p_lm1, p
+            amp = 1.0 / (1.0 + l)
+            if m == 0:
+                f = f + amp * float(torch.randn(1, generator=g, dtype=torch.float64)) * p
+            else:
+                c1, c2 = torch.randn(2, generator=g, dtype=torch.float64).tolist()
+                f = f + amp * math.sqrt(2.0) * p * (c1 * cm + c2 * sm)
+    return f
+
+
+def _smooth_random(x, seed, lmax=16):
+    """Seeded spherical-harmonic field of degree <= lmax, scaled about 0.5 and clipped to [0, 1]."""
+    f = spherical_harmonic_field(x, seed, lmax)
     f = 0.5 + 0.5 * f / (f.abs().max() + 1e-30) * 1.2
     return torch.clamp(f, 0.0, 1.0)
 

@@ -31,8 +31,6 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import api
-
 RADIUS = 6.371e6
 TI, TJ = 0, 1
 AI, AIJ, AJ = 0, 1, 2
@@ -52,6 +50,18 @@ def _tri_area(a, b, c):
 def _arc_angle(a, b):
     """Angle between unit vectors, robust for small angles."""
     return np.arctan2(np.linalg.norm(np.cross(a, b), axis=-1), np.einsum("...i,...i", a, b))
+
+
+def apply_plan_numpy(plan, var, var_pl):
+    """Host-side application of a composed halo plan (dst[e] <- src[e] over the flat point
+    index: region points, then the 12 pole slots) to var (m, lall, K, gall), var_pl (m, 2, K, 6)."""
+    dst, src = plan
+    m, L, K, G = var.shape
+    flat = np.concatenate([var.transpose(0, 2, 1, 3).reshape(m, K, L * G),
+                           var_pl.transpose(0, 2, 1, 3).reshape(m, K, 12)], axis=2)
+    flat[:, :, dst] = flat[:, :, src]
+    var[...] = flat[:, :, :L * G].reshape(m, K, L, G).transpose(0, 2, 1, 3)
+    var_pl[...] = flat[:, :, L * G:].reshape(m, K, 2, 6).transpose(0, 2, 1, 3)
 
 
 def diamond_corners():
@@ -122,6 +132,10 @@ class Grid:
     kall: int
     R: float = RADIUS
     arrays: dict = field(default_factory=dict)
+    # provider of the region topology and the halo plan: an object with
+    # topology_info(glevel, rlevel) -> (have_sgp, rgn4pl, pole_ring) and
+    # comm_plan(glevel, rlevel, pole_fill) -> (dst, src); None: this library's host tables
+    tables: object = None
 
     def __post_init__(self):
         gl, rl = self.glevel, self.rlevel
@@ -131,8 +145,12 @@ class Grid:
         self.gmin, self.gmax = 2, self.nmax + 1
         self.lall = 10 * 4 ** rl
         self.kmin, self.kmax = (2, self.kall - 1) if self.kall > 1 else (1, 1)
-        self.have_sgp, self.rgn4pl, self.pole_ring = api.topology_info(gl, rl)
-        self.plan = api.comm_plan(gl, rl, False)
+        tables = self.tables
+        if tables is None:
+            from . import api as tables
+        self.have_sgp, self.rgn4pl, self.pole_ring = tables.topology_info(gl, rl)
+        self.plan = tables.comm_plan(gl, rl, False)
+        self.tables = None  # the plan is held; the provider is not needed after construction
         self._build_positions()
         self._build_metrics()
         self._build_gradient()
@@ -145,7 +163,7 @@ class Grid:
         m = a.shape[0]
         v = a.reshape(m, self.lall, 1, self.gall).copy()
         vp = a_pl.reshape(m, 2, 1, 6).copy()
-        api.apply_plan_numpy(self.plan, v, vp)
+        apply_plan_numpy(self.plan, v, vp)
         return v.reshape(a.shape), vp.reshape(a_pl.shape)
 
     def _build_positions(self):

@@ -157,8 +157,10 @@ int ica_horizontal_limiter_thuburn_f32(ica_ctx *ctx,
  * after start-up (a host model whose pool allocator owns the GPU, a run whose
  * footprint must stay fixed).  The scratch (the Qout copy the halo fill runs on and
  * the pole inflow bounds) is a fixed array in the library's device memory, about
- * 32 MiB on every GPU the library is loaded on.  The first call on a device looks up
- * that array's address; make it before any stream capture.  Grids with
+ * 32.1 MiB.  ica_init looks up its address on the context's device, which loads it
+ * there, so create the context before a pool allocator claims the GPU; every GPU
+ * with a context then holds the array until the process exits.  (Should that lookup
+ * fail, the first call repeats it: make that call before any stream capture.)  Grids with
  * gall*kall*lall > ICA_NOALLOC_MAX_CELLS or kall > ICA_NOALLOC_MAX_KALL get
  * ICA_ERR_ARG.  Nothing needs to start at zero.  All calls share the one array, so
  * calls that overlap on a GPU (other streams, other host threads) race. */

@@ -230,3 +230,26 @@ def step(d, have_sgp, topo, dt, state, fields, geo, nthreads=None):
                    _p(geo["GMTR_p"]), _p(geo["GMTR_p_pl"]), _p(geo["GMTR_t"]), _p(geo["GMTR_t_pl"]),
                    _p(geo["GMTR_a"]), _p(geo["GMTR_a_pl"]), _p(geo["coef_grad"]), _p(geo["coef_grad_pl"]),
                    int(nthreads))
+
+
+class GridTables:
+    """Region topology and composed halo plan from this oracle's restatement of the
+    reference's mod_adm / mod_comm (one emulated rank), in the form the synthetic grid
+    builder takes (icoatmosbenchmark_v1_b200.grid.Grid(tables=...)), so that a grid can be
+    built without the library under test.  The plan is read off COMM_data_transfer itself:
+    every point starts holding its own flat index, and after the transfer a point that
+    holds another index is a destination whose source is that index."""
+
+    def topology_info(self, glevel, rlevel):
+        t = Topo(glevel, rlevel, 1)
+        return t.have_sgp(1), np.array([t.rgn4pl(1), t.rgn4pl(2)], np.int32), None
+
+    def comm_plan(self, glevel, rlevel, pole_fill=False):
+        t = Topo(glevel, rlevel, 1)
+        L, G = t.lall, t.gall
+        var = np.arange(L * G, dtype=np.float64).reshape(1, L, 1, G)
+        var_pl = (L * G + np.arange(12, dtype=np.float64)).reshape(1, 2, 1, 6)
+        (t.comm_var if pole_fill else t.data_transfer)([var], [var_pl])
+        flat = np.concatenate([var.reshape(-1), var_pl.reshape(-1)]).astype(np.int64)
+        dst = np.nonzero(flat != np.arange(flat.size))[0]
+        return dst.astype(np.int32), flat[dst].astype(np.int32)

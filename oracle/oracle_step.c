@@ -206,6 +206,23 @@ static void vertical_column(int kall, int kmin, int kmax, double dt,
   free(ck); free(q); free(qh); free(zero);
 }
 
+/* Scratch kept across calls (process lifetime), so that a step does not map and fault its
+   temporaries again (at glevel 8 they are gigabytes, which made the CPU time mostly page
+   faults).  Slot s holds one buffer that only grows; its contents are not kept meaningful
+   between uses.  orc_step is not reentrant. */
+enum { SCR_FLX, SCR_XC, SCR_CH, SCR_CM, SCR_ZERO, SCR_TRACER0, SCR_NSLOT = SCR_TRACER0 + 4 * 256 };
+static double *scr_ptr[SCR_NSLOT];
+static size_t scr_len[SCR_NSLOT];
+static double *scratch(int slot, size_t n, int zero) {
+  if (scr_len[slot] < n) {
+    free(scr_ptr[slot]);
+    scr_ptr[slot] = malloc(sizeof(double) * n);
+    scr_len[slot] = scr_ptr[slot] ? n : 0;
+  }
+  if (zero && scr_ptr[slot]) memset(scr_ptr[slot], 0, sizeof(double) * n);
+  return scr_ptr[slot];
+}
+
 void orc_step(const orc_dims *d, const int *have_sgp, const orc_topo *topo,
               int ntr, double dt,
               double *rhog, double *rhog_pl, double *rhogq, double *rhogq_pl,
@@ -225,26 +242,42 @@ void orc_step(const orc_dims *d, const int *have_sgp, const orc_topo *topo,
   const int gall_pl = d->gall_pl, lall_pl = d->lall_pl;
   const int gmin = d->gmin, gmax = d->gmax, iall = d->gall_1d;
   const size_t n3 = (size_t)gall * kall * lall, n3p = (size_t)gall_pl * kall * lall_pl;
-  (void)nthreads;
-  double *flx = malloc(sizeof(double) * n3 * 6), *flx_pl = calloc(n3p, sizeof(double));
-  double *xc = malloc(sizeof(double) * n3 * 9), *xc_pl = calloc(n3p * 3, sizeof(double));
-  double *ch = malloc(sizeof(double) * n3 * 6), *ch_pl = calloc(n3p, sizeof(double));
-  double *cm = malloc(sizeof(double) * n3 * 6), *cm_pl = calloc(n3p, sizeof(double));
+  int nthr = nthreads > 0 ? nthreads : 1;
+  if (nthr > 256) nthr = 256;
+  double *flx = scratch(SCR_FLX, n3 * 6, 0), *flx_pl = calloc(n3p, sizeof(double));
+  double *xc = scratch(SCR_XC, n3 * 9, 0), *xc_pl = calloc(n3p * 3, sizeof(double));
+  double *ch = scratch(SCR_CH, n3 * 6, 0), *ch_pl = calloc(n3p, sizeof(double));
+  double *cm = scratch(SCR_CM, n3 * 6, 0), *cm_pl = calloc(n3p, sizeof(double));
+  /* the density correction d of the limiter: zero (read only) */
+  double *zero = scratch(SCR_ZERO, n3, 1), *zero_pl = calloc(n3p, sizeof(double));
+  /* every thread's tracer temporaries, set up before the parallel region */
+  for (int th = 0; th < nthr; ++th) {
+    scratch(SCR_TRACER0 + 4 * th + 0, n3, 0);
+    scratch(SCR_TRACER0 + 4 * th + 1, n3 * 3, 0);
+    scratch(SCR_TRACER0 + 4 * th + 2, n3 * 6, 0);
+    scratch(SCR_TRACER0 + 4 * th + 3, n3 * 2, 0);
+  }
   orc_horizontal_flux(d, have_sgp, flx, flx_pl, xc, xc_pl, rhog, rhog_pl, rhogvx, rhogvx_pl,
                       rhogvy, rhogvy_pl, rhogvz, rhogvz_pl, dt, GRD_xr, GRD_xr_pl,
                       GMTR_p, GMTR_p_pl, GMTR_t, GMTR_t_pl, GMTR_a, GMTR_a_pl);
   orc_courant(d, ch, ch_pl, cm, cm_pl, flx, flx_pl, rhog, rhog_pl);
 
 #ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr)
 #endif
   for (int t = 0; t < ntr; ++t) {
+#ifdef _OPENMP
+    const int th = omp_get_thread_num();
+#else
+    const int th = 0;
+#endif
     double *Q = rhogq + (size_t)t * n3, *Qp = rhogq_pl + (size_t)t * n3p;
-    double *q = malloc(sizeof(double) * n3), *q_pl = calloc(n3p, sizeof(double));
-    double *gr = malloc(sizeof(double) * n3 * 3), *gr_pl = calloc(n3p * 3, sizeof(double));
-    double *qa = malloc(sizeof(double) * n3 * 6), *qa_pl = calloc(n3p, sizeof(double));
-    double *qo = malloc(sizeof(double) * n3 * 2), *qo_pl = calloc(n3p * 2, sizeof(double));
-    double *zero = calloc(n3, sizeof(double)), *zero_pl = calloc(n3p, sizeof(double));
+    /* the thread's region temporaries (every value the tracer reads is written first, as
+       with fresh malloc'd memory); the pole arrays start at zero */
+    double *q = scr_ptr[SCR_TRACER0 + 4 * th + 0], *q_pl = calloc(n3p, sizeof(double));
+    double *gr = scr_ptr[SCR_TRACER0 + 4 * th + 1], *gr_pl = calloc(n3p * 3, sizeof(double));
+    double *qa = scr_ptr[SCR_TRACER0 + 4 * th + 2], *qa_pl = calloc(n3p, sizeof(double));
+    double *qo = scr_ptr[SCR_TRACER0 + 4 * th + 3], *qo_pl = calloc(n3p * 2, sizeof(double));
     for (size_t i = 0; i < n3; ++i) q[i] = Q[i] / rhog[i];
     if (d->have_pl)
       for (size_t i = 0; i < n3p; ++i) q_pl[i] = Qp[i] / rhog_pl[i];
@@ -269,10 +302,14 @@ void orc_step(const orc_dims *d, const int *have_sgp, const orc_topo *topo,
           for (int v = 3; v <= 6; ++v) s = s + P3(flx_pl, v, k, l) * P3(qa_pl, v, k, l);
           P3(Qp, 1, k, l) = P3(Qp, 1, k, l) - s;
         }
-    free(q); free(q_pl); free(gr); free(gr_pl); free(qa); free(qa_pl);
-    free(qo); free(qo_pl); free(zero); free(zero_pl);
+    free(q_pl); free(gr_pl); free(qa_pl); free(qo_pl);
   }
-  /* density after the horizontal sub-step */
+  free(zero_pl);
+  /* density after the horizontal sub-step (columns are independent: threads over regions
+     and levels, each value computed by the same operations as in a serial loop) */
+#ifdef _OPENMP
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads > 0 ? nthreads : 1)
+#endif
   for (int l = 1; l <= lall; ++l)
     for (int k = 1; k <= kall; ++k)
       for (int j = gmin; j <= gmax; ++j)
@@ -293,6 +330,9 @@ void orc_step(const orc_dims *d, const int *have_sgp, const orc_topo *topo,
   orc_dims d1 = {0};
   d1.kall = kall; d1.kmin = d->kmin; d1.kmax = d->kmax;
   d1.gall = 1; d1.lall = 1; d1.have_pl = 0; d1.gall_pl = 6; d1.lall_pl = 2;
+#ifdef _OPENMP
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads > 0 ? nthreads : 1)
+#endif
   for (int l = 1; l <= lall; ++l)
     for (int j = gmin; j <= gmax; ++j)
       for (int i = gmin; i <= gmax; ++i) {
@@ -310,5 +350,5 @@ void orc_step(const orc_dims *d, const int *have_sgp, const orc_topo *topo,
   /* halo fill of the state */
   orc_comm_single(topo, rhog, rhog_pl, kall, 1);
   orc_comm_single(topo, rhogq, rhogq_pl, kall, ntr);
-  free(flx); free(flx_pl); free(xc); free(xc_pl); free(ch); free(ch_pl); free(cm); free(cm_pl);
+  free(flx_pl); free(xc_pl); free(ch_pl); free(cm_pl);
 }

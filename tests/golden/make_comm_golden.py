@@ -75,4 +75,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_comm_golden.py <root of the IcoAtmosBenchmark_v1 checkout>")
+    main(sys.argv[1])

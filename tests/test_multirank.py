@@ -56,7 +56,8 @@ def test_reference_arm_two_ranks(built):
     rank 1 does no work, both exit 0."""
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", str(_port()), "bench.py", "--impl", "reference",
-           "--gpus", "2", "--steps", "1", "--warmup", "0", "--ref-glevel", "3", "--kall", "6", "--ntr", "1"]
+           "--gpus", "2", "--steps", "1", "--warmup", "0", "--glevel", "3", "--kall", "6", "--ref-kall", "4",
+           "--ntr", "1"]
     r = subprocess.run(cmd, cwd=ROOT, env=_env(), capture_output=True, text=True, timeout=540)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
@@ -64,3 +65,15 @@ def test_reference_arm_two_ranks(built):
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+@pytest.mark.timeout(600)
+def test_reference_arm_loads_no_library_code(built):
+    """The reference arm (and bench.py's cpu_baseline leg) builds its grid from the oracle's own
+    topology and halo plan: the process never maps the library under test."""
+    code = ("import bench; bench.cpu_reference(3, 6, 2, 1, 0, 2); "
+            "print('MAPPED', any('libicoadv' in ln for ln in open('/proc/self/maps')))")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=_env(), capture_output=True, text=True,
+                       timeout=540)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "MAPPED False" in r.stdout, r.stdout

@@ -116,3 +116,17 @@ def test_init_without_gpu_reports_error(api):
     rc = api.lib().ica_init(C.byref(d), C.byref(h))
     assert rc == -3 and not h.value  # ICA_ERR_CUDA, no context
     assert api.lib().ica_last_error()
+
+
+@pytest.mark.parametrize("gl,rl", [(3, 0), (4, 1)])
+def test_grid_from_oracle_tables_equals_grid_from_library(built, gl, rl):
+    """The synthetic grid built with the oracle's topology and halo plan (the reference arm's
+    grid) is the grid the library's host tables give, array for array."""
+    from icoatmosbenchmark_v1_b200.grid import Grid
+    from oracle import oracle as O
+    a = Grid(gl, rl, 6)
+    b = Grid(gl, rl, 6, tables=O.GridTables())
+    assert np.array_equal(a.have_sgp, b.have_sgp)
+    assert set(a.arrays) == set(b.arrays)
+    for k in a.arrays:
+        assert np.array_equal(a.arrays[k], b.arrays[k]), k

@@ -87,3 +87,52 @@ def test_noalloc_rejects_grid_beyond_fixed_scratch(built, cuda):
         assert "fixed scratch" in api.lib().ica_last_error().decode()
     finally:
         ctx.close()
+
+
+_FRESH = r"""
+import ctypes as C, sys
+import numpy as np, torch
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
+from cases import case
+from icoatmosbenchmark_v1_b200 import api
+c = case(5, 0, 42)
+ctx = api.IcoAdv(5, 0, 40)
+g = c["geo"]
+ctx.set_geometry(*[g[k] for k in ("GRD_xr", "GRD_xr_pl", "GMTR_p", "GMTR_p_pl", "GMTR_t", "GMTR_t_pl",
+                                  "GMTR_a", "GMTR_a_pl")])
+D = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+ins = [D(c[k]) for k in ("q", "q_pl", "d", "d_pl", "ch", "ch_pl", "cm", "cm_pl")]
+outs = [[D(c["qa"]), D(c["qa_pl"]), D(np.zeros((2,) + c["q"].shape)), D(np.zeros((2, 2, 42, 6)))] for _ in range(2)]
+P = lambda t: C.c_void_p(t.data_ptr())
+L = api.lib()
+# the same kernels through the allocating entry point first: their code is loaded and
+# that entry point's own scratch allocated before the measurement
+assert L.ica_horizontal_limiter_thuburn_dev(ctx.h, P(outs[0][0]), P(outs[0][1]), *map(P, ins), P(outs[0][2]),
+                                            P(outs[0][3]), None, None) == 0
+torch.cuda.synchronize()
+free0 = torch.cuda.mem_get_info()[0]
+assert L.ica_horizontal_limiter_thuburn_noalloc(ctx.h, P(outs[1][0]), P(outs[1][1]), *map(P, ins), P(outs[1][2]),
+                                                P(outs[1][3]), None, None) == 0, L.ica_last_error()
+torch.cuda.synchronize()
+free1 = torch.cuda.mem_get_info()[0]
+for a, b in zip(outs[0], outs[1]):
+    assert torch.equal(a, b)
+print("FREE", free0, free1)
+ctx.close()
+"""
+
+
+def test_noalloc_first_call_in_fresh_process_takes_no_memory(built):
+    """The first noalloc call of a process: its fixed array was loaded by ica_init, so the
+    GPU's free memory is the same before and after that call."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    env = dict(os.environ, ICOADV_NO_BUILD="1")
+    r = subprocess.run([sys.executable, "-c", _FRESH, str(root)], capture_output=True, text=True, env=env,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    line = [x for x in r.stdout.splitlines() if x.startswith("FREE")][-1].split()
+    assert int(line[1]) == int(line[2]), line
