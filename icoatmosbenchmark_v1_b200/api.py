@@ -160,6 +160,27 @@ class IcoAdv:
         self.glevel, self.rlevel, self.vlayer, self.device = glevel, rlevel, vlayer, device
         self._ext = None
 
+    @classmethod
+    def regions(cls, gall_1d, kall, kmin, kmax, lall, have_pl, have_sgp, device=0):
+        """A context for arrays that hold part of a grid, sized as a reference kernel driver
+        holds them (ADM_gall_1d, ADM_kall, ADM_kmin, ADM_kmax, ADM_lall, ADM_have_pl,
+        ADM_have_sgp): ica_init_regions.  It has no region topology (no halo fill)."""
+        self = cls.__new__(cls)
+        self.h = C.c_void_p()
+        sg = np.ascontiguousarray(np.asarray(have_sgp, dtype=np.int32).reshape(-1))
+        if sg.size != lall:
+            raise ValueError("have_sgp needs lall entries")
+        _check("ica_init_regions", lib().ica_init_regions(int(gall_1d), int(kall), int(kmin), int(kmax), int(lall),
+                                                          int(bool(have_pl)), sg.ctypes.data_as(C.POINTER(C.c_int)),
+                                                          int(device), C.byref(self.h)))
+        s = Sizes()
+        _check("ica_get_sizes", lib().ica_get_sizes(self.h, C.byref(s)))
+        self.sizes = s
+        self.glevel = self.rlevel = None
+        self.vlayer, self.device = kall - 2, device
+        self._ext = None
+        return self
+
     def close(self):
         if self.h:
             lib().ica_finalize(self.h)
@@ -359,6 +380,15 @@ class IcoAdv:
     def fast_set_host_chunk(self, tracers):
         """Tracers per chunk of advect_fast_host's overlapped copies (0: by size)."""
         _check("ica_fast_set_host_chunk", lib().ica_fast_set_host_chunk(self.h, int(tracers)))
+
+    def fast_status(self):
+        """Status word of the batched kernels since the last call (0: every bounded wait of
+        the horizontal kernel ended in time); reading it clears it."""
+        f = C.c_int(0)
+        rc = lib().ica_fast_status(self.h, C.byref(f))
+        if rc not in (0, -4):
+            _check("ica_fast_status", rc)
+        return f.value
 
     def fast_timing(self, enable):
         ms = C.c_double()

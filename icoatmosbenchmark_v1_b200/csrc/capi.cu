@@ -45,6 +45,13 @@ void Ctx::release(const char *name) {
   bufs.erase(it);
 }
 
+int Ctx::need_grid(const char *what) const {
+  if (topo) return ICA_OK;
+  set_error(std::string(what) + ": this context was made by ica_init_regions and holds no region topology "
+            "(the halo fill and the composed steps need a whole grid, ica_init)");
+  return ICA_ERR_STATE;
+}
+
 int Ctx::check_launch(const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, what);
@@ -126,12 +133,57 @@ int ica_init(const ica_dims *dims, ica_ctx **out) {
   c->D.kmax = s.kmax;
   c->D.lall = s.lall;
   c->D.have_sgp = c->d_have_sgp;
+  c->D.have_pl = 1;
   // the noalloc limiter's fixed scratch: loaded now, while the context is created, so that
   // its first call takes no device memory (with lazy module loading the array would
   // otherwise be set up inside that call)
   if (noalloc_scratch_address(&c->noalloc_scratch) != ICA_OK) c->noalloc_scratch = nullptr;
   e = cudaGetLastError();
   if (e != cudaSuccess) { delete c; return cuda_fail(e, "ica_init"); }
+  *out = c;
+  return ICA_OK;
+}
+
+int ica_init_regions(int gall_1d, int kall, int kmin, int kmax, int lall, int have_pl, const int *have_sgp,
+                     int device, ica_ctx **out) {
+  if (!out || !have_sgp) return set_error("ica_init_regions: NULL argument"), ICA_ERR_ARG;
+  *out = nullptr;
+  if (gall_1d < 3 || gall_1d > 4098 || kall < 1 || kall > 4096 || kmin < 1 || kmax < kmin || kmax > kall ||
+      lall < 1 || lall > 40960 || (long long)gall_1d * gall_1d * kall * lall >= (1LL << 31))
+    return set_error("ica_init_regions: sizes out of range"), ICA_ERR_ARG;
+  for (int l = 0; l < lall; ++l)
+    if (have_sgp[l] != 0 && have_sgp[l] != 1) return set_error("ica_init_regions: have_sgp must be 0 or 1"), ICA_ERR_ARG;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  int rc = ica_device_check(device);
+  if (rc) return rc;
+  ica_ctx *c = new ica_ctx();
+  c->device = device;
+  ica_sizes &s = c->sz;
+  s.gall_1d = gall_1d;
+  s.gall = gall_1d * gall_1d;
+  s.gmin = 2;
+  s.gmax = gall_1d - 1;
+  s.kall = kall, s.kmin = kmin, s.kmax = kmax;
+  s.lall = lall;
+  s.gall_pl = kGallPl;
+  s.lall_pl = kLallPl;
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
+  if (cudaMalloc(&c->d_have_sgp, sizeof(int) * lall) != cudaSuccess) {
+    delete c;
+    return set_error("cudaMalloc(have_sgp)"), ICA_ERR_NOMEM;
+  }
+  e = cudaMemcpy(c->d_have_sgp, have_sgp, sizeof(int) * lall, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaMemcpy(have_sgp)"); }
+  c->D.gall_1d = s.gall_1d, c->D.gall = s.gall, c->D.gmin = s.gmin, c->D.gmax = s.gmax;
+  c->D.kall = s.kall, c->D.kmin = s.kmin, c->D.kmax = s.kmax;
+  c->D.lall = s.lall;
+  c->D.have_sgp = c->d_have_sgp;
+  c->D.have_pl = have_pl ? 1 : 0;
+  if (noalloc_scratch_address(&c->noalloc_scratch) != ICA_OK) c->noalloc_scratch = nullptr;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { delete c; return cuda_fail(e, "ica_init_regions"); }
   *out = c;
   return ICA_OK;
 }
@@ -243,13 +295,15 @@ int flux_dev(Ctx *c, T *flx_h, T *flx_h_pl, T *GRD_xc, T *GRD_xc_pl, const T *rh
   FluxIn<T> in{rho, rho_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl};
   FluxOut<T> out{flx_h, flx_h_pl, GRD_xc, GRD_xc_pl};
   launch_horizontal_flux<T>(c->D, in, out, c->geo<T>(), dt, c->stream);
-  c->launches += 2;
+  c->launches += c->D.have_pl ? 2 : 1;
   return c->check_launch("horizontal_flux");
 }
 
 template <typename T>
 int comm_dev(Ctx *c, T *var, T *var_pl, int kmax, int vmax, bool pole_fill) {
   if (!var || !var_pl || kmax < 1 || vmax < 1) return set_error("COMM: bad argument"), ICA_ERR_ARG;
+  int rc = c->need_grid(pole_fill ? "COMM_var" : "COMM_data_transfer");
+  if (rc) return rc;
   const Plan &p = c->plan[pole_fill ? 1 : 0];
   launch_gather<T>(c->D, p.n, p.dst, p.src, kmax, vmax, var, var_pl, c->stream);
   c->launches += 1;
@@ -263,10 +317,14 @@ int hlim_dev(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, c
   if (!q_a || !q_a_pl || !q || !q_pl || !d || !d_pl || !ch || !ch_pl || !cmask || !cmask_pl || !Qout_prev ||
       !Qout_prev_pl || ((Qout_post == nullptr) != (Qout_post_pl == nullptr)))
     return set_error("horizontal_limiter_thuburn: bad argument"), ICA_ERR_ARG;
+  if (!Qout_post) {  // the on-GPU Qout halo fill needs the whole grid
+    int rc = c->need_grid("horizontal_limiter_thuburn with Qout_post = NULL");
+    if (rc) return rc;
+  }
   const size_t n2 = (size_t)c->sz.gall * c->sz.kall * c->sz.lall * 2, n2p = (size_t)kGallPl * c->sz.kall * kLallPl * 2;
   LimIn<T> in{q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask_pl};
   launch_hlim_qout<T>(c->D, in, Qout_prev, Qout_prev_pl, scratch_Qin_pl, c->stream);
-  c->launches += 2;
+  c->launches += c->D.have_pl ? 2 : 1;
   const T *Qo = Qout_post, *Qo_pl = Qout_post_pl;
   if (!Qout_post) {  // NICAM: COMM_data_transfer(Qout, Qout_pl) on a copy of the pre-fill Qout
     cudaError_t e = cudaMemcpyAsync(scratch_Qout, Qout_prev, n2 * sizeof(T), cudaMemcpyDeviceToDevice, c->stream);
@@ -280,7 +338,7 @@ int hlim_dev(Ctx *c, T *q_a, T *q_a_pl, const T *q, const T *q_pl, const T *d, c
     Qo_pl = scratch_Qout_pl;
   }
   launch_hlim_apply<T>(c->D, in, q_a, q_a_pl, Qo, Qo_pl, scratch_Qin_pl, c->stream);
-  c->launches += 2;
+  c->launches += c->D.have_pl ? 2 : 1;
   return c->check_launch("horizontal_limiter_thuburn");
 }
 
@@ -307,7 +365,7 @@ int vlim_dev(Ctx *c, T *q_h, T *q_h_pl, const T *q, const T *q_pl, const T *d, c
   if (!q_h || !q_h_pl || !q || !q_pl || !d || !d_pl || !ck || !ck_pl)
     return set_error("vertical_limiter_thuburn: NULL argument"), ICA_ERR_ARG;
   launch_vlim<T>(c->D, q_h, q_h_pl, q, q_pl, d, d_pl, ck, ck_pl, c->stream);
-  c->launches += 2;
+  if (c->D.kmax > c->D.kmin) c->launches += c->D.have_pl ? 2 : 1;
   return c->check_launch("vertical_limiter_thuburn");
 }
 
@@ -524,6 +582,8 @@ int ica_comm_var_dev(ica_ctx *c, double *var, double *var_pl, int kmax, int vmax
 namespace icoadv {
 
 int Ctx::step_ctx(StepCtx &S) {
+  int rc0 = need_grid("advect_step");
+  if (rc0) return rc0;
   if (!geo_set || !stepgeo_set) return set_error("advect_step: geometry not registered"), ICA_ERR_STATE;
   const size_t n3 = (size_t)sz.gall * sz.kall * sz.lall, n3p = (size_t)kGallPl * sz.kall * kLallPl;
   S.D = D;
@@ -940,6 +1000,8 @@ int Ctx::build_fast_tables() {
 
 int Ctx::fast_inst(FastInst &I, int ntr, double dt, bool f64) {
   I = FastInst{};
+  int rc0 = need_grid("advect_fast");
+  if (rc0) return rc0;
   if (!geo_set || !stepgeo_set) return set_error("advect_fast: geometry not registered"), ICA_ERR_STATE;
   if (sz.kall < 4 || sz.kall > 128) return set_error("advect_fast: kall must be in [4, 128]"), ICA_ERR_ARG;
   if ((long long)sz.lall * (sz.kall - 2) * sz.gall >= (1LL << 31))  // 32-bit cell-level indices in the kernels
@@ -1002,9 +1064,15 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt, bool f64) {
   }
   const size_t n3 = (size_t)sz.lall * sz.kall * sz.gall;
   I.Fg = (double *)buf("fast_Fg", 3 * n3 * sizeof(double));
-  if (f64) I.Dg64 = (double *)buf("fast_Dg64", 9 * n3 * sizeof(double));
-  else I.Dg = (float *)buf("fast_Dg", 9 * n3 * sizeof(float));
-  if (!I.Fg || (f64 ? !I.Dg64 : !I.Dg)) return set_error("cudaMalloc(fast face fluxes)"), ICA_ERR_NOMEM;
+  if (f64) I.dupc64 = (double4 *)buf("fast_dupc64", 3 * n3 * sizeof(double4));
+  else I.dupc = (float4 *)buf("fast_dupc", 3 * n3 * sizeof(float4));
+  if (!I.Fg || (f64 ? !I.dupc64 : !I.dupc)) return set_error("cudaMalloc(fast face fluxes)"), ICA_ERR_NOMEM;
+  if (!fast.err) {  // the device status word, zero until a bounded wait gives up
+    fast.err = (int *)buf("fast_err", sizeof(int));
+    if (!fast.err || cudaMemsetAsync(fast.err, 0, sizeof(int), stream) != cudaSuccess)
+      return set_error("cudaMalloc(fast status word)"), ICA_ERR_NOMEM;
+  }
+  I.err = fast.err;
   I.work_next = (unsigned long long *)buf("fast_work_next", sizeof(unsigned long long));
   if (!I.work_next) return set_error("cudaMalloc(fast work counter)"), ICA_ERR_NOMEM;
   return ICA_OK;
@@ -1042,6 +1110,19 @@ int ica_boundary_tables(int glevel, int rlevel, int *nb, int *bsrc, int *blist, 
   if (blist) std::memcpy(blist, bl.data(), bl.size() * sizeof(int));
   if (pole_ring) std::memcpy(pole_ring, ring.data(), ring.size() * sizeof(int));
   return ICA_OK;
+}
+
+int ica_fast_status(ica_ctx *c, int *flags) {
+  CTX_OK(c);
+  if (!flags) return set_error("ica_fast_status: NULL argument"), ICA_ERR_ARG;
+  *flags = 0;
+  if (!c->fast.err) return ICA_OK;
+  cudaSetDevice(c->device);
+  cudaError_t e = cudaMemcpyAsync(flags, c->fast.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->fast.err, 0, sizeof(int), c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_fast_status");
+  return *flags ? ICA_ERR_TIMEOUT : ICA_OK;
 }
 
 int ica_fast_set_host_chunk(ica_ctx *c, int tracers) {

@@ -37,6 +37,7 @@ struct FastState {  // fused path: boundary tables, tile shape, kernel timing
   bool off64_ready = false;
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+  int *err = nullptr;  // device status word of the batched kernels (a buffer of the context)
 };
 
 struct FastInst;
@@ -67,6 +68,9 @@ struct Ctx {
   long long launches = 0;
 
   ~Ctx();
+  // contexts made by ica_init_regions hold part of a grid (the arrays a reference driver
+  // holds) and no region topology: what needs the whole grid returns ICA_ERR_STATE
+  int need_grid(const char *what) const;
   void *buf(const char *name, size_t bytes);
   void release(const char *name);
   int check_launch(const char *what);

@@ -3,6 +3,7 @@
 // (singular point, index clamps, unused faces), usable on global or shared data.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -46,11 +47,21 @@ struct FastInst {
   double *sval64;  // the same in FP64 (FP64 variant)
   double *bbuf;  // (ntr, K, nb, 5): grad x, y, z, Qout min, Qout max
   double *Fg;    // (3, lall, K, gall): face flux 0.5 (rhov . HN) of the 3 faces of each owner, per step
-  float *Dg;     // (9, lall, K, gall): face a, component c at a*3+c: -rhov rr dt / 2 (GRD_xc - GRD_xr)
+  // (3, lall, K, gall) per owner face a: x, y, z = GRD_xc - GRD_x of the face's upwind cell (the
+  // remap displacement that cell applies to its gradient); w = the owner-side upwind mask of
+  // horizontal_limiter_thuburn (1: the neighbour is upwind, 0: the owner is)
+  float4 *dupc;
   float4 *vco;   // (lall, K, gall): ck(k,1), ck(k,2), 1/rhog, rhogw(k) after the horizontal sub-step
   double4 *vco64;  // the same in FP64 (FP64 variant)
-  double *Dg64;    // centroid displacements in FP64 (FP64 variant), layout of Dg
+  double4 *dupc64;  // dupc in FP64 (FP64 variant)
   unsigned long long *work_next;  // work-item counter of the persistent horizontal kernel
+  int *err;  // device status word: bit 0 = a bounded wait of the horizontal kernel gave up
+};
+
+// TMA descriptors of one instance's tile windows (built on the host per step, since the state
+// buffers alternate): rhogq_in as (i, j, l*K + k, tracer) FP64 and rhog_in as (i, j, l*K + k).
+struct TileMaps {
+  CUtensorMap q, rho;
 };
 
 // Up to kMaxInst grid instances advanced by the same launches (batches of uneven grid
@@ -59,6 +70,9 @@ constexpr int kMaxInst = 4;
 struct MultiInst {
   int n;
   FastInst inst[kMaxInst];
+};
+struct MultiMaps {
+  TileMaps m[kMaxInst];
 };
 
 // Instance of flat work item w, given the number of work items cnt(inst) of each
@@ -95,6 +109,7 @@ __device__ __forceinline__ double fld_pl(const FastInst &I, int var, size_t o) {
 template <typename R> struct Arith;
 template <> struct Arith<float> {
   using V2 = float2;
+  using V4 = float4;
   static constexpr float BIG = FLT_MAX, RR_EPS = FLT_EPSILON;
   static __device__ __forceinline__ float mn(float a, float b) { return fminf(a, b); }
   static __device__ __forceinline__ float mx(float a, float b) { return fmaxf(a, b); }
@@ -103,6 +118,7 @@ template <> struct Arith<float> {
 };
 template <> struct Arith<double> {
   using V2 = double2;
+  using V4 = double4;
   static constexpr double BIG = DBL_MAX, RR_EPS = DBL_EPSILON;
   static __device__ __forceinline__ double mn(double a, double b) { return (b < a) ? b : a; }
   static __device__ __forceinline__ double mx(double a, double b) { return (b > a) ? b : a; }

@@ -357,11 +357,24 @@ __global__ void k_fast_offsets(FastInst I, T *off) {
   }
 }
 
-// Face fluxes and centroid displacements of every owner cell and level, once per step
-// (dyn_horiz_adv_flux/src/mod_src_tracer.f90:141-309): FP32 triangle values and faces
-// between interior cells, the FP64 value of k_fast_seam on seam faces, zero where the
-// reference has no face.  One thread per (owner cell, level); every tile that needs a
-// face reads this one value, so its two cells see the same flux.
+// Threshold of the upwind masks (0.5 - sign(0.5, ch - EPS)) and of the zero-outflow guards
+// (zerosw) in either arithmetic: the FP64 EPS, also in FP32, not epsilon(1.0).  These are switches, not
+// roundings: with FP32's own EPS a face whose Courant number lies in (2.2e-16, 1.2e-7) is
+// taken from the other side than in FP64, which moves its 4-point bounds into or out of the
+// cell's qnext; at a slotted-cylinder edge (glevel 7, kall 96) that gave 9e-4 relative error
+// against the FP64 oracle in 10 cells.  With the FP64 threshold the same run is at 1.6e-7.
+// (The standalone *_f32 kernel entry points keep the reference's RP = SP semantics.)
+template <typename R>
+__device__ __forceinline__ R eps_thr() { return (R)DBL_EPSILON; }
+
+// Face fluxes of every owner cell and level, once per step (dyn_horiz_adv_flux/src/
+// mod_src_tracer.f90:141-309): FP32 triangle values and faces between interior cells, the
+// FP64 value of k_fast_seam on seam faces, zero where the reference has no face.  With each
+// face the owner-side upwind mask (cmask of horizontal_limiter_thuburn, from the owner's
+// Courant number) and the remap displacement of the upwind cell: GRD_xc - GRD_x of that
+// cell, i.e. the fixed per-face offset GRD_xr - GRD_x of its side plus the centroid
+// displacement -rhov rr dt / 2.  One thread per (owner cell, level); every tile that needs a
+// face reads these values, so the face's two cells see the same flux and mask.
 template <typename R>
 __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
   using A = Arith<R>;
@@ -433,26 +446,28 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
       F[a] = I.sflux[(size_t)k * I.ns + sid];
     }
   }
+  // the owner's Courant number of each face and its upwind mask, in the form the tile kernel
+  // used to form them (FP32 flux, rarea and 1/rho of the owner), and the upwind side's offset
+  const R ra = (R)rarea(I, l, i, j), rinv = (R)(1.0 / I.rho_in[o]);
+  const R EPSf = eps_thr<R>();
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     I.Fg[(size_t)a * n3 + o] = F[a];
+    const R chown = ((R)F[a] * ra * dtf) * rinv;
+    const bool cm = (R(0.5) - A::sgn(R(0.5), chown - EPSf)) != R(0.0);
+    R v[3] = {R(0.0), R(0.0), R(0.0)};
+    if (inner[a]) {
+      const size_t ob = ((size_t)l * 18 + a * 6 + (cm ? 3 : 0)) * I.gall + c;
 #pragma unroll
-    for (int x = 0; x < 3; ++x) {
-      if (sizeof(R) == 8) I.Dg64[(size_t)(a * 3 + x) * n3 + o] = d[a][x];
-      else I.Dg[(size_t)(a * 3 + x) * n3 + o] = (float)d[a][x];
+      for (int x = 0; x < 3; ++x)
+        v[x] = (sizeof(R) == 8 ? (R)I.off64[ob + (size_t)x * I.gall] : (R)I.off32[ob + (size_t)x * I.gall]) + d[a][x];
     }
+    const R w = cm ? R(1.0) : R(0.0);
+    if (sizeof(R) == 8) I.dupc64[(size_t)a * n3 + o] = make_double4(v[0], v[1], v[2], w);
+    else I.dupc[(size_t)a * n3 + o] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)w);
   }
 }
 
-// Threshold of the upwind masks (0.5 - sign(0.5, ch - EPS)) and of the zero-outflow guards
-// (zerosw) in either arithmetic: the FP64 EPS, also in FP32, not epsilon(1.0).  These are switches, not
-// roundings: with FP32's own EPS a face whose Courant number lies in (2.2e-16, 1.2e-7) is
-// taken from the other side than in FP64, which moves its 4-point bounds into or out of the
-// cell's qnext; at a slotted-cylinder edge (glevel 7, kall 96) that gave 9e-4 relative error
-// against the FP64 oracle in 10 cells.  With the FP64 threshold the same run is at 1.6e-7.
-// (The standalone *_f32 kernel entry points keep the reference's RP = SP semantics.)
-template <typename R>
-__device__ __forceinline__ R eps_thr() { return (R)DBL_EPSILON; }
 
 // ---- vertical Thuburn limiter (dyn_vert_adv_limiter/src/mod_src_tracer.f90:107-186), d = 0, FP32:
 // the tracer-independent part of a level (upwind flags, Courant sums) and the per-tracer bounds
@@ -491,161 +506,192 @@ __device__ __forceinline__ void vlim_qout(const VLim<R> &v, R qm, R qk, R qp, R 
 // ---- horizontal sub-step -----------------------------------------------------------
 // One CTA per (region tile, level), all tracers in batches of TB.  Local frame: cell (i,j)
 // of the region -> (x,y) = (i - i0, j - j0); the tile is x in [0,TX), y in [0,TY); the ring
-// (one thread per cell) x in [-1,TX], y in [-1,TY]; the window of shared per-cell data
-// x in [-3,TX+1], y in [-3,TY+1].
+// (one thread per cell) x in [-1,TX], y in [-1,TY]; the window of rhogq and rhog that the
+// ring's stencils read, x in [-3,TX+2], y in [-2,TY+1].  The window's first column i0-4 is
+// even for even TX (i0 = gmin + TX*n), so a TMA copy of its FP64 rows starts on a 16-byte
+// boundary, as the tensor copy requires.
 template <int TX, int TY>
 struct TileGeo {
+  static_assert(TX % 2 == 0, "the window's first column must be even");
   static constexpr int RW = TX + 2, RH = TY + 2, NR = RW * RH;  // ring cells
   static constexpr int NT = (NR + 31) / 32 * 32;                // threads (whole warps)
-  static constexpr int WW = TX + 5, WH = TY + 5, NW = WW * WH;
+  static constexpr int WW = TX + 6, WH = TY + 4, NW = WW * WH;  // window
 };
 
 template <int TX, int TY, int TB, typename R>
 struct TileSmem {
   using V2 = typename Arith<R>::V2;
+  using V4 = typename Arith<R>::V4;
   static constexpr int NT = TileGeo<TX, TY>::NT, NW = TileGeo<TX, TY>::NW;
-  double rinv[NW];  // 1 / rho
-  double F[3][NW];  // face flux 0.5 (rhov . HN) by owner, from k_fast_faces
-  double stage[2][TB][NW];  // rhogq of the window, FP64, two batches in flight (cp.async)
+  alignas(128) double stage[2][TB][NW];  // rhogq of the window, FP64, [tracer][y][x]: two batches in flight
+  alignas(128) double rho[NW];           // rhog of the window
+  double rinv[NW];                       // 1 / rhog (0 outside the array)
   // tracer pairs (x: tracer 2p, y: tracer 2p+1): one 8-byte access serves both, and a
   // half-warp (one ring row) touches consecutive slots, so no padding is needed for banks
   V2 q2[TB / 2][NW];
-  struct {
-    V2 gq[TB / 2][5][NT];  // grad x, y, z, Qout min, Qout max of ring cells
-    V2 qa[TB / 2][3][NT];  // limited face values of the faces owned by ring cells
-  } t;
+  V2 qa[TB / 2][3][NT];  // limited values of the faces owned by ring cells
+  V4 dup[3][NT];         // owner faces: upwind cell's remap displacement, owner-side mask (k_fast_faces)
+  double flx[6][NT];     // flx_h (FP64) of the 6 faces of a tile cell
+  unsigned long long mbar[2];  // one per stage buffer: its TMA copies have landed
 };
 
-// one work item (tile, level) of instance I.  I is taken by value and the body inlined once
-// per call site, so every field of I stays a constant-bank operand (a reference to the
-// parameter measured 9% more instructions: fields reloaded around the global stores).
+// ---- TMA and mbarrier helpers (this GPU's memory only; no cluster multicast)
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for the phase of parity `parity` of barrier b, for 2 s at most (false: gave up).
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity) {
+  if (mbar_try(b, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try(b, parity))
+    if (global_ns() - t0 > 2000000000ull) return false;
+  return true;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *m, int c0, int c1, int c2,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_u32(dst)),
+      "l"((unsigned long long)m), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];\n" ::"r"(smem_u32(dst)),
+      "l"((unsigned long long)m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
 template <int TX, int TY, int TB, typename R>
-__device__ __forceinline__ void horiz_item(const FastInst I, const int tile, const int k,
-                                           TileSmem<TX, TY, TB, R> &s) {
+__device__ __forceinline__ void tile_smem_init(TileSmem<TX, TY, TB, R> &s) {
+  if (threadIdx.x == 0) {
+    mbar_init(&s.mbar[0], 1);
+    mbar_init(&s.mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// one work item (tile, level) of instance I; `phase` holds the parity each stage barrier waits
+// for next (bit b: barrier b).  Returns false if a wait for a TMA copy gave up (the error word
+// is set; the caller stops).  I is taken by value and the body inlined once per call site, so
+// every field of I stays a constant-bank operand.
+template <int TX, int TY, int TB, typename R>
+__device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, const int tile, const int k,
+                                           TileSmem<TX, TY, TB, R> &s, unsigned &phase) {
   using A = Arith<R>;
   using V2 = typename A::V2;
+  using V4 = typename A::V4;
   using Gm = TileGeo<TX, TY>;
   constexpr int RW = Gm::RW, NR = Gm::NR, NT = Gm::NT, WW = Gm::WW, NW = Gm::NW;
+  constexpr int TP = TB / 2;  // tracer pairs of a batch: one V2 holds tracers 2p and 2p+1
+  constexpr int NSLOT = (NW + NT - 1) / NT;
+  constexpr unsigned QBYTES = (unsigned)(TB * NW * sizeof(double)), RBYTES = (unsigned)(NW * sizeof(double));
   const int tiles_per_rgn = I.ntx * I.nty;
   const int l = tile / tiles_per_rgn;
   const int tr = tile % tiles_per_rgn;
   const int i0 = I.gmin + (tr % I.ntx) * TX, j0 = I.gmin + (tr / I.ntx) * TY;
   const int tid = threadIdx.x;
   const int G = I.G, K = I.K, ntr = I.ntr;
+  const int nbat = (ntr + TB - 1) / TB;
   const bool sgp = I.have_sgp[l] != 0;
-  const size_t slab = (size_t)I.gall, lk = (size_t)K * I.gall, tstride = (size_t)I.lall * K * I.gall;
-  const size_t base = (size_t)l * lk + (size_t)k * slab;
+  const size_t slab = (size_t)I.gall, n3 = (size_t)I.lall * K * I.gall;
+  const size_t base = ((size_t)l * K + k) * slab;
   const double dt = I.dt;
   const R dtf = (R)dt;
   const R BIGf = A::BIG, EPSf = eps_thr<R>();
+  // TMA coordinates of the window (0-based column, row, slab l*K + k): x = -3, y = -2
+  const int wx = i0 - 4, wy = j0 - 3, wsl = l * K + k;
+  bool ok = true;
+  if (tid == 0) {  // rhog and the first two batches' rhogq stream in during the set-up below
+    mbar_expect_tx(&s.mbar[0], QBYTES + RBYTES);
+    tma_load_3d(&s.rho[0], &T->rho, wx, wy, wsl, &s.mbar[0]);
+    tma_load_4d(&s.stage[0][0][0], &T->q, wx, wy, wsl, 0, &s.mbar[0]);
+    if (nbat > 1) {
+      mbar_expect_tx(&s.mbar[1], QBYTES);
+      tma_load_4d(&s.stage[1][0][0], &T->q, wx, wy, wsl, TB, &s.mbar[1]);
+    }
+  }
 
   // this thread's ring cell
   const bool ring = tid < NR;
   const int x = ring ? tid % RW - 1 : TX + 8, y = ring ? tid / RW - 1 : TY + 8;
   const int ci = i0 + x, cj = j0 + y;
-  const int ec = ring ? (y + 3) * WW + (x + 3) : 0;   // window slot of the cell
+  const int ew = ring ? (y + 2) * WW + (x + 3) : 0;  // window slot of the cell
   const bool in_arr = ring && ci >= 1 && ci <= G && cj >= 1 && cj <= G;
   auto interior = [&](int i, int j) { return i >= I.gmin && i <= I.gmax && j >= I.gmin && j <= I.gmax; };
+  auto in_tile = [&](int a, int b) { return a >= 0 && a < TX && b >= 0 && b < TY; };
   const bool c_int = in_arr && interior(ci, cj);
   const int bs = in_arr ? I.bsrc[(size_t)l * I.gall + (cj - 1) * G + (ci - 1)] : -3;
-  const bool tile_cell = c_int && bs == -1;                          // gradient / Qout formed in the tile
-  const bool active = x >= 0 && x < TX && y >= 0 && y < TY && c_int;  // updated by this thread
-  const bool owner = x < TX && y < TY && in_arr;                     // face values of its 3 faces
+  const bool tile_cell = c_int && bs == -1;  // gradient / Qout formed in the tile
+  const bool active = c_int && in_tile(x, y);  // updated by this thread
   const size_t ccell = in_arr ? (size_t)(cj - 1) * G + (ci - 1) : 0;
-  const double ra64 = c_int ? rarea(I, l, ci, cj) : 1.0;
-  const R ra32 = (R)ra64;
+  const size_t oc = base + ccell;
 
-  // the window slots of this thread (e = tid + r*NT): global offset in the level
-  constexpr int NSLOT = (NW + NT - 1) / NT;
-  constexpr int TP = TB / 2;  // tracer pairs of a batch: one V2 holds tracers 2p and 2p+1
-  int sofs[NSLOT];
-  bool sok[NSLOT];
+  // ---- set-up, tracer-independent: every global load first (one round trip together)
+  double Fo[3] = {0.0, 0.0, 0.0}, Fn[3] = {0.0, 0.0, 0.0};  // flux of faces 1-3 (own), 4-6 (owners')
+  V4 d4[3];
+  R cmn[3] = {R(0.0), R(0.0), R(0.0)};  // owner-side masks of faces 4-6
+  const V4 *dupc = (const V4 *)(sizeof(R) == 8 ? (const void *)I.dupc64 : (const void *)I.dupc);
 #pragma unroll
-  for (int r = 0; r < NSLOT; ++r) {
-    const int e = tid + r * NT;
-    const int lx = e % WW, ly = e / WW;
-    const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-    sok[r] = e < NW && lx >= 1 && ly >= 1 && i >= 1 && i <= G && j >= 1 && j <= G;
-    sofs[r] = sok[r] ? (j - 1) * G + (i - 1) : 0;
+  for (int a = 0; a < 3; ++a) d4[a] = V4{R(0.0), R(0.0), R(0.0), R(0.0)};
+  double rho_c = 1.0, ra64 = 1.0, wk = 0.0, wk1 = 0.0;
+  if (in_arr) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) Fo[a] = I.Fg[(size_t)a * n3 + oc], d4[a] = dupc[(size_t)a * n3 + oc];
   }
-  // rhogq window of the batch starting at tracer tb into stage[buf], asynchronously
-  auto issue = [&](int tb, int buf) {
-    const int nb = min(TB, ntr - tb);
-#pragma unroll
-    for (int tt = 0; tt < TB; ++tt) {
-      if (tt >= nb) break;
-      const double *src = I.Q_in + (size_t)(tb + tt) * tstride + base;
-#pragma unroll
-      for (int r = 0; r < NSLOT; ++r)
-        if (sok[r]) {
-          const unsigned dst = (unsigned)__cvta_generic_to_shared(&s.stage[buf][tt][tid + r * NT]);
-          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src + sofs[r]));
-        }
-    }
-    asm volatile("cp.async.commit_group;\n" ::);
-  };
-  // the first two batches' windows stream in during the tracer-independent part
-  issue(0, 0);
-  if (TB < ntr) issue(TB, 1);
-  // that part's per-cell inputs from global memory, in flight together: gradient
-  // coefficients, remap offsets of both sides of the owner's faces, centroid displacements,
-  // rho and rhogw of the tile cell
-  R cgr[21], offr[18], dgr[9];
-  const bool own_int = owner && c_int;
-#pragma unroll
-  for (int n = 0; n < 21; ++n) cgr[n] = tile_cell ? (sizeof(R) == 8 ? (R)I.cg[((size_t)l * 21 + n) * I.gall + ccell]
-                                             : (R)I.cg32[((size_t)l * 21 + n) * I.gall + ccell])
-                            : R(0);
-#pragma unroll
-  for (int n = 0; n < 18; ++n)
-    offr[n] = !own_int ? R(0)
-              : (sizeof(R) == 8) ? (R)I.off64[((size_t)l * 18 + n) * I.gall + ccell]
-                                 : (R)I.off32[((size_t)l * 18 + n) * I.gall + ccell];
-#pragma unroll
-  for (int n = 0; n < 9; ++n)
-    dgr[n] = !own_int ? R(0)
-             : (sizeof(R) == 8) ? (R)I.Dg64[(size_t)n * tstride + base + ccell]
-                                : (R)I.Dg[(size_t)n * tstride + base + ccell];
-  double rho_c = 0.0, wk = 0.0, wk1 = 0.0;
-  if (active) rho_c = I.rho_in[base + ccell], wk = fld(I, 3, base + ccell), wk1 = fld(I, 3, base + slab + ccell);
-  // ---- (0a) 1/rho and the face fluxes (k_fast_faces) of this level in the window
-  for (int e = tid; e < NW; e += NT) {
-    const int lx = e % WW, ly = e / WW;  // local slot: x = lx - 3
-    const int i = i0 - 3 + lx, j = j0 - 3 + ly;
-    const bool in = i >= 1 && i <= G && j >= 1 && j <= G;
-    const size_t o = base + (size_t)(j - 1) * G + (i - 1);
-    s.rinv[e] = in ? 1.0 / I.rho_in[o] : 1.0;
-    // owners x, y in [-2, T] are read by the Courant numbers of the ring cells
-    const bool own = in && lx >= 1 && ly >= 1 && lx <= TX + 3 && ly <= TY + 3;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) s.F[a][e] = own ? I.Fg[(size_t)a * tstride + o] : 0.0;
+  if (c_int) {  // owners of faces 4, 5, 6: (i-1, j) face AI, (i-1, j-1) face AIJ, (i, j-1) face AJ
+    Fn[0] = I.Fg[oc - 1], cmn[0] = dupc[oc - 1].w;
+    Fn[1] = I.Fg[n3 + oc - G - 1], cmn[1] = dupc[n3 + oc - G - 1].w;
+    Fn[2] = I.Fg[2 * n3 + oc - G], cmn[2] = dupc[2 * n3 + oc - G].w;
+    rho_c = I.rho_in[oc], ra64 = rarea(I, l, ci, cj);
   }
-  __syncthreads();
-  // ---- (0d) per ring cell: Courant numbers, masks, outflow sums, gradient coefficients;
-  // per owner: upwind offsets; per tile cell: flx_h (FP64), rho after the horizontal
-  // sub-step and the tracer-independent inputs of the vertical sub-step
+  if (active) wk = fld(I, 3, oc), wk1 = fld(I, 3, oc + slab);
+  R cgr[21];
+#pragma unroll
+  for (int n = 0; n < 21; ++n)
+    cgr[n] = tile_cell ? (sizeof(R) == 8 ? (R)I.cg[((size_t)l * 21 + n) * I.gall + ccell]
+                                         : (R)I.cg32[((size_t)l * 21 + n) * I.gall + ccell])
+                       : R(0);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) s.dup[a][tid] = d4[a];
+  // Courant numbers, upwind sides and the Thuburn outflow sums of the cell
+  const R ra32 = (R)ra64;
   R chm[7], omc = R(0.0), rden = R(0.0), zsw = R(1.0);
-  unsigned inmask = 0, cmown = 0;
-  R dup[3][3];
-  const int nbe[7] = {0, ec, ec, ec, ec - 1, ec - WW - 1, ec - WW};  // owner slot of face m
+  unsigned upm = 0;  // bit m: this cell is the upwind cell of its face m (its outflow faces)
 #pragma unroll
   for (int m = 0; m < 7; ++m) chm[m] = R(0.0);
-  if (tile_cell) {
-    const R rcinv = (R)s.rinv[ec];  // Courant numbers by the reciprocal of rho (one division per cell)
+  if (c_int) {
+    const R rcinv = (R)(1.0 / rho_c);  // by the reciprocal of rho (one division per cell)
     R ch[7];
 #pragma unroll
     for (int m = 1; m <= 6; ++m) {
-      const R Fm = (R)s.F[(m - 1) % 3][nbe[m]];
+      const R Fm = (R)(m <= 3 ? Fo[m - 1] : Fn[m - 4]);
       ch[m] = ((m <= 3 ? Fm : -Fm) * ra32 * dtf) * rcinv;
       chm[m] = A::mn(ch[m], R(0.0));
-      R chown = ch[m];
-      if (m >= 4) {  // the owner's own Courant number of this face, as the owner forms it
-        const int oi = (m == 6) ? ci : ci - 1, oj = (m == 4) ? cj : cj - 1;
-        chown = (Fm * (R)rarea(I, l, oi, oj) * dtf) * (R)s.rinv[nbe[m]];
-      }
-      const R cm = R(0.5) - A::sgn(R(0.5), chown - EPSf);
-      const bool in = (m <= 3) ? (cm != R(0.0)) : (cm == R(0.0));
-      inmask |= in ? (1u << m) : 0u;
+      // the owner's mask decides the side: owner upwind where it is 0 (faces 1-3 are this
+      // cell's own), the neighbour where it is 1 (faces 4-6, whose owner is the neighbour)
+      const bool up = (m <= 3) ? (d4[m - 1].w == R(0.0)) : (cmn[m - 4] != R(0.0));
+      upm |= up ? (1u << m) : 0u;
     }
     const R Cin = chm[1] + chm[2] + chm[3] + chm[4] + chm[5] + chm[6];
     const R Cout =
@@ -654,163 +700,167 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
     omc = R(1.0) - Cin - Cout;
     rden = (R(1.0) - zsw) / (Cout + zsw);
   }
+  // the faces this thread fills in qa: its outflow faces between two interior cells (seam faces
+  // come from k_fast_seam) that touch a cell of the tile; as owner, its faces 1-3 that touch a
+  // tile cell and are seam faces (the seam value) or absent (zero)
+  constexpr int DX[7] = {0, 1, 1, 0, -1, -1, 0}, DY[7] = {0, 0, 1, 1, 0, -1, -1};
+  unsigned dom = 0, seam_own = 0, zero_own = 0;
+  if (c_int) {
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    dup[a][0] = dup[a][1] = dup[a][2] = R(0.0);
-    if (own_int) {
-      const R Fa = (R)s.F[a][ec];
-      const R chown = (Fa * ra32 * dtf) * (R)s.rinv[ec];
-      const bool cm = (R(0.5) - A::sgn(R(0.5), chown - EPSf)) != R(0.0);
-      cmown |= cm ? (1u << a) : 0u;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) dup[a][c] = (cm ? offr[a * 6 + 3 + c] : offr[a * 6 + c]) + dgr[a * 3 + c];
+    for (int m = 1; m <= 6; ++m) {
+      const bool need = in_tile(x, y) || in_tile(x + DX[m], y + DY[m]);
+      if (need && interior(ci + DX[m], cj + DY[m]) && ((upm >> m) & 1u)) dom |= 1u << m;
     }
   }
-  double flx[7];
+  if (in_arr && x < TX && y < TY) {
 #pragma unroll
-  for (int m = 0; m < 7; ++m) flx[m] = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      const int nx = x + DX[a + 1], ny = y + DY[a + 1];
+      const bool need = (active) || (in_tile(nx, ny) && interior(ci + DX[a + 1], cj + DY[a + 1]));
+      if (!need) continue;
+      if (!face_exists(I, ci, cj, a + 1)) zero_own |= 1u << a;
+      else if (!c_int || !interior(ci + DX[a + 1], cj + DY[a + 1])) seam_own |= 1u << a;
+    }
+  }
+  // flx_h of the tile cells (FP64), rhog after the horizontal sub-step and the
+  // tracer-independent inputs of the vertical sub-step
   if (active) {
     double sum = 0.0;
 #pragma unroll
     for (int m = 1; m <= 6; ++m) {
-      flx[m] = cell_flx(I, l, ci, cj, m, sgp, s.F[(m - 1) % 3][nbe[m]], ra64);
-      sum = (m == 1) ? flx[m] : sum + flx[m];
+      const double f = cell_flx(I, l, ci, cj, m, sgp, m <= 3 ? Fo[m - 1] : Fn[m - 4], ra64);
+      s.flx[m - 1][tid] = f;
+      sum = (m == 1) ? f : sum + f;
     }
     const double rho_h = rho_c - sum;
-    I.rho_out[base + ccell] = rho_h;
+    I.rho_out[oc] = rho_h;
     const double rhinv = 1.0 / rho_h;
     if (sizeof(R) == 8)
-      I.vco64[base + ccell] = make_double4(-wk * dt * I.rdgz[k] * rhinv, wk1 * dt * I.rdgz[k] * rhinv, rhinv, wk);
+      I.vco64[oc] = make_double4(-wk * dt * I.rdgz[k] * rhinv, wk1 * dt * I.rdgz[k] * rhinv, rhinv, wk);
     else
-      I.vco[base + ccell] = make_float4((float)(-wk * dt * I.rdgz[k] * rhinv), (float)(wk1 * dt * I.rdgz[k] * rhinv),
-                                        (float)rhinv, (float)wk);
+      I.vco[oc] = make_float4((float)(-wk * dt * I.rdgz[k] * rhinv), (float)(wk1 * dt * I.rdgz[k] * rhinv),
+                              (float)rhinv, (float)wk);
   }
 
-  // q of the batch starting at tracer tb from stage[buf] (window x, y in [-2, T+1]), by pairs
-  auto load_q = [&](int tb, int buf) {
-    const int nb = min(TB, ntr - tb);
+  // q of the batch in stage[buf] (window slots of this thread), by tracer pairs
+  auto load_q = [&](int buf) {
 #pragma unroll
-    for (int pp = 0; pp < TP; ++pp)
+    for (int r = 0; r < NSLOT; ++r) {
+      const int e = tid + r * NT;
+      if (e < NW) {
+        const double ri = s.rinv[e];
 #pragma unroll
-      for (int r = 0; r < NSLOT; ++r) {
-        const int e = tid + r * NT;
-        if (e < NW) {
-          V2 v = A::v2(R(0.0), R(0.0));
-          if (sok[r]) {
-            const double ri = s.rinv[e];
-            if (2 * pp < nb) v.x = (R)(s.stage[buf][2 * pp][e] * ri);
-            if (2 * pp + 1 < nb) v.y = (R)(s.stage[buf][2 * pp + 1][e] * ri);
-          }
-          s.q2[pp][e] = v;
-        }
+        for (int pp = 0; pp < TP; ++pp)
+          s.q2[pp][e] = A::v2((R)(s.stage[buf][2 * pp][e] * ri), (R)(s.stage[buf][2 * pp + 1][e] * ri));
       }
+    }
   };
+  // ---- 1/rho of the window, then q of the first batch (rho and batch 0 share barrier 0)
+  ok = mbar_wait(&s.mbar[0], phase & 1u) && ok;
+  phase ^= 1u;
+#pragma unroll
+  for (int r = 0; r < NSLOT; ++r) {
+    const int e = tid + r * NT;
+    if (e < NW) {
+      const int i = wx + 1 + e % WW, j = wy + 1 + e / WW;  // 1-based cell of the slot
+      s.rinv[e] = (i >= 1 && i <= G && j >= 1 && j <= G) ? 1.0 / s.rho[e] : 0.0;
+    }
+  }
+  load_q(0);
+  __syncthreads();
+
+  const int st7[7] = {ew, ew + 1, ew + WW + 1, ew + WW, ew - 1, ew - WW - 1, ew - WW};
+  const int fslot[7] = {0, tid, tid, tid, tid - 1, tid - RW - 1, tid - RW};  // owner thread of face m
   auto cx = [](const V2 &v, int h) { return h ? v.y : v.x; };
-  // gradient and Qout of this (FP32) cell from q at the cell and its 6 neighbours
-  auto cell_gq = [&](const R qs[7], R out[5]) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      R g = cgr[c * 7] * qs[0];
-#pragma unroll
-      for (int n = 1; n < 7; ++n) g = g + cgr[c * 7 + n] * qs[n];
-      out[c] = g;
-    }
-    // 4-point bounds of the 6 faces (mod_src_tracer.f90:152-214): face m is the cell and
-    // the neighbours m-1, m, m+1 (cyclic, n0 = n6)
-    const R c0 = qs[0], n1 = qs[1], n2 = qs[2], n3 = qs[3], n4 = qs[4], n5 = qs[5], n6 = qs[6];
-    R lo[7], hi[7];
-    const R l12 = A::mn(n1, n2), l34 = A::mn(n3, n4), l56 = A::mn(n5, n6);
-    const R h12 = A::mx(n1, n2), h34 = A::mx(n3, n4), h56 = A::mx(n5, n6);
-    lo[1] = A::mn(c0, A::mn(n6, l12)), hi[1] = A::mx(c0, A::mx(n6, h12));
-    lo[2] = A::mn(c0, A::mn(l12, n3)), hi[2] = A::mx(c0, A::mx(h12, n3));
-    lo[3] = A::mn(c0, A::mn(n2, l34)), hi[3] = A::mx(c0, A::mx(n2, h34));
-    lo[4] = A::mn(c0, A::mn(l34, n5)), hi[4] = A::mx(c0, A::mx(h34, n5));
-    lo[5] = A::mn(c0, A::mn(n4, l56)), hi[5] = A::mx(c0, A::mx(n4, h56));
-    lo[6] = A::mn(c0, A::mn(l56, n1)), hi[6] = A::mx(c0, A::mx(h56, n1));
-    R qnmin = c0, qnmax = c0, CQmin = R(0.0), CQmax = R(0.0);
-#pragma unroll
-    for (int m = 1; m <= 6; ++m) {
-      const bool in = (inmask >> m) & 1u;
-      const R qmn = in ? lo[m] : BIGf, qmx = in ? hi[m] : -BIGf;
-      qnmin = A::mn(qnmin, qmn);
-      qnmax = A::mx(qnmax, qmx);
-      CQmin = (m == 1) ? chm[1] * qmn : CQmin + chm[m] * qmn;
-      CQmax = (m == 1) ? chm[1] * qmx : CQmax + chm[m] * qmx;
-    }
-    out[3] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
-    out[4] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
-  };
-  // Per batch b: (B) gradient + Qout, (C) face values, then (D) the update of batch b
-  // together with (A) q of batch b+1, whose rhogq window streamed in during B and C.
-  // Three barriers per batch.
-  // the first batch's window has landed (the second may still be in flight)
-  if (TB < ntr) asm volatile("cp.async.wait_group 1;\n" ::);
-  else asm volatile("cp.async.wait_group 0;\n" ::);
-  __syncthreads();
-  // ---- (A) q of the first batch
-  load_q(0, 0);
-  __syncthreads();
   for (int t0 = 0, b = 0; t0 < ntr; t0 += TB, ++b) {
     const int ntg = min(TB, ntr - t0);
-    // ---- (B) gradient and Qout of the ring cells
-    if (in_arr) {
-      if (bs >= 0) {  // region-boundary cell or halo cell: the FP64 boundary values
+    // ---- (B) per interior ring cell and tracer: gradient and Qout (formed here, or the FP64
+    // boundary values of a region-boundary cell), the 4-point bounds of its 6 faces, and the
+    // limited value of each of its outflow faces; owners fill their seam and absent faces
+    if (c_int) {
 #pragma unroll
-        for (int pp = 0; pp < TP; ++pp) {
-          R o[2][5];
+      for (int pp = 0; pp < TP; ++pp) {
+        V2 q7[7];
+#pragma unroll
+        for (int n = 0; n < 7; ++n) q7[n] = s.q2[pp][st7[n]];
+        R g[2][3], qmn_c[2], qmx_c[2], lo[2][7], hi[2][7], q0[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          R qs[7];
+#pragma unroll
+          for (int n = 0; n < 7; ++n) qs[n] = cx(q7[n], h);
+          q0[h] = qs[0];
+          // bounds of face m: the cell and its neighbours m-1, m, m+1 (cyclic, n0 = n6),
+          // mod_src_tracer.f90:152-214
+          const R c0 = qs[0], n1 = qs[1], n2 = qs[2], n3 = qs[3], n4 = qs[4], n5 = qs[5], n6 = qs[6];
+          const R l12 = A::mn(n1, n2), l34 = A::mn(n3, n4), l56 = A::mn(n5, n6);
+          const R h12 = A::mx(n1, n2), h34 = A::mx(n3, n4), h56 = A::mx(n5, n6);
+          lo[h][1] = A::mn(c0, A::mn(n6, l12)), hi[h][1] = A::mx(c0, A::mx(n6, h12));
+          lo[h][2] = A::mn(c0, A::mn(l12, n3)), hi[h][2] = A::mx(c0, A::mx(h12, n3));
+          lo[h][3] = A::mn(c0, A::mn(n2, l34)), hi[h][3] = A::mx(c0, A::mx(n2, h34));
+          lo[h][4] = A::mn(c0, A::mn(l34, n5)), hi[h][4] = A::mx(c0, A::mx(h34, n5));
+          lo[h][5] = A::mn(c0, A::mn(n4, l56)), hi[h][5] = A::mx(c0, A::mx(n4, h56));
+          lo[h][6] = A::mn(c0, A::mn(l56, n1)), hi[h][6] = A::mx(c0, A::mx(h56, n1));
+          if (tile_cell) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              R gg = cgr[c * 7] * qs[0];
+#pragma unroll
+              for (int n = 1; n < 7; ++n) gg = gg + cgr[c * 7 + n] * qs[n];
+              g[h][c] = gg;
+            }
+            // Thuburn outflow bounds (mod_src_tracer.f90:219-282, d = 0): the inflow faces are
+            // this cell's faces that are not outflow faces
+            R qnmin = c0, qnmax = c0, CQmin = R(0.0), CQmax = R(0.0);
+#pragma unroll
+            for (int m = 1; m <= 6; ++m) {
+              const bool in = !((upm >> m) & 1u);
+              const R qmn = in ? lo[h][m] : BIGf, qmx = in ? hi[h][m] : -BIGf;
+              qnmin = A::mn(qnmin, qmn);
+              qnmax = A::mx(qnmax, qmx);
+              CQmin = (m == 1) ? chm[1] * qmn : CQmin + chm[m] * qmn;
+              CQmax = (m == 1) ? chm[1] * qmx : CQmax + chm[m] * qmx;
+            }
+            qmn_c[h] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
+            qmx_c[h] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
+          } else {  // region-boundary cell: the FP64 boundary values (k_fast_boundary)
+            const bool okt = 2 * pp + h < ntg;
+            const double *bv = bval(I, okt ? t0 + 2 * pp + h : t0, k, bs);
+            g[h][0] = okt ? (R)bv[0] : R(0.0);
+            g[h][1] = okt ? (R)bv[1] : R(0.0);
+            g[h][2] = okt ? (R)bv[2] : R(0.0);
+            qmn_c[h] = okt ? (R)bv[3] : R(0.0);
+            qmx_c[h] = okt ? (R)bv[4] : R(0.0);
+          }
+        }
+        // limited values of the outflow faces (remap with the upwind gradient, clipped to the
+        // face's 4-point bounds, then to the upwind cell's Qout; :378-410)
+#pragma unroll
+        for (int m = 1; m <= 6; ++m) {
+          if (!((dom >> m) & 1u)) continue;
+          const int a = (m - 1) % 3;
+          const V4 dv = s.dup[a][fslot[m]];
+          R v[2];
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const bool ok = 2 * pp + h < ntg;
-            const double *bv = bval(I, ok ? t0 + 2 * pp + h : t0, k, bs);
-#pragma unroll
-            for (int c = 0; c < 5; ++c) o[h][c] = ok ? (R)bv[c] : R(0.0);
+            R w = q0[h];
+            w = w + g[h][0] * dv.x;
+            w = w + g[h][1] * dv.y;
+            w = w + g[h][2] * dv.z;
+            w = A::mn(A::mx(w, lo[h][m]), hi[h][m]);
+            v[h] = A::mx(A::mn(w, qmx_c[h]), qmn_c[h]);
           }
-#pragma unroll
-          for (int c = 0; c < 5; ++c) s.t.gq[pp][c][tid] = A::v2(o[0][c], o[1][c]);
-        }
-      } else if (!tile_cell) {  // halo point no list reaches: grad 0, Qout = q
-#pragma unroll
-        for (int pp = 0; pp < TP; ++pp) {
-          const V2 qc = s.q2[pp][ec];
-          s.t.gq[pp][0][tid] = s.t.gq[pp][1][tid] = s.t.gq[pp][2][tid] = A::v2(R(0.0), R(0.0));
-          s.t.gq[pp][3][tid] = s.t.gq[pp][4][tid] = qc;
-        }
-      } else {
-        const int st7[7] = {ec, ec + 1, ec + WW + 1, ec + WW, ec - 1, ec - WW - 1, ec - WW};
-#pragma unroll
-        for (int pp = 0; pp < TP; ++pp) {
-          V2 q2[7];
-#pragma unroll
-          for (int n = 0; n < 7; ++n) q2[n] = s.q2[pp][st7[n]];
-          R o[2][5];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            R qs[7];
-#pragma unroll
-            for (int n = 0; n < 7; ++n) qs[n] = cx(q2[n], h);
-            cell_gq(qs, o[h]);
-          }
-#pragma unroll
-          for (int c = 0; c < 5; ++c) s.t.gq[pp][c][tid] = A::v2(o[0][c], o[1][c]);
+          s.qa[pp][a][fslot[m]] = A::v2(v[0], v[1]);
         }
       }
     }
-    __syncthreads();
-    // ---- (C) limited values of the faces owned by ring cells x, y in [-1, T-1]
-    if (owner) {
-      const int nbt[3] = {tid + 1, tid + RW + 1, tid + RW};  // ring thread of the neighbour
-      const int nbs[3] = {ec + 1, ec + WW + 1, ec + WW};       // window slot of the neighbour
+    if (seam_own | zero_own) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        const int ni = (a < 2) ? ci + 1 : ci, nj = (a > 0) ? cj + 1 : cj;
-        // needed by a tile cell (the owner or the neighbour)?
-        const bool need = (x >= 0 && y >= 0) || (ni - i0 >= 0 && nj - j0 >= 0 && ni - i0 < TX && nj - j0 < TY);
-        if (!need || !face_exists(I, ci, cj, a + 1)) {
+        if ((zero_own >> a) & 1u) {
 #pragma unroll
-          for (int pp = 0; pp < TP; ++pp) s.t.qa[pp][a][tid] = A::v2(R(0.0), R(0.0));
-          continue;
-        }
-        if (!c_int || !interior(ni, nj)) {  // seam face: value of k_fast_seam
+          for (int pp = 0; pp < TP; ++pp) s.qa[pp][a][tid] = A::v2(R(0.0), R(0.0));
+        } else if ((seam_own >> a) & 1u) {
           const int sid = I.seam_id[((size_t)l * I.gall + ccell) * 3 + a];
 #pragma unroll
           for (int pp = 0; pp < TP; ++pp) {
@@ -819,66 +869,59 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
             for (int h = 0; h < 2; ++h)
               v[h] = (2 * pp + h < ntg) ? (sizeof(R) == 8 ? (R)I.sval64[((size_t)(t0 + 2 * pp + h) * K + k) * I.ns + sid]
                                                           : (R)I.sval[((size_t)(t0 + 2 * pp + h) * K + k) * I.ns + sid])
-                                          : R(0.0);
-            s.t.qa[pp][a][tid] = A::v2(v[0], v[1]);
+                                        : R(0.0);
+            s.qa[pp][a][tid] = A::v2(v[0], v[1]);
           }
-          continue;
-        }
-        const bool cmu = (cmown >> a) & 1u;  // 1: the neighbour is upwind
-        const int ut = cmu ? nbt[a] : tid, us = cmu ? nbs[a] : ec;
-        // the face's 4 points besides the cell: AI {j-1, i+1, i+1j+1}, AIJ {i+1, i+1j+1, j+1},
-        // AJ {i+1j+1, j+1, i-1}
-        const int p1 = (a == 0) ? ec - WW : (a == 1 ? ec + 1 : ec + WW + 1);
-        const int p2 = (a == 0) ? ec + 1 : (a == 1 ? ec + WW + 1 : ec + WW);
-        const int p3 = (a == 0) ? ec + WW + 1 : (a == 1 ? ec + WW : ec - 1);
-#pragma unroll
-        for (int pp = 0; pp < TP; ++pp) {
-          const V2 qu = s.q2[pp][us], g0 = s.t.gq[pp][0][ut], g1 = s.t.gq[pp][1][ut], g2 = s.t.gq[pp][2][ut];
-          const V2 on = s.t.gq[pp][3][ut], ox = s.t.gq[pp][4][ut];
-          const V2 c0 = s.q2[pp][ec], b1 = s.q2[pp][p1], b2 = s.q2[pp][p2], b3 = s.q2[pp][p3];
-          R v[2];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            R w = cx(qu, h);
-            w = w + cx(g0, h) * dup[a][0];
-            w = w + cx(g1, h) * dup[a][1];
-            w = w + cx(g2, h) * dup[a][2];
-            const R lo = A::mn(A::mn(A::mn(cx(c0, h), cx(b1, h)), cx(b2, h)), cx(b3, h));
-            const R hi = A::mx(A::mx(A::mx(cx(c0, h), cx(b1, h)), cx(b2, h)), cx(b3, h));
-            w = A::mn(A::mx(w, lo), hi);
-            v[h] = A::mx(A::mn(w, cx(ox, h)), cx(on, h));
-          }
-          s.t.qa[pp][a][tid] = A::v2(v[0], v[1]);
         }
       }
     }
-    asm volatile("cp.async.wait_group 0;\n" ::);  // this thread's copies of batch b+1 have landed
     __syncthreads();
     // ---- (D) horizontal update of the tile cells (FP64): rhogq after the horizontal sub-step
     if (active) {
+      double fx[7];
+#pragma unroll
+      for (int m = 1; m <= 6; ++m) fx[m] = s.flx[m - 1][tid];
 #pragma unroll
       for (int pp = 0; pp < TP; ++pp) {
-        const V2 f1 = s.t.qa[pp][0][tid], f2 = s.t.qa[pp][1][tid], f3 = s.t.qa[pp][2][tid];
-        const V2 f4 = s.t.qa[pp][0][tid - 1], f5 = s.t.qa[pp][1][tid - RW - 1], f6 = s.t.qa[pp][2][tid - RW];
+        const V2 f1 = s.qa[pp][0][tid], f2 = s.qa[pp][1][tid], f3 = s.qa[pp][2][tid];
+        const V2 f4 = s.qa[pp][0][tid - 1], f5 = s.qa[pp][1][tid - RW - 1], f6 = s.qa[pp][2][tid - RW];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int tt = 2 * pp + h;
           if (tt >= ntg) break;
-          const size_t o = (size_t)(t0 + tt) * tstride + base + ccell;
-          const double Qin = s.stage[b & 1][tt][ec];
+          const size_t o = (size_t)(t0 + tt) * n3 + oc;
+          const double Qin = s.stage[b & 1][tt][ew];
           const R qa[7] = {R(0.0), cx(f1, h), cx(f2, h), cx(f3, h), cx(f4, h), cx(f5, h), cx(f6, h)};
-          double sum = flx[1] * (double)qa[1];
+          double sum = fx[1] * (double)qa[1];
 #pragma unroll
-          for (int m = 2; m <= 6; ++m) sum = sum + flx[m] * (double)qa[m];
+          for (int m = 2; m <= 6; ++m) sum = sum + fx[m] * (double)qa[m];
           I.Q_out[o] = Qin - sum;
         }
       }
     }
-    // ---- (A) q of the next batch; then its buffer's successor streams in
-    if (t0 + TB < ntr) load_q(t0 + TB, (b + 1) & 1);
+    // ---- (A) q of the next batch, whose copy streamed in during (B)
+    if (b + 1 < nbat) {
+      const int nb1 = (b + 1) & 1;
+      ok = mbar_wait(&s.mbar[nb1], (phase >> nb1) & 1u) && ok;
+      phase ^= 1u << nb1;
+      load_q(nb1);
+    }
     __syncthreads();
-    if (t0 + 2 * TB < ntr) issue(t0 + 2 * TB, b & 1);
+    // every read of stage[b & 1] is done: batch b + 2 streams into it
+    if (tid == 0 && b + 2 < nbat) {
+      mbar_expect_tx(&s.mbar[b & 1], QBYTES);
+      tma_load_4d(&s.stage[b & 1][0][0], &T->q, wx, wy, wsl, (b + 2) * TB, &s.mbar[b & 1]);
+    }
   }
+  if (!ok && tid == 0) atomicOr(I.err, 1);
+  return ok;
+}
+
+template <int TX, int TY, int TB, typename R>
+__device__ __forceinline__ TileSmem<TX, TY, TB, R> &tile_smem(unsigned char *raw) {
+  // the dynamic allocation carries 128 bytes of slack for this alignment (TMA destinations)
+  const size_t a = ((size_t)raw + 127) & ~(size_t)127;
+  return *reinterpret_cast<TileSmem<TX, TY, TB, R> *>(a);
 }
 
 // Batches of instances: persistent, one wave of CTAs; each takes the next work item
@@ -886,11 +929,12 @@ __device__ __forceinline__ void horiz_item(const FastInst I, const int tile, con
 // drew cheap items take more (as fast as one CTA per item; a static stride was 9% slower).
 template <int TX, int TY, int TB, typename R>
 __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
-    k_fast_horiz(const __grid_constant__ MultiInst M, long long nwork) {
-  using S = TileSmem<TX, TY, TB, R>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S &s = *reinterpret_cast<S *>(smem_raw);
+    k_fast_horiz(const __grid_constant__ MultiInst M, const __grid_constant__ MultiMaps T, long long nwork) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  auto &s = tile_smem<TX, TY, TB, R>(smem_raw);
   __shared__ long long s_item;
+  tile_smem_init(s);
+  unsigned phase = 0;
   for (;;) {
     if (threadIdx.x == 0) s_item = (long long)atomicAdd(M.inst[0].work_next, 1ULL);
     __syncthreads();
@@ -899,23 +943,27 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
     const int ii = find_inst(M, wi, [](const FastInst &J) { return (long long)J.lall * J.ntx * J.nty * (J.K - 2); });
     const int ntl = M.inst[ii].lall * M.inst[ii].ntx * M.inst[ii].nty;
     const int tile = (int)(wi % ntl), k = 1 + (int)(wi / ntl);
+    bool ok;
     switch (ii) {
-      case 0: horiz_item<TX, TY, TB, R>(M.inst[0], tile, k, s); break;
-      case 1: horiz_item<TX, TY, TB, R>(M.inst[1], tile, k, s); break;
-      case 2: horiz_item<TX, TY, TB, R>(M.inst[2], tile, k, s); break;
-      default: horiz_item<TX, TY, TB, R>(M.inst[3], tile, k, s); break;
+      case 0: ok = horiz_item<TX, TY, TB, R>(M.inst[0], &T.m[0], tile, k, s, phase); break;
+      case 1: ok = horiz_item<TX, TY, TB, R>(M.inst[1], &T.m[1], tile, k, s, phase); break;
+      case 2: ok = horiz_item<TX, TY, TB, R>(M.inst[2], &T.m[2], tile, k, s, phase); break;
+      default: ok = horiz_item<TX, TY, TB, R>(M.inst[3], &T.m[3], tile, k, s, phase); break;
     }
-    __syncthreads();  // the next item's fields overwrite this item's shared data; s_item is reread
+    // the next item's data overwrite this item's shared data; s_item is reread
+    if (__syncthreads_or(!ok)) break;
   }
 }
 
 // one grid: one CTA per (tile, level) (grid x = tile, y = level - 1)
 template <int TX, int TY, int TB, typename R>
-__global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2)) k_fast_horiz1(FastInst I) {
-  using S = TileSmem<TX, TY, TB, R>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S &s = *reinterpret_cast<S *>(smem_raw);
-  horiz_item<TX, TY, TB, R>(I, (int)blockIdx.x, 1 + (int)blockIdx.y, s);
+__global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
+    k_fast_horiz1(const __grid_constant__ FastInst I, const __grid_constant__ TileMaps T) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  auto &s = tile_smem<TX, TY, TB, R>(smem_raw);
+  tile_smem_init(s);
+  unsigned phase = 0;
+  horiz_item<TX, TY, TB, R>(I, &T, (int)blockIdx.x, 1 + (int)blockIdx.y, s, phase);
 }
 
 // ---- vertical sub-step: one thread per (interior column, TV tracers), streaming the
@@ -1220,9 +1268,50 @@ __global__ void k_fast_carry(const __grid_constant__ MultiInst M) {
 }
 
 // ---------------------------------------------------------------------------------------
+// TMA descriptors of the tile windows.  cuTensorMapEncodeTiled is a driver-API function; it is
+// reached through the runtime's driver entry point, so the library links only cudart.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// rhogq_in as (i, j, l*K + k, tracer) with box (WW, WH, 1, TB) and rhog_in as (i, j, l*K + k)
+// with box (WW, WH, 1); out-of-range elements of a box are filled with zeros.
+static cudaError_t tile_maps(const FastInst &I, int WW, int WH, int TB, TileMaps &T) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return cudaErrorNotSupported;
+  const cuuint64_t G = (cuuint64_t)I.G, S = (cuuint64_t)I.lall * I.K;
+  const cuuint64_t dq[4] = {G, G, S, (cuuint64_t)I.ntr};
+  const cuuint64_t sq[3] = {G * 8, G * G * 8, S * G * G * 8};
+  const cuuint32_t bq[4] = {(cuuint32_t)WW, (cuuint32_t)WH, 1, (cuuint32_t)TB};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = enc(&T.q, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)I.Q_in, dq, sq, bq, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  r = enc(&T.rho, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)I.rho_in, dq, sq, bq, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  return cudaSuccess;
+}
+
 template <int TX, int TY, int TB, bool ONE, typename R>
 static cudaError_t launch_tile_n(const MultiInst &M, cudaStream_t st) {
-  const int smem = (int)sizeof(TileSmem<TX, TY, TB, R>);
+  const int smem = (int)sizeof(TileSmem<TX, TY, TB, R>) + 128;  // + slack for the 128-byte alignment
   constexpr int NT = TileGeo<TX, TY>::NT;
   static int per_sm[64] = {};  // resident CTAs per SM, per device (set up once, outside any capture)
   int dev = 0;
@@ -1244,16 +1333,22 @@ static cudaError_t launch_tile_n(const MultiInst &M, cudaStream_t st) {
   int nsm = 0;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
+  MultiMaps T;
+  for (int i = 0; i < M.n; ++i) {
+    e = tile_maps(M.inst[i], TileGeo<TX, TY>::WW, TileGeo<TX, TY>::WH, TB, T.m[i]);
+    if (e != cudaSuccess) return e;
+  }
   long long nwork = 0;
   for (int i = 0; i < M.n; ++i) nwork += (long long)M.inst[i].lall * M.inst[i].ntx * M.inst[i].nty * (M.inst[i].K - 2);
   if (ONE) {
     const FastInst &I = M.inst[0];
-    k_fast_horiz1<TX, TY, TB, R><<<dim3((unsigned)(I.lall * I.ntx * I.nty), (unsigned)(I.K - 2)), NT, smem, st>>>(I);
+    k_fast_horiz1<TX, TY, TB, R><<<dim3((unsigned)(I.lall * I.ntx * I.nty), (unsigned)(I.K - 2)), NT, smem, st>>>(
+        I, T.m[0]);
   } else {
     const long long grid = nwork < (long long)nsm * per_sm[dev] ? nwork : (long long)nsm * per_sm[dev];
     e = cudaMemsetAsync(M.inst[0].work_next, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    k_fast_horiz<TX, TY, TB, R><<<(unsigned)grid, NT, smem, st>>>(M, nwork);
+    k_fast_horiz<TX, TY, TB, R><<<(unsigned)grid, NT, smem, st>>>(M, T, nwork);
   }
   return cudaGetLastError();
 }

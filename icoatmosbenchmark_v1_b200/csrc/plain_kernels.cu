@@ -489,20 +489,20 @@ template <typename T>
 void launch_horizontal_flux(const Dims &D, const FluxIn<T> &in, const FluxOut<T> &out, const Geo<T> &g, T dt,
                             cudaStream_t s) {
   k_horizontal_flux<T><<<slab_grid(D, 128), 128, 0, s>>>(D, in, out, g, dt);
-  k_horizontal_flux_pl<T><<<(D.kall * kLallPl + 63) / 64, 64, 0, s>>>(D, in, out, g, dt);
+  if (D.have_pl) k_horizontal_flux_pl<T><<<(D.kall * kLallPl + 63) / 64, 64, 0, s>>>(D, in, out, g, dt);
 }
 
 template <typename T>
 void launch_hlim_qout(const Dims &D, const LimIn<T> &in, T *Qout, T *Qout_pl, T *Qin_pl, cudaStream_t s) {
   k_hlim_qout<T><<<slab_grid(D, 128), 128, 0, s>>>(D, in, Qout);
-  k_hlim_qout_pl<T><<<(D.kall * kLallPl + 63) / 64, 64, 0, s>>>(D, in, Qout_pl, Qin_pl);
+  if (D.have_pl) k_hlim_qout_pl<T><<<(D.kall * kLallPl + 63) / 64, 64, 0, s>>>(D, in, Qout_pl, Qin_pl);
 }
 
 template <typename T>
 void launch_hlim_apply(const Dims &D, const LimIn<T> &in, T *q_a, T *q_a_pl, const T *Qout, const T *Qout_pl,
                        const T *Qin_pl, cudaStream_t s) {
   k_hlim_apply<T><<<slab_grid(D, 128), 128, 0, s>>>(D, in, q_a, Qout);
-  k_hlim_apply_pl<T><<<(D.kall * kLallPl * 5 + 63) / 64, 64, 0, s>>>(D, in, q_a_pl, Qout_pl, Qin_pl);
+  if (D.have_pl) k_hlim_apply_pl<T><<<(D.kall * kLallPl * 5 + 63) / 64, 64, 0, s>>>(D, in, q_a_pl, Qout_pl, Qin_pl);
 }
 
 template <typename T>
@@ -512,7 +512,7 @@ void launch_vlim(const Dims &D, T *q_h, T *q_h_pl, const T *q, const T *q_pl, co
   const int ncol = D.gall * D.lall;
   k_vlim<T, false><<<(ncol + 127) / 128, 128, 0, s>>>(ncol, D.gall, D.kall, D.kmin, D.kmax, q_h, q, d, ck);
   const int ncp = kGallPl * kLallPl;
-  k_vlim<T, true><<<1, 32, 0, s>>>(ncp, kGallPl, D.kall, D.kmin, D.kmax, q_h_pl, q_pl, d_pl, ck_pl);
+  if (D.have_pl) k_vlim<T, true><<<1, 32, 0, s>>>(ncp, kGallPl, D.kall, D.kmin, D.kmax, q_h_pl, q_pl, d_pl, ck_pl);
 }
 
 template <typename T>

@@ -20,6 +20,7 @@ struct Dims {
   int kall, kmin, kmax;           // 1-based kmin/kmax
   int lall;
   const int *have_sgp;            // device array [lall]
+  int have_pl;                    // ADM_have_pl: the pole regions are processed
 };
 
 template <typename T> struct Geo {

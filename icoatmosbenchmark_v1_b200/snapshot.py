@@ -10,11 +10,11 @@ snapshots are for one region of a glevel-7 grid with the poles (`ADM_lall = 1`,
 
 This module reads and writes that format (arrays come back in this library's C layout:
 Fortran var(ij,k,l,m) is the C array [m][l][k][ij]) and runs a snapshot through the
-library: the snapshot's region is placed in region 1 of a whole grid (the library's
-context always holds all regions; the other regions get zero inputs and their outputs
-are not looked at), the kernel runs through its host-pointer entry point, and the
-outputs of that region and of the poles are compared with the expected ones, in the
-driver's `+check[name] max=..., min=..., sum=...` form.
+library as a driver would: a context made by ica_init_regions with the driver's own sizes
+(ADM_gall_1d, ADM_kall, ADM_kmin, ADM_kmax, ADM_lall = 1, ADM_have_pl, ADM_have_sgp(1)),
+the kernel through its host-pointer entry point on the snapshot's arrays as they are, and
+the outputs compared with the expected ones, in the driver's
+`+check[name] max=..., min=..., sum=...` form.
 
     python -m icoatmosbenchmark_v1_b200.snapshot run dyn_horiz_adv_flux snapshot.dyn_horiz_adv_flux.pe000000
 """
@@ -144,25 +144,7 @@ def value_check(name, a):
     return f" +check[{name[:16]:<16s}] max={_es(a.max())},min={_es(a.min())},sum={_es(a.sum())}"
 
 
-def _embed(a, lall):
-    """Region 1 of a whole grid from a one-region array [..., 1, K, G] (regions axis -3, or
-    -2 for the per-column geometry [..., 1, 1, G] with K0 = 1)."""
-    a = np.asarray(a)
-    shape = list(a.shape)
-    ax = len(shape) - 3
-    shape[ax] = lall
-    full = np.zeros(shape)
-    idx = [slice(None)] * len(shape)
-    idx[ax] = slice(0, a.shape[ax])
-    full[tuple(idx)] = a
-    return full
-
-
-def _region1(a):
-    return np.asarray(a)[..., :1, :, :]
-
-
-def run_snapshot(kernel, path, dims=SnapshotDims(), dt=360.0, device=0, precision="f64"):
+def run_snapshot(kernel, path, dims=SnapshotDims(), dt=360.0, device=0, precision="f64", have_sgp=(1,)):
     """Runs the snapshot's inputs through the library and returns (outputs, diffs): the
     computed outputs of the snapshot's region and the poles, and expected - computed per
     output (the driver's point-by-point diff).  precision "f32" runs the FP32 entry points,
@@ -174,9 +156,10 @@ def run_snapshot(kernel, path, dims=SnapshotDims(), dt=360.0, device=0, precisio
         raise ValueError(f"precision {precision!r}: f64 or f32")
     rp = np.float64 if precision == "f64" else np.float32
     s = read_snapshot(kernel, path, dims)
-    ctx = api.IcoAdv(dims.glevel, 0, dims.kall - 2, device)
-    lall = ctx.sizes.lall
-    full = {k: (_embed(v, lall) if not k.endswith("_pl") else np.ascontiguousarray(v)) for k, v in s.items()}
+    # the driver's module globals (problem_size.inc:28-50): one region with the singular point,
+    # both poles, levels kmin = 2 .. kmax = kall - 1
+    ctx = api.IcoAdv.regions(dims.gall_1d, dims.kall, 2, dims.kall - 1, dims.lall, True, list(have_sgp), device)
+    full = {k: np.ascontiguousarray(v) for k, v in s.items()}
     # kernel arguments in the working precision (the metrics stay FP64: the context keeps both).
     # In FP32 the +-HUGE-scale Qout bounds of cells without outflow become +-inf, as the
     # single-precision drivers' conversion of the same snapshot does
@@ -208,7 +191,7 @@ def run_snapshot(kernel, path, dims=SnapshotDims(), dt=360.0, device=0, precisio
             got = OrderedDict(q_h=qh, q_h_pl=qh_pl)
     finally:
         ctx.close()
-    got = OrderedDict((k, (v if k.endswith("_pl") else _region1(v)).astype(np.float64)) for k, v in got.items())
+    got = OrderedDict((k, v.astype(np.float64)) for k, v in got.items())
     diffs = OrderedDict((k, s[k] - v) for k, v in got.items())
     return got, diffs
 

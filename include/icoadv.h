@@ -65,6 +65,19 @@ typedef struct {
 /* Create a context: sizes, the CUDA stream and the halo/pole gather plan.
  * Replaces ADM_setup + COMM_setup (mod_adm.f90:165, mod_comm.f90:147). */
 int ica_init(const ica_dims *dims, ica_ctx **ctx);
+/* A context for arrays that hold part of a grid, sized by the module globals the reference's
+ * kernel drivers keep (kernels/NICAM/dyn_horiz_adv_flux/src/problem_size.inc:28-50):
+ * ADM_gall_1d, ADM_kall, ADM_kmin, ADM_kmax, ADM_lall, ADM_have_pl and
+ * ADM_have_sgp(1:ADM_lall) (0 or 1); ADM_gall = gall_1d^2, ADM_gmin = 2,
+ * ADM_gmax = gall_1d - 1.  The drivers' own case, one region of a glevel-7 grid and both
+ * poles, is (130, 42, 2, 41, 1, 1, {1}).  The kernel entry points (horizontal_flux,
+ * horizontal_limiter_thuburn with Qout_post given, vertical_limiter_thuburn) run on such
+ * arrays as on a whole grid, and have_pl = 0 leaves the pole arrays untouched, as the
+ * reference's `if (ADM_have_pl)` blocks do.  The context holds no region topology, so the
+ * COMM entry points, the limiter's on-GPU Qout fill (Qout_post = NULL), the composed steps
+ * and the batched path return ICA_ERR_STATE: the neighbours of a region are not known. */
+int ica_init_regions(int gall_1d, int kall, int kmin, int kmax, int lall, int have_pl,
+                     const int *have_sgp, int device, ica_ctx **ctx);
 int ica_finalize(ica_ctx *ctx);
 int ica_get_sizes(const ica_ctx *ctx, ica_sizes *out);
 /* The context's CUDA stream (a cudaStream_t), for the *_dev entry points. */
@@ -349,6 +362,11 @@ int ica_fast_set_shape(ica_ctx *ctx, int shape);
 /* Tracers per chunk of ica_advect_fast's copies; 0 (the default) sizes chunks at about
  * 1 GiB of rhogq, 1 to 4 tracers.  The result does not depend on it. */
 int ica_fast_set_host_chunk(ica_ctx *ctx, int tracers);
+/* Status of the batched kernels since the last call: *flags = 0, or bit 0 set if a wait of the
+ * horizontal kernel for its tile copies (TMA) gave up after its time limit (the step's result
+ * is then invalid); returns ICA_ERR_TIMEOUT in that case.  Synchronises the stream and clears
+ * the flags. */
+int ica_fast_status(ica_ctx *ctx, int *flags);
 /* CUDA-event timing of the horizontal kernel: returns the total milliseconds and
  * the number of launches recorded since the last call, then enables (1) or
  * disables (0) recording for the following calls.  Synchronises the stream. */

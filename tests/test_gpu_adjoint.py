@@ -105,33 +105,35 @@ def _run(ctx, dt, S, F, nsteps):
 
 
 def _central(dJ, S0, F0, which, idx, h0, grad, rtol, floor):
-    """Central differences of J at element idx of S0[which] or F0[which] with h0 and h0/2.
-    A point is away from limiter kinks when, at both h, the one-sided differences agree to
-    1e-4 and the two central differences agree to rtol (a kink within +-h, or rounding
-    noise of the forward run at too small an h, breaks one or the other): ('kink', fd)
-    otherwise.  Away from kinks: ('ok', fd) if |grad - fd| <= rtol max(|fd|, floor), else
-    ('bad', fd)."""
-    fds = []
-    for h in (h0, h0 / 2):
-        d = []
-        for sgn in (1, -1):
-            S = {k: v.clone() for k, v in S0.items()}
-            F = dict(F0)
-            if which in S:
-                S[which][idx] += sgn * h
-            else:
-                F[which] = F0[which].clone()
-                F[which][idx] += sgn * h
-            d.append(dJ(S, F))
-        right, left = d[0] / h, -d[1] / h
-        fd = (d[0] - d[1]) / (2 * h)
-        if abs(right - left) > 1e-4 * max(abs(right), abs(left), floor):
-            return "kink", fd
-        fds.append(fd)
-    fd = fds[0]
-    if abs(fds[0] - fds[1]) > rtol * max(abs(fd), floor):
+    """Central difference fd of J at element idx of S0[which] or F0[which] with step h0, checked
+    for limiter kinks near the point.  J is piecewise smooth (piecewise linear in the tracer), so
+    a kink at distance d < h0 biases fd by up to half its slope jump.  From J at +-h0 and +-2 h0
+    (J at the point itself is 0, as dJ is a difference from it): the second-order one-sided
+    differences (-3 J(0) + 4 J(+h) - J(+2h)) / 2h and its mirror agree to O(h^2) on a smooth
+    piece, and so do the central differences at h0 and 2 h0.  A kink with d < h0 moves one or
+    the other by at least the bias it puts on fd, so requiring both to agree to tau = rtol / 2
+    leaves fd within tau of the slope at the point.  ('kink', fd) when they do not agree;
+    away from kinks ('ok', fd) if |grad - fd| <= rtol max(|fd|, floor), else ('bad', fd)."""
+    J = {}
+    for m in (1, -1, 2, -2):
+        S = {k: v.clone() for k, v in S0.items()}
+        F = dict(F0)
+        if which in S:
+            S[which][idx] += m * h0
+        else:
+            F[which] = F0[which].clone()
+            F[which][idx] += m * h0
+        J[m] = dJ(S, F)
+    h = h0
+    fd = (J[1] - J[-1]) / (2 * h)
+    fd2 = (J[2] - J[-2]) / (4 * h)
+    right = (4 * J[1] - J[2]) / (2 * h)
+    left = (J[-2] - 4 * J[-1]) / (2 * h)
+    scale = max(abs(fd), floor)
+    tau = 0.5 * rtol
+    if abs(right - left) > tau * scale or abs(fd - fd2) > tau * scale:
         return "kink", fd
-    return ("ok" if abs(grad - fd) <= rtol * max(abs(fd), floor) else "bad"), fd
+    return ("ok" if abs(grad - fd) <= rtol * scale else "bad"), fd
 
 
 def _pick_interior(rng, g, shape, kall):

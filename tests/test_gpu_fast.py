@@ -41,6 +41,7 @@ def test_fast_matches_fp64_oracle(O, glevel, rlevel, kall, ntr, nsteps):
             O.step(c["dims"], g.have_sgp, c["topo"], c["dt"], S, f, g.arrays, nthreads=8)
             r.step()
         got = {k: v.cpu().numpy() for k, v in r.state.items()}
+        assert ctx.fast_status() == 0  # every wait of the tile kernel for its TMA copies ended in time
         for k in ("rhog", "rhog_pl", "rhogq", "rhogq_pl"):
             e = rel_err(got[k], S[k])
             assert e <= FP32_TOL, (k, e)
@@ -65,6 +66,7 @@ def test_fast_every_tile_shape(O):
             got = r.state["rhogq"].cpu().numpy()
             assert rel_err(got, S["rhogq"]) <= FP32_TOL, s
             outs.append(got)
+        assert ctx.fast_status() == 0
         for o in outs[1:]:  # the tile shape does not change any result
             np.testing.assert_array_equal(o, outs[0])
     finally:

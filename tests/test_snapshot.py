@@ -149,32 +149,37 @@ def test_run_snapshot_matches_expected(tmp_path, O, cuda, kernel):
 
 
 class _OracleCtx:
-    """Stands in for api.IcoAdv on CPU (same methods, in-place outputs), computing with the
-    oracle, so that the snapshot plumbing (region embedding, geometry without the K0 axis,
-    the driver's initial output values) is checked without a GPU."""
+    """Stands in for api.IcoAdv on CPU (same constructor for a driver's arrays, the same
+    methods, in-place outputs), computing with the oracle on the driver's one region, so
+    that the snapshot plumbing (the driver's sizes, geometry without the K0 axis, the
+    driver's initial output values) is checked without a GPU."""
 
-    def __init__(self, glevel, rlevel, vlayer, device=0):
-        from icoatmosbenchmark_v1_b200.grid import Grid
+    @classmethod
+    def regions(cls, gall_1d, kall, kmin, kmax, lall, have_pl, have_sgp, device=0):
         from oracle import oracle
-        self.O, self.g = oracle, Grid(glevel, rlevel, vlayer + 2)
-        self.d = oracle.make_dims(glevel, rlevel, vlayer + 2)
-        self.sizes = type("Sizes", (), {"lall": self.g.lall})()
+        self = cls.__new__(cls)
+        glevel = int(round(np.log2(gall_1d - 2)))
+        self.O = oracle
+        self.d = oracle.make_dims(glevel, 0, kall, kmin, kmax, lall=lall, have_pl=int(have_pl))
+        self.have_sgp = np.asarray(have_sgp, np.int32)
+        self.gall, self.lall = gall_1d * gall_1d, lall
+        self.sizes = type("Sizes", (), {"lall": lall})()
+        return self
 
     def set_geometry(self, *geo):
         names = ("GRD_xr", "GRD_xr_pl", "GMTR_p", "GMTR_p_pl", "GMTR_t", "GMTR_t_pl", "GMTR_a", "GMTR_a_pl")
-        ref = self.g.geometry()
-        for n, a in zip(names, geo):
-            assert a.shape == ref[n].shape, (n, a.shape, ref[n].shape)
+        for n, a in zip(names, geo):  # the library's layout: [..., lall, gall] and [..., 2, 6]
+            assert a.shape[-2:] == ((2, 6) if n.endswith("_pl") else (self.lall, self.gall)), (n, a.shape)
         self.geo = dict(zip(names, geo))
 
     def horizontal_flux(self, flx, flx_pl, xc, xc_pl, rho, rho_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, dt):
-        a, ap, x, xp = self.O.horizontal_flux(self.d, self.g.have_sgp, rho, rho_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl,
+        a, ap, x, xp = self.O.horizontal_flux(self.d, self.have_sgp, rho, rho_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl,
                                               dt, self.geo)
         flx[...], xc[...] = a, x
         flx_pl[:, :, 1:], xc_pl[..., 1:] = ap[:, :, 1:], xp[..., 1:]  # pole centre not written
 
     def horizontal_limiter_thuburn(self, qa, qa_pl, q, q_pl, d, d_pl, ch, ch_pl, cm, cm_pl, qo, qo_pl, post, post_pl):
-        a, ap, o, op = self.O.horizontal_limiter(self.d, self.g.have_sgp, qa, qa_pl, q, q_pl, d, d_pl, ch, ch_pl, cm,
+        a, ap, o, op = self.O.horizontal_limiter(self.d, self.have_sgp, qa, qa_pl, q, q_pl, d, d_pl, ch, ch_pl, cm,
                                                  cm_pl, Qout_post=post, Qout_post_pl=post_pl)
         qa[...], qa_pl[...], qo[...], qo_pl[...] = a, ap, o, op
 
@@ -188,8 +193,9 @@ class _OracleCtx:
 
 @pytest.mark.parametrize("kernel", S.KERNELS)
 def test_run_snapshot_plumbing_with_oracle(tmp_path, O, monkeypatch, kernel):
-    """run_snapshot's embedding of the snapshot's region in a whole grid, with the oracle in
-    place of the CUDA library: the region's outputs come back equal to the expected ones."""
+    """run_snapshot on the driver's one-region arrays, with the oracle in place of the CUDA
+    library (the oracle restates the kernels for any ADM_lall): the region's outputs come back
+    equal to the expected ones, which the oracle computed on the whole grid."""
     from icoatmosbenchmark_v1_b200 import api
     monkeypatch.setattr(api, "IcoAdv", _OracleCtx)
     paths, dt = synthetic_snapshots(tmp_path, O)
