@@ -198,7 +198,9 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    t_host = time.perf_counter()
     g = Grid(args.glevel, 0, args.kall)
+    t_host = time.perf_counter() - t_host
     dt = default_dt(args.glevel)
     f = F.make_fields(g, device=dev)
     st = F.make_state(g, args.ntr, "mixed", device=dev, fields=f)
@@ -207,6 +209,9 @@ def run_ours(args, world, rank, local):
     ctx.set_grid(g)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     upd = (10 * 4 ** args.glevel + 2) * args.kall * args.ntr
+    grid_setup = measure_grid_setup(ctx, g, stream, t_host)
+    if args.shard and args.mode == "fast":
+        return run_sharded(args, world, rank, local, ctx, g, st, f, dt, upd, grid_setup)
 
     if args.mode == "plain":
         def step():
@@ -309,7 +314,8 @@ def run_ours(args, world, rank, local):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": cfg,
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+                "grid_setup": grid_setup}
         if err is not None:
             line["max_rel_err_vs_fp64"] = err  # first step vs the FP64 plain path (bit-exact to the oracle)
             line["mass_drift"] = {"value": drift, "steps": 1 + args.warmup + args.steps}
@@ -376,6 +382,71 @@ def measure_fast64(args, ctx, g, init, ref, f, dt, shape, ms32):
            "time_vs_fp32_variant": ms / ms32}
     del r
     return out
+
+
+def measure_grid_setup(ctx, g, stream, t_host):
+    """The grid's positions and metrics built on the device (ica_grid_build_dev, timed with CUDA
+    events after one warm build) beside the host (numpy) build the run uses, and the largest
+    difference between the two relative to each array's largest magnitude."""
+    import torch
+    out = ctx.build_grid(g.R)  # warm: the context's scratch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = ctx.build_grid(g.R)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    err = 0.0
+    for k, v in out.items():
+        ref = torch.as_tensor(g.arrays[k], device=v.device)
+        err = max(err, float((v - ref).abs().max() / ref.abs().max().clamp_min(1e-300)))
+    del out
+    torch.cuda.empty_cache()
+    return {"device_ms": e0.elapsed_time(e1), "host_numpy_s": t_host, "max_rel_diff": err,
+            "what": "positions, GMTR_p/t/a, GRD_xr, coef_grad and pole arrays"}
+
+
+def run_sharded(args, world, rank, local, ctx, g, st, f, dt, upd, grid_setup):
+    """--shard: the workload region-sharded over the ranks (strong scaling: the same grid on
+    every N), each rank computing its block of regions with the two exchanges of a step as NCCL
+    send/recv (ShardedRunner).  value = the whole grid's updates / the max over ranks of the
+    step time."""
+    import torch
+
+    from icoatmosbenchmark_v1_b200 import shard
+    plan = shard.ShardPlan.build(args.glevel, 0, world)
+    ctx.fast_set_shape(args.tile_shape if args.tile_shape >= 0 else 3)
+    run = shard.ShardedRunner(ctx, plan, rank, st, f, dt)
+    for _ in range(args.warmup):
+        run.step()
+    torch.cuda.synchronize()
+    barrier(world)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    sampler.start()
+    n0 = ctx.launch_count
+    e0.record(stream)
+    for _ in range(args.steps):
+        run.step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = allreduce_max(e0.elapsed_time(e1) / args.steps, world)
+    bval_b, halo_b = plan.bytes_per_step(args.kall, args.ntr)
+    status = ctx.fast_status()
+    if rank == 0:
+        cfg = workload_config(args)
+        cfg["parallelism"] = f"regions sharded over {world} ranks (blocks {plan.blocks}), NCCL send/recv"
+        line = {"metric": METRIC, "value": upd / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+                "exchange_bytes_per_step": {"boundary_values": bval_b, "halo": halo_b},
+                "gpu_launches": ctx.launch_count - n0, "clocks": clocks, "grid_setup": grid_setup,
+                "status": status}
+        print(json.dumps(line), flush=True)
+    ctx.close()
 
 
 UNEVEN = ((7, 96, 40), (6, 42, 12))  # (glevel, kall, tracers) of the two instances
@@ -661,6 +732,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true", help="skip the error / mass-drift check")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint sweep measurement")
+    ap.add_argument("--shard", action="store_true",
+                    help="shard the grid's regions over the ranks (NCCL exchanges) instead of running replicas")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the FP64 variant and the uneven batch (extra keys of the default line)")
     ap.add_argument("--adjoint-steps", type=int, default=12, help="steps of the adjoint sweep")

@@ -273,6 +273,29 @@ class IcoAdv:
         self._call("ica_comm_var", self._dtype(var), [var, var_pl], int(kmax), int(vmax))
 
     # ---- composed step -----------------------------------------------------------
+    GRID_KEYS = (("GRD_x", (3,), (3, 2, 6)), ("GRD_xr", (3, 3), (3, 2, 6)), ("GMTR_p", (8,), (8, 2, 6)),
+                 ("GMTR_t", (5, 2), (5, 2, 6)), ("GMTR_a", (12, 3), (18, 2, 6)))
+
+    def build_grid(self, radius):
+        """The grid's positions and metrics built on the device (ica_grid_build_dev): a dict of
+        CUDA tensors with the names and shapes of grid.Grid.arrays (GRD_x, GRD_xr, GMTR_p/t/a,
+        coef_grad and their pole arrays)."""
+        import torch
+        L, g = self.sizes.lall, self.sizes.gall
+        dev = torch.device("cuda", self.device)
+        out = {}
+        for name, lead, pl in self.GRID_KEYS:
+            out[name] = torch.empty(lead + (L, g), dtype=torch.float64, device=dev)
+            out[name + "_pl"] = torch.empty(pl, dtype=torch.float64, device=dev)
+        out["coef_grad"] = torch.empty((L, 3, 7, g), dtype=torch.float64, device=dev)
+        out["coef_grad_pl"] = torch.empty((2, 3, 6), dtype=torch.float64, device=dev)
+        order = ("GRD_x", "GRD_x_pl", "GRD_xr", "GRD_xr_pl", "GMTR_p", "GMTR_p_pl", "GMTR_t", "GMTR_t_pl",
+                 "GMTR_a", "GMTR_a_pl", "coef_grad", "coef_grad_pl")
+        with self._ordered():
+            _check("ica_grid_build_dev", lib().ica_grid_build_dev(self.h, C.c_double(radius),
+                                                                  *[C.c_void_p(out[k].data_ptr()) for k in order]))
+        return out
+
     def set_step_geometry(self, GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact, bfact):
         keep = [np.ascontiguousarray(a, np.float64) for a in (GRD_x, GRD_x_pl, coef_grad, coef_grad_pl, rdgz, afact,
                                                                bfact)]
@@ -364,6 +387,43 @@ class IcoAdv:
         fp = [_ptr(a, np.float32)[0] for a in (rhogvx, rhogvx_pl, rhogvy, rhogvy_pl, rhogvz, rhogvz_pl, rhogw,
                                              rhogw_pl)]
         _check("ica_advect_fast", lib().ica_advect_fast(self.h, int(ntr), C.c_double(dt), *sp, *fp))
+
+    def advect_fast_part_dev(self, part, dt, state_in, state_out, fields32):
+        """Half of a batched step of a region-sharded rank: part 1 the boundary pass, part 2 the
+        rest and the rank's own halo copies (ica_advect_fast_part_dev)."""
+        ntr = state_in["rhogq"].shape[0]
+        sp = [_ptr(state_in[k], np.float64)[0] for k in STATE_KEYS]
+        so = [_ptr(state_out[k], np.float64)[0] for k in STATE_KEYS]
+        fp = [_ptr(fields32[k], np.float32)[0] for k in FIELD_KEYS]
+        with self._ordered():
+            _check("ica_advect_fast_part_dev", lib().ica_advect_fast_part_dev(self.h, int(part), int(ntr),
+                                                                              C.c_double(dt), *sp, *so, *fp))
+
+    def shard_set(self, l0, l1, poles, dst=None, src=None):
+        """This context computes regions [l0, l1) (and the pole centres if poles), with the halo
+        copies dst <- src whose two points it owns; shard_set(None, ...) returns to the whole grid."""
+        if l0 is None:
+            _check("ica_shard_set", lib().ica_shard_set(self.h, 0, 0, 0, -1, None, None))
+            return
+        d = np.ascontiguousarray(dst, np.int32)
+        s = np.ascontiguousarray(src, np.int32)
+        ip = C.POINTER(C.c_int)
+        _check("ica_shard_set", lib().ica_shard_set(self.h, int(l0), int(l1), int(bool(poles)), int(d.size),
+                                                    d.ctypes.data_as(ip), s.ctypes.data_as(ip)))
+
+    def shard_bval(self, ntr, bidx, buf, unpack):
+        fn = lib().ica_shard_bval_unpack if unpack else lib().ica_shard_bval_pack
+        with self._ordered():
+            _check("ica_shard_bval", fn(self.h, int(ntr), int(bidx.numel()), C.c_void_p(bidx.data_ptr()),
+                                        C.c_void_p(buf.data_ptr())))
+
+    def shard_points(self, pts, var, var_pl, buf, unpack):
+        fn = lib().ica_shard_points_unpack if unpack else lib().ica_shard_points_pack
+        vmax, kmax = int(var.shape[0]), int(var.shape[2])
+        with self._ordered():
+            _check("ica_shard_points", fn(self.h, int(pts.numel()), C.c_void_p(pts.data_ptr()), kmax, vmax,
+                                          C.c_void_p(var.data_ptr()), C.c_void_p(var_pl.data_ptr()),
+                                          C.c_void_p(buf.data_ptr())))
 
     def fast_shapes(self):
         n = C.c_int()

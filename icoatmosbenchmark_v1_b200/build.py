@@ -33,6 +33,7 @@ SOURCES = {
     "fast_kernels.cu": [],
     "noalloc.cu": [],
     "adjoint.cu": ["--fmad=false"],
+    "geometry.cu": ["--fmad=false"],
 }
 
 

@@ -242,6 +242,8 @@ Ctx::~Ctx() {
                   (void *)fast.seam_id})
     if (p) cudaFree(p);
   for (auto &ev : fast.events) cudaEventDestroy(ev.first), cudaEventDestroy(ev.second);
+  if (fast.local.dst) cudaFree(fast.local.dst);
+  if (fast.local.src) cudaFree(fast.local.src);
   if (stream) cudaStreamDestroy(stream);
   if (copy_in) cudaStreamDestroy(copy_in);
   if (copy_out) cudaStreamDestroy(copy_out);
@@ -1075,6 +1077,9 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt, bool f64) {
   I.err = fast.err;
   I.work_next = (unsigned long long *)buf("fast_work_next", sizeof(unsigned long long));
   if (!I.work_next) return set_error("cudaMalloc(fast work counter)"), ICA_ERR_NOMEM;
+  I.l0 = fast.sharded ? fast.l0 : 0;
+  I.l1 = fast.sharded ? fast.l1 : sz.lall;
+  I.poles = fast.sharded ? fast.poles : 1;
   return ICA_OK;
 }
 
@@ -1172,7 +1177,8 @@ template <typename F>
 static int advect_fast_impl(Ctx *c, int ntr, double dt, const double *rhog_in, const double *rhog_in_pl,
                             const double *rhogq_in, const double *rhogq_in_pl, double *rhog_out, double *rhog_out_pl,
                             double *rhogq_out, double *rhogq_out_pl, const F *vx, const F *vx_pl, const F *vy,
-                            const F *vy_pl, const F *vz, const F *vz_pl, const F *w, const F *w_pl) {
+                            const F *vy_pl, const F *vz, const F *vz_pl, const F *w, const F *w_pl,
+                            unsigned parts = 3u) {
   if (ntr < 1 || !rhog_in || !rhog_in_pl || !rhogq_in || !rhogq_in_pl || !rhog_out || !rhog_out_pl || !rhogq_out ||
       !rhogq_out_pl || !vx || !vx_pl || !vy || !vy_pl || !vz || !vz_pl || !w || !w_pl)
     return set_error("ica_advect_fast: NULL argument"), ICA_ERR_ARG;
@@ -1191,12 +1197,14 @@ static int advect_fast_impl(Ctx *c, int ntr, double dt, const double *rhog_in, c
     cudaEventCreate(&e1);
     c->fast.events.push_back({e0, e1});
   }
-  cudaError_t e = fast_step(I, c->fast.shape, c->stream, e0, e1, c->launches);
+  cudaError_t e = fast_step(I, c->fast.shape, c->stream, e0, e1, c->launches, parts);
   if (e != cudaSuccess) return cuda_fail(e, "ica_advect_fast");
-  const Plan &p = c->plan[0];
-  launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, 1, rhog_out, rhog_out_pl, c->stream);
-  launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, ntr, rhogq_out, rhogq_out_pl, c->stream);
-  c->launches += 2;
+  if (parts & 2u) {  // the halo fill of the new state (a sharded rank: its own copies only)
+    const Plan &p = c->fast.sharded ? c->fast.local : c->plan[0];
+    launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, 1, rhog_out, rhog_out_pl, c->stream);
+    launch_gather<double>(c->D, p.n, p.dst, p.src, c->sz.kall, ntr, rhogq_out, rhogq_out_pl, c->stream);
+    c->launches += 2;
+  }
   return c->check_launch("ica_advect_fast");
 }
 
@@ -1305,6 +1313,91 @@ int ica_advect_fast_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, c
                                  rhogq_out, rhogq_out_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl);
 }
 
+int ica_advect_fast_part_dev(ica_ctx *c, int part, int ntr, double dt, const double *rhog_in,
+                             const double *rhog_in_pl, const double *rhogq_in, const double *rhogq_in_pl,
+                             double *rhog_out, double *rhog_out_pl, double *rhogq_out, double *rhogq_out_pl,
+                             const float *vx, const float *vx_pl, const float *vy, const float *vy_pl, const float *vz,
+                             const float *vz_pl, const float *w, const float *w_pl) {
+  CTX_OK(c);
+  if (part != 1 && part != 2) return set_error("ica_advect_fast_part_dev: part must be 1 or 2"), ICA_ERR_ARG;
+  return advect_fast_impl<float>(c, ntr, dt, rhog_in, rhog_in_pl, rhogq_in, rhogq_in_pl, rhog_out, rhog_out_pl,
+                                 rhogq_out, rhogq_out_pl, vx, vx_pl, vy, vy_pl, vz, vz_pl, w, w_pl,
+                                 part == 1 ? 1u : 2u);
+}
+
+int ica_shard_set(ica_ctx *c, int l0, int l1, int poles, int nlocal, const int *dst, const int *src) {
+  CTX_OK(c);
+  int rc = c->need_grid("ica_shard_set");
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  FastState &f = c->fast;
+  if (nlocal < 0) {  // back to the whole grid
+    f.sharded = false;
+    return ICA_OK;
+  }
+  const int npt = c->sz.lall * c->sz.gall + kLallPl * kGallPl;
+  if (l0 < 0 || l1 > c->sz.lall || l1 <= l0 || (nlocal > 0 && (!dst || !src)))
+    return set_error("ica_shard_set: bad region range or copy list"), ICA_ERR_ARG;
+  for (int e = 0; e < nlocal; ++e)
+    if (dst[e] < 0 || dst[e] >= npt || src[e] < 0 || src[e] >= npt)
+      return set_error("ica_shard_set: copy list point out of range"), ICA_ERR_ARG;
+  if (f.local.dst) cudaFree(f.local.dst);
+  if (f.local.src) cudaFree(f.local.src);
+  f.local = Plan{};
+  if (cudaMalloc(&f.local.dst, sizeof(int) * (nlocal + 1)) != cudaSuccess ||
+      cudaMalloc(&f.local.src, sizeof(int) * (nlocal + 1)) != cudaSuccess)
+    return set_error("cudaMalloc(shard copy list)"), ICA_ERR_NOMEM;
+  cudaError_t e = cudaMemcpy(f.local.dst, dst, sizeof(int) * nlocal, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(f.local.src, src, sizeof(int) * nlocal, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_shard_set");
+  f.local.n = nlocal;
+  f.sharded = true;
+  f.l0 = l0, f.l1 = l1, f.poles = poles ? 1 : 0;
+  return ICA_OK;
+}
+
+static int shard_bval(ica_ctx *c, int ntr, int n, const int *bidx, double *buf, bool unpack) {
+  CTX_OK(c);
+  int rc = c->need_grid("ica_shard_bval");
+  if (rc) return rc;
+  if (ntr < 1 || n < 0 || (n > 0 && (!bidx || !buf))) return set_error("ica_shard_bval: bad argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  rc = c->build_fast_tables();
+  if (rc) return rc;
+  double *bbuf = (double *)c->buf("fast_bbuf", (size_t)ntr * c->sz.kall * c->fast.nb * 5 * sizeof(double));
+  if (!bbuf) return set_error("cudaMalloc(fast boundary buffer)"), ICA_ERR_NOMEM;
+  cudaError_t e = shard_bval_copy(bidx, n, c->fast.nb, c->sz.kall, ntr, bbuf, buf, unpack, c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_shard_bval");
+  c->launches += n > 0;
+  return c->check_launch("ica_shard_bval");
+}
+int ica_shard_bval_pack(ica_ctx *c, int ntr, int n, const int *bidx, double *buf) {
+  return shard_bval(c, ntr, n, bidx, buf, false);
+}
+int ica_shard_bval_unpack(ica_ctx *c, int ntr, int n, const int *bidx, const double *buf) {
+  return shard_bval(c, ntr, n, bidx, const_cast<double *>(buf), true);
+}
+
+static int shard_points(ica_ctx *c, int n, const int *pts, int kmax, int vmax, double *var, double *var_pl, double *buf,
+                        bool unpack) {
+  CTX_OK(c);
+  if (n < 0 || kmax < 1 || vmax < 1 || (n > 0 && (!pts || !var || !var_pl || !buf)))
+    return set_error("ica_shard_points: bad argument"), ICA_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaError_t e = shard_point_copy(pts, n, c->sz.lall, c->sz.gall, kmax, vmax, var, var_pl, buf, unpack, c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ica_shard_points");
+  c->launches += n > 0;
+  return c->check_launch("ica_shard_points");
+}
+int ica_shard_points_pack(ica_ctx *c, int n, const int *pts, int kmax, int vmax, const double *var,
+                          const double *var_pl, double *buf) {
+  return shard_points(c, n, pts, kmax, vmax, const_cast<double *>(var), const_cast<double *>(var_pl), buf, false);
+}
+int ica_shard_points_unpack(ica_ctx *c, int n, const int *pts, int kmax, int vmax, double *var, double *var_pl,
+                            const double *buf) {
+  return shard_points(c, n, pts, kmax, vmax, var, var_pl, const_cast<double *>(buf), true);
+}
+
 int ica_advect_fast64_dev(ica_ctx *c, int ntr, double dt, const double *rhog_in, const double *rhog_in_pl,
                           const double *rhogq_in, const double *rhogq_in_pl, double *rhog_out, double *rhog_out_pl,
                           double *rhogq_out, double *rhogq_out_pl, const double *vx, const double *vx_pl,
@@ -1343,6 +1436,7 @@ static int batch_insts(ica_batch *b, const Args *args, MultiInst &M) {
     Ctx *c = b->ctx[i];
     const Args &a = args[i];
     if (!fast_args_ok(a)) return set_error("ica_batch: bad arguments of instance " + std::to_string(i)), ICA_ERR_ARG;
+    if (c->fast.sharded) return set_error("ica_batch: instance " + std::to_string(i) + " is a sharded context"), ICA_ERR_STATE;
     c->fast.shape = b->shape;
     FastInst &I = M.inst[i];
     const int rc = c->fast_inst(I, a.ntr, a.dt, f64);

@@ -38,6 +38,11 @@ struct FastState {  // fused path: boundary tables, tile shape, kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
   int *err = nullptr;  // device status word of the batched kernels (a buffer of the context)
+  // region-sharded run (ica_shard_set): this context computes regions [l0, l1) and, with
+  // poles, the pole centres; `local` holds the halo copies whose two points it owns
+  bool sharded = false;
+  int l0 = 0, l1 = 0, poles = 1;
+  Plan local;
 };
 
 struct FastInst;

@@ -56,7 +56,17 @@ struct FastInst {
   double4 *dupc64;  // dupc in FP64 (FP64 variant)
   unsigned long long *work_next;  // work-item counter of the persistent horizontal kernel
   int *err;  // device status word: bit 0 = a bounded wait of the horizontal kernel gave up
+  // the regions [l0, l1) this instance computes (a rank of a region-sharded run; the whole
+  // grid otherwise), and whether it computes the two pole centres
+  int l0, l1, poles;
 };
+
+// Is point p (region point l*gall + ij, or a pole point after them) computed by instance I?
+__device__ __forceinline__ bool owns_point(const FastInst &I, int p) {
+  if (p >= I.lall * I.gall) return I.poles != 0;
+  const int l = p / I.gall;
+  return l >= I.l0 && l < I.l1;
+}
 
 // TMA descriptors of one instance's tile windows (built on the host per step, since the state
 // buffers alternate): rhogq_in as (i, j, l*K + k, tracer) FP64 and rhog_in as (i, j, l*K + k).

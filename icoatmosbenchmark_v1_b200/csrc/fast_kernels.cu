@@ -119,6 +119,7 @@ __global__ void k_fast_boundary(const __grid_constant__ MultiInst M) {
   const int b = (int)(tid % I.nb);
   const int k = 1 + (int)(tid / I.nb);
   const int p = I.blist[b];
+  if (!owns_point(I, p)) return;  // another rank's boundary cell or pole centre
   const size_t tstride = (size_t)I.lall * I.K * I.gall;
   double *dst0 = I.bbuf + ((size_t)k * I.nb + b) * 5;
   const size_t dstride = (size_t)I.K * I.nb * 5;  // next tracer
@@ -264,6 +265,7 @@ __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
   const int sidx = (int)(tid % I.ns), k = 1 + (int)(tid / I.ns);
   const int code = I.seam_list[sidx];
   const int a = code % 3 + 1, p = code / 3;
+  if (!owns_point(I, p)) return;  // a face of another rank's region
   const int l = p / I.gall, c = p % I.gall;
   const int G = I.G, i = c % G + 1, j = c / G + 1;
   const bool sgp = I.have_sgp[l] != 0;
@@ -379,7 +381,7 @@ template <typename R>
 __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
   using A = Arith<R>;
   long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int ii = find_inst(M, w, [](const FastInst &I) { return (long long)I.lall * (I.K - 2) * I.gall; });
+  const int ii = find_inst(M, w, [](const FastInst &I) { return (long long)(I.l1 - I.l0) * (I.K - 2) * I.gall; });
   if (ii < 0) return;
   const FastInst &I = M.inst[ii];
   // 32-bit index arithmetic (a 64-bit division is several times the cost of this thread's
@@ -387,7 +389,7 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
   const unsigned wu = (unsigned)w, gall = (unsigned)I.gall, kin = (unsigned)(I.K - 2), Gu = (unsigned)I.G;
   const int G = I.G, c = (int)(wu % gall);
   const unsigned lk = wu / gall;
-  const int k = 1 + (int)(lk % kin), l = (int)(lk / kin);
+  const int k = 1 + (int)(lk % kin), l = I.l0 + (int)(lk / kin);
   const int i = (int)((unsigned)c % Gu) + 1, j = (int)((unsigned)c / Gu) + 1;
   const size_t n3 = (size_t)I.lall * I.K * I.gall, o = ((size_t)l * I.K + k) * I.gall + c;
   const R dtf = (R)I.dt;
@@ -772,8 +774,39 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
   const int st7[7] = {ew, ew + 1, ew + WW + 1, ew + WW, ew - 1, ew - WW - 1, ew - WW};
   const int fslot[7] = {0, tid, tid, tid, tid - 1, tid - RW - 1, tid - RW};  // owner thread of face m
   auto cx = [](const V2 &v, int h) { return h ? v.y : v.x; };
+  // global values a batch reads that nothing stages: the FP64 boundary values of a region-boundary
+  // cell (5 per tracer) and the seam faces' values; they come from DRAM (bbuf and sval are
+  // larger than L2), so the next batch's are prefetched into L1 one batch ahead
+  auto prefetch_batch = [&](int tb) {
+    const int nt = min(TB, ntr - tb);
+    if (c_int && !tile_cell) {
+#pragma unroll
+      for (int tt = 0; tt < TB; ++tt)
+        if (tt < nt) {
+          const double *bv = bval(I, tb + tt, k, bs);
+          asm volatile("prefetch.global.L1 [%0];\n" ::"l"(bv));
+          asm volatile("prefetch.global.L1 [%0];\n" ::"l"(bv + 4));
+        }
+    }
+    if (seam_own) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if ((seam_own >> a) & 1u) {
+          const int sid = I.seam_id[((size_t)l * I.gall + ccell) * 3 + a];
+#pragma unroll
+          for (int tt = 0; tt < TB; ++tt)
+            if (tt < nt) {
+              const void *pv = (sizeof(R) == 8) ? (const void *)(I.sval64 + ((size_t)(tb + tt) * K + k) * I.ns + sid)
+                                                : (const void *)(I.sval + ((size_t)(tb + tt) * K + k) * I.ns + sid);
+              asm volatile("prefetch.global.L1 [%0];\n" ::"l"(pv));
+            }
+        }
+    }
+  };
+  prefetch_batch(0);
   for (int t0 = 0, b = 0; t0 < ntr; t0 += TB, ++b) {
     const int ntg = min(TB, ntr - t0);
+    if (t0 + TB < ntr) prefetch_batch(t0 + TB);
     // ---- (B) per interior ring cell and tracer: gradient and Qout (formed here, or the FP64
     // boundary values of a region-boundary cell), the 4-point bounds of its 6 faces, and the
     // limited value of each of its outflow faces; owners fill their seam and absent faces
@@ -940,9 +973,10 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
     __syncthreads();
     long long wi = s_item;
     if (wi >= nwork) break;
-    const int ii = find_inst(M, wi, [](const FastInst &J) { return (long long)J.lall * J.ntx * J.nty * (J.K - 2); });
-    const int ntl = M.inst[ii].lall * M.inst[ii].ntx * M.inst[ii].nty;
-    const int tile = (int)(wi % ntl), k = 1 + (int)(wi / ntl);
+    const int ii =
+        find_inst(M, wi, [](const FastInst &J) { return (long long)(J.l1 - J.l0) * J.ntx * J.nty * (J.K - 2); });
+    const int tpr = M.inst[ii].ntx * M.inst[ii].nty, ntl = (M.inst[ii].l1 - M.inst[ii].l0) * tpr;
+    const int tile = M.inst[ii].l0 * tpr + (int)(wi % ntl), k = 1 + (int)(wi / ntl);
     bool ok;
     switch (ii) {
       case 0: ok = horiz_item<TX, TY, TB, R>(M.inst[0], &T.m[0], tile, k, s, phase); break;
@@ -963,7 +997,7 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
   auto &s = tile_smem<TX, TY, TB, R>(smem_raw);
   tile_smem_init(s);
   unsigned phase = 0;
-  horiz_item<TX, TY, TB, R>(I, &T, (int)blockIdx.x, 1 + (int)blockIdx.y, s, phase);
+  horiz_item<TX, TY, TB, R>(I, &T, I.l0 * I.ntx * I.nty + (int)blockIdx.x, 1 + (int)blockIdx.y, s, phase);
 }
 
 // ---- vertical sub-step: one thread per (interior column, TV tracers), streaming the
@@ -981,8 +1015,8 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
   const int ntv = min(TV, I.ntr - t0);
   const int n = I.gmax - I.gmin + 1;
   const long long col = (blk / ngr) * blockDim.x + threadIdx.x;
-  if (col >= (long long)I.lall * n * n) return;
-  const int l = (int)(col / ((long long)n * n)), r = (int)(col % ((long long)n * n));
+  if (col >= (long long)(I.l1 - I.l0) * n * n) return;
+  const int l = I.l0 + (int)(col / ((long long)n * n)), r = (int)(col % ((long long)n * n));
   const int i = I.gmin + r % n, j = I.gmin + r / n;
   const int K = I.K;
   const size_t slab = (size_t)I.gall, tstride = (size_t)I.lall * K * slab;
@@ -1124,7 +1158,7 @@ __global__ void __launch_bounds__(256, 2) k_fast_vert(const __grid_constant__ Mu
   // blocks of an instance: (tracer group fastest, column block)
   long long blk = blockIdx.x;
   const int ii = find_inst(M, blk, [](const FastInst &J) {
-    const long long nc = (long long)J.lall * (J.gmax - J.gmin + 1) * (J.gmax - J.gmin + 1);
+    const long long nc = (long long)(J.l1 - J.l0) * (J.gmax - J.gmin + 1) * (J.gmax - J.gmin + 1);
     return (long long)((J.ntr + TV - 1) / TV) * ((nc + 255) / 256);
   });
   switch (ii) {
@@ -1144,7 +1178,7 @@ __global__ void __launch_bounds__(256, 2) k_fast_vert(const __grid_constant__ Mu
 template <int KMAX>
 __global__ void __launch_bounds__(KMAX) k_fast_pole(const __grid_constant__ MultiInst M) {
   long long tl = blockIdx.x;
-  const int ii = find_inst(M, tl, [](const FastInst &J) { return (long long)kLallPl * J.ntr; });
+  const int ii = find_inst(M, tl, [](const FastInst &J) { return J.poles ? (long long)kLallPl * J.ntr : 0LL; });
   if (ii < 0) return;  // whole CTA
   const FastInst &I = M.inst[ii];
   const int t = (int)tl;
@@ -1260,7 +1294,7 @@ __global__ void k_fast_carry(const __grid_constant__ MultiInst M) {
   if (ii < 0) return;
   const FastInst &I = M.inst[ii];
   const int p = I.carry[tid % I.ncarry], k = (int)(tid / I.ncarry);
-  if (p < 0) return;
+  if (p < 0 || !owns_point(I, p)) return;
   const int l = p / I.gall, c = p % I.gall;
   const size_t off = ((size_t)l * I.K + k) * I.gall + c, tstride = (size_t)I.lall * I.K * I.gall;
   I.rho_out[off] = I.rho_in[off];
@@ -1339,10 +1373,11 @@ static cudaError_t launch_tile_n(const MultiInst &M, cudaStream_t st) {
     if (e != cudaSuccess) return e;
   }
   long long nwork = 0;
-  for (int i = 0; i < M.n; ++i) nwork += (long long)M.inst[i].lall * M.inst[i].ntx * M.inst[i].nty * (M.inst[i].K - 2);
+  for (int i = 0; i < M.n; ++i)
+    nwork += (long long)(M.inst[i].l1 - M.inst[i].l0) * M.inst[i].ntx * M.inst[i].nty * (M.inst[i].K - 2);
   if (ONE) {
     const FastInst &I = M.inst[0];
-    k_fast_horiz1<TX, TY, TB, R><<<dim3((unsigned)(I.lall * I.ntx * I.nty), (unsigned)(I.K - 2)), NT, smem, st>>>(
+    k_fast_horiz1<TX, TY, TB, R><<<dim3((unsigned)((I.l1 - I.l0) * I.ntx * I.nty), (unsigned)(I.K - 2)), NT, smem, st>>>(
         I, T.m[0]);
   } else {
     const long long grid = nwork < (long long)nsm * per_sm[dev] ? nwork : (long long)nsm * per_sm[dev];
@@ -1379,28 +1414,37 @@ cudaError_t fast_build_offsets64(const FastInst &I, double *off, cudaStream_t st
 }
 
 cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
-                            long long &launches) {
+                            long long &launches, unsigned parts) {
   if (M.n < 1 || M.n > kMaxInst) return cudaErrorInvalidValue;
+  for (int i = 0; i < M.n; ++i)
+    if (M.inst[i].l0 < 0 || M.inst[i].l1 > M.inst[i].lall || M.inst[i].l1 <= M.inst[i].l0) return cudaErrorInvalidValue;
   long long nbk = 0, nsk = 0, npl = 0, nc = 0, nvb = 0, nvb64 = 0, nfk = 0;
   int kmax = 0;
   constexpr int TV = 4, TV64 = 2;  // tracers per column thread: FP32, FP64 variant
   for (int i = 0; i < M.n; ++i) {
     const FastInst &I = M.inst[i];
-    const long long n = I.gmax - I.gmin + 1, ncol = (long long)I.lall * n * n;
+    const long long n = I.gmax - I.gmin + 1, ncol = (long long)(I.l1 - I.l0) * n * n;
     nbk += (long long)I.nb * (I.K - 2);
     nsk += (long long)I.ns * (I.K - 2);
-    nfk += (long long)I.lall * (I.K - 2) * I.gall;
-    npl += (long long)kLallPl * I.ntr;
+    nfk += (long long)(I.l1 - I.l0) * (I.K - 2) * I.gall;
+    npl += I.poles ? (long long)kLallPl * I.ntr : 0LL;
     nc += (long long)I.ncarry * I.K;
     nvb += (long long)((I.ntr + TV - 1) / TV) * ((ncol + 255) / 256);
     nvb64 += (long long)((I.ntr + TV64 - 1) / TV64) * ((ncol + 255) / 256);
     kmax = I.K > kmax ? I.K : kmax;
   }
-  k_fast_boundary<<<(unsigned)((nbk + 127) / 128), 128, 0, st>>>(M);
+  if (kmax > 128) return cudaErrorInvalidValue;
+  if (parts & 1u) {  // the boundary values other regions read (exchanged between ranks when sharded)
+    k_fast_boundary<<<(unsigned)((nbk + 127) / 128), 128, 0, st>>>(M);
+    launches += 1;
+  }
+  if (!(parts & 2u)) return cudaGetLastError();
   k_fast_seam<<<(unsigned)((nsk + 127) / 128), 128, 0, st>>>(M);
-  if (kmax <= 64) k_fast_pole<64><<<(unsigned)npl, 64, 0, st>>>(M);
-  else if (kmax <= 128) k_fast_pole<128><<<(unsigned)npl, 128, 0, st>>>(M);
-  else return cudaErrorInvalidValue;
+  if (npl > 0) {
+    if (kmax <= 64) k_fast_pole<64><<<(unsigned)npl, 64, 0, st>>>(M);
+    else k_fast_pole<128><<<(unsigned)npl, 128, 0, st>>>(M);
+    launches += 1;
+  }
   if (ev0) cudaEventRecord(ev0, st);
   const bool f64 = M.inst[0].f64 != 0;
   for (int i = 1; i < M.n; ++i)
@@ -1435,16 +1479,63 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
     else k_fast_vert<TV64, double><<<(unsigned)nvb64, 256, 0, st>>>(M);
   }
   k_fast_carry<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(M);
-  launches += 7;
+  launches += 5;
   return cudaGetLastError();
 }
 
 cudaError_t fast_step(const FastInst &I, int shape, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
-                      long long &launches) {
+                      long long &launches, unsigned parts) {
   MultiInst M;
   M.n = 1;
   M.inst[0] = I;
-  return fast_step_multi(M, shape, st, ev0, ev1, launches);
+  return fast_step_multi(M, shape, st, ev0, ev1, launches, parts);
+}
+
+// ---- region-sharded runs: the exchanges' pack and unpack (contiguous buffers, no peer access)
+__global__ void k_bval_copy(const int *bidx, int n, int nb, int K, int ntr, double *bbuf, double *buf, int unpack) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * K * ntr * 5) return;
+  const int v = (int)(t % 5);
+  long long r = t / 5;
+  const int e = (int)(r % n);
+  r /= n;  // = tr * K + k
+  double *a = bbuf + ((size_t)r * nb + bidx[e]) * 5 + v;
+  double *b = buf + ((size_t)r * n + e) * 5 + v;
+  if (unpack) *a = *b;
+  else *b = *a;
+}
+cudaError_t shard_bval_copy(const int *bidx, int n, int nb, int K, int ntr, double *bbuf, double *buf, bool unpack,
+                            cudaStream_t st) {
+  const long long total = (long long)n * K * ntr * 5;
+  if (total == 0) return cudaSuccess;
+  k_bval_copy<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(bidx, n, nb, K, ntr, bbuf, buf, unpack ? 1 : 0);
+  return cudaGetLastError();
+}
+// points p of a (vmax, lall, kmax, gall) array and its (vmax, 2, kmax, 6) pole array <-> buf (vmax, kmax, n)
+__global__ void k_point_copy(const int *pts, int n, int lall, int gall, int kmax, int vmax, double *var,
+                             double *var_pl, double *buf, int unpack) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * kmax * vmax) return;
+  const int e = (int)(t % n);
+  const int k = (int)((t / n) % kmax), v = (int)(t / ((long long)n * kmax));
+  const int p = pts[e];
+  double *a;
+  if (p < lall * gall) a = var + (((size_t)v * lall + p / gall) * kmax + k) * gall + p % gall;
+  else {
+    const int q = p - lall * gall;
+    a = var_pl + (((size_t)v * kLallPl + q / kGallPl) * kmax + k) * kGallPl + q % kGallPl;
+  }
+  double *b = buf + ((size_t)v * kmax + k) * n + e;
+  if (unpack) *a = *b;
+  else *b = *a;
+}
+cudaError_t shard_point_copy(const int *pts, int n, int lall, int gall, int kmax, int vmax, double *var,
+                             double *var_pl, double *buf, bool unpack, cudaStream_t st) {
+  const long long total = (long long)n * kmax * vmax;
+  if (total == 0) return cudaSuccess;
+  k_point_copy<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(pts, n, lall, gall, kmax, vmax, var, var_pl, buf,
+                                                                unpack ? 1 : 0);
+  return cudaGetLastError();
 }
 
 }  // namespace icoadv

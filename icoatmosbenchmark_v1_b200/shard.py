@@ -115,3 +115,187 @@ class ShardPlan:
         nb = sum(v.size for v in self.bval_recv.values())
         nh = sum(v[0].size for v in self.halo_recv.values())
         return nb * 5 * 8 * kall * ntr, nh * 8 * kall * (ntr + 1)
+
+
+# ---- the device side: a rank's part of the step and its two exchanges ------------------------
+class LibraryBackend:
+    """Pack / unpack of the exchanges with the library's kernels on one context's device buffers
+    (ica_shard_bval_pack/unpack, ica_shard_points_pack/unpack): contiguous buffers, no peer access."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+
+    def pack_bval(self, ntr, kall, bidx):
+        import torch
+        buf = torch.empty((ntr, kall, bidx.numel(), 5), dtype=torch.float64, device=bidx.device)
+        self.ctx.shard_bval(ntr, bidx, buf, unpack=False)
+        return buf
+
+    def unpack_bval(self, ntr, kall, bidx, buf):
+        self.ctx.shard_bval(ntr, bidx, buf, unpack=True)
+
+    def pack_points(self, pts, var, var_pl):
+        import torch
+        vmax, kmax = var.shape[0], var.shape[2]
+        buf = torch.empty((vmax, kmax, pts.numel()), dtype=torch.float64, device=pts.device)
+        self.ctx.shard_points(pts, var, var_pl, buf, unpack=False)
+        return buf
+
+    def unpack_points(self, pts, var, var_pl, buf):
+        self.ctx.shard_points(pts, var, var_pl, buf, unpack=True)
+
+
+class TorchBackend:
+    """The same pack / unpack as torch index operations on a rank's arrays (any device): the boundary
+    values live in `bbuf` (ntr, kall, nb, 5); points index region arrays (vmax, lall, kmax, gall)
+    and pole arrays (vmax, 2, kmax, 6) as the flat point numbering does."""
+
+    def __init__(self, bbuf=None):
+        self.bbuf = bbuf
+
+    def pack_bval(self, ntr, kall, bidx):
+        return self.bbuf[:, :, bidx.long()].clone()
+
+    def unpack_bval(self, ntr, kall, bidx, buf):
+        self.bbuf[:, :, bidx.long()] = buf
+
+    @staticmethod
+    def _flat(var, var_pl):
+        import torch
+        m, L, K, G = var.shape
+        return torch.cat([var.permute(0, 2, 1, 3).reshape(m, K, L * G), var_pl.permute(0, 2, 1, 3).reshape(m, K, 12)], 2)
+
+    def pack_points(self, pts, var, var_pl):
+        return self._flat(var, var_pl)[:, :, pts.long()].contiguous()
+
+    def unpack_points(self, pts, var, var_pl, buf):
+        m, L, K, G = var.shape
+        f = self._flat(var, var_pl)
+        f[:, :, pts.long()] = buf
+        var.copy_(f[:, :, :L * G].reshape(m, K, L, G).permute(0, 2, 1, 3))
+        var_pl.copy_(f[:, :, L * G:].reshape(m, K, 2, 6).permute(0, 2, 1, 3))
+
+
+def p2p_exchange(sends, recvs, group=None):
+    """One exchange between ranks: sends {q: tensor} to each rank q and receives {q: tensor} (filled
+    in place) from each rank q, as one group of point-to-point operations (NCCL send/recv inside
+    ncclGroupStart/End on GPUs, gloo on CPUs).  Every rank lists its operations in rank order."""
+    import torch.distributed as dist
+    ops = []
+    for q in sorted(set(sends) | set(recvs)):
+        if q in sends:
+            ops.append(dist.P2POp(dist.isend, sends[q].contiguous(), q, group=group))
+        if q in recvs:
+            ops.append(dist.P2POp(dist.irecv, recvs[q], q, group=group))
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+    return recvs
+
+
+class ShardedRunner:
+    """One rank of a region-sharded batched step (ica_shard_set): the rank's part of the step in two
+    halves, with the boundary-value exchange between them and the halo exchange of the new state
+    after them.  The state is double-buffered (FP64), the fields FP32; every rank holds the whole
+    grid's arrays and computes its own regions (and rank 0 the pole centres).
+
+    step() runs the four phases with p2p_exchange over torch.distributed (one process per GPU);
+    the phase methods let one process drive several emulated ranks (each with its own context on
+    one GPU) and move their buffers itself."""
+
+    def __init__(self, ctx, plan, rank, state, fields, dt, group=None, backend=None):
+        import torch
+        self.ctx, self.plan, self.rank, self.dt, self.group = ctx, plan, rank, dt, group
+        self.backend = backend or LibraryBackend(ctx)
+        a0, a1 = plan.blocks[rank]
+        dst, src = plan.halo_local[rank]
+        ctx.shard_set(a0, a1, rank == 0, dst, src)
+        dev = state["rhog"].device
+        I = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.int32), device=dev)  # noqa: E731
+        self.bsend = {q: I(v) for (r, q2), v in plan.bval_recv.items() if q2 == rank for q in [r]}
+        self.brecv = {q: I(v) for (r, q), v in plan.bval_recv.items() if r == rank}
+        self.hsend = {q: I(v[1]) for (r, q2), v in plan.halo_recv.items() if q2 == rank for q in [r]}
+        self.hrecv = {q: I(v[0]) for (r, q), v in plan.halo_recv.items() if r == rank}
+        self.a = state
+        self.b = {k: torch.empty_like(v) for k, v in state.items()}
+        from .api import FIELD_KEYS
+        self.f32 = {k: fields[k].to(torch.float32).contiguous() for k in FIELD_KEYS}
+        self.ntr = int(state["rhogq"].shape[0])
+        self.kall = int(state["rhog"].shape[1])
+
+    @property
+    def state(self):
+        return self.a
+
+    # ---- phases
+    def part(self, p):
+        self.ctx.advect_fast_part_dev(p, self.dt, self.a, self.b, self.f32)
+
+    def bval_sends(self):
+        return {q: self.backend.pack_bval(self.ntr, self.kall, idx) for q, idx in self.bsend.items()}
+
+    def bval_recv_buffers(self):
+        import torch
+        dev = self.a["rhog"].device
+        return {q: torch.empty((self.ntr, self.kall, idx.numel(), 5), dtype=torch.float64, device=dev)
+                for q, idx in self.brecv.items()}
+
+    def bval_unpack(self, bufs):
+        for q, buf in bufs.items():
+            self.backend.unpack_bval(self.ntr, self.kall, self.brecv[q], buf)
+
+    def _state_vars(self, S):
+        return ((S["rhog"].unsqueeze(0), S["rhog_pl"].unsqueeze(0)), (S["rhogq"], S["rhogq_pl"]))
+
+    def halo_sends(self):
+        import torch
+        out = {}
+        for q, pts in self.hsend.items():
+            out[q] = torch.cat([self.backend.pack_points(pts, v, vp) for v, vp in self._state_vars(self.b)], 0)
+        return out
+
+    def halo_recv_buffers(self):
+        import torch
+        dev = self.a["rhog"].device
+        return {q: torch.empty((1 + self.ntr, self.kall, pts.numel()), dtype=torch.float64, device=dev)
+                for q, pts in self.hrecv.items()}
+
+    def halo_unpack(self, bufs):
+        for q, buf in bufs.items():
+            (r, rp), (t, tp) = self._state_vars(self.b)
+            self.backend.unpack_points(self.hrecv[q], r, rp, buf[:1])
+            self.backend.unpack_points(self.hrecv[q], t, tp, buf[1:])
+
+    def swap(self):
+        self.a, self.b = self.b, self.a
+
+    def step(self):
+        self.part(1)
+        self.bval_unpack(p2p_exchange(self.bval_sends(), self.bval_recv_buffers(), self.group))
+        self.part(2)
+        self.halo_unpack(p2p_exchange(self.halo_sends(), self.halo_recv_buffers(), self.group))
+        self.swap()
+
+
+def emulated_step(runners):
+    """One step of several ranks driven by one process (one GPU, a context per rank): each phase
+    runs on every rank before the next, and the exchanges copy each sender's packed buffer into
+    the receiver's buffer.  No kernel of one rank waits for another's."""
+    for r in runners:
+        r.part(1)
+    sends = [r.bval_sends() for r in runners]
+    for r in runners:
+        bufs = r.bval_recv_buffers()
+        for q, buf in bufs.items():
+            buf.copy_(sends[q][r.rank])
+        r.bval_unpack(bufs)
+    for r in runners:
+        r.part(2)
+    sends = [r.halo_sends() for r in runners]
+    for r in runners:
+        bufs = r.halo_recv_buffers()
+        for q, buf in bufs.items():
+            buf.copy_(sends[q][r.rank])
+        r.halo_unpack(bufs)
+    for r in runners:
+        r.swap()

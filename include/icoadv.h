@@ -102,6 +102,21 @@ int ica_set_geometry(ica_ctx *ctx,
                      const double *GMTR_t, const double *GMTR_t_pl,
                      const double *GMTR_a, const double *GMTR_a_pl);
 
+/* The grid and its metrics built on the device, for a whole-grid context (ica_init): the cell
+ * positions of this library's icosahedral grid (recursive bisection of the ten diamonds of the
+ * region table, radius `radius`) and from them the setup of the reference's dyn_metrics kernel,
+ * GMTR_p/t/a_setup (kernels/NICAM/dyn_metrics/src/mod_gmtr.f90:46-741) and OPRT_gradient_setup
+ * (dyn_metrics/src/mod_oprt.f90:499-734), with the halo fills of COMM.  Device arrays, written
+ * asynchronously on the context stream, in the layouts ica_set_geometry and
+ * ica_set_step_geometry read: GRD_x(gall,1,lall,3) GRD_x_pl(6,1,2,3), GRD_xr(gall,1,lall,3,3)
+ * GRD_xr_pl(6,1,2,3), GMTR_p(gall,1,lall,8) GMTR_p_pl(6,1,2,8), GMTR_t(gall,1,lall,2,5)
+ * GMTR_t_pl(6,1,2,5), GMTR_a(gall,1,lall,3,12) GMTR_a_pl(6,1,2,18), coef_grad(gall,0:6,3,lall)
+ * coef_grad_pl(0:5,3,2).  Context scratch: about 9 doubles per cell. */
+int ica_grid_build_dev(ica_ctx *ctx, double radius,
+                       double *GRD_x, double *GRD_x_pl, double *GRD_xr, double *GRD_xr_pl,
+                       double *GMTR_p, double *GMTR_p_pl, double *GMTR_t, double *GMTR_t_pl,
+                       double *GMTR_a, double *GMTR_a_pl, double *coef_grad, double *coef_grad_pl);
+
 /* ---- horizontal_flux: kernels/NICAM/dyn_horiz_adv_flux/src/mod_src_tracer.f90:42-49,78-90
  * out flx_h(gall,kall,lall,6) flx_h_pl(6,kall,2)
  *     GRD_xc(gall,kall,lall,3,3) GRD_xc_pl(6,kall,2,3)
@@ -342,6 +357,40 @@ int ica_advect_fast(ica_ctx *ctx, int ntr, double dt,
                     const float *rhogvy, const float *rhogvy_pl,
                     const float *rhogvz, const float *rhogvz_pl,
                     const float *rhogw, const float *rhogw_pl);
+/* ---- Region sharding of the batched step over ranks (one process and GPU per rank).  Every
+ * rank holds the whole grid's arrays and computes a contiguous block of regions [l0, l1) (the
+ * reference's region order, mod_adm.f90:791-801), rank 0 also the two pole centres
+ * (mod_adm.f90:190).  Within a step one region reads another's values in two places, and
+ * each becomes an exchange: the boundary values (gradient and Qout of the cells other
+ * regions' halos copy, 5 values per tracer and level) after the boundary pass, and the halo
+ * fill of the new state.  The caller moves the packed buffers between ranks (NCCL send/recv
+ * through torch.distributed in icoatmosbenchmark_v1_b200/shard.py); nothing reads another
+ * GPU's memory.
+ * ica_shard_set: this context computes regions [l0, l1) (0-based) and, if poles, the pole
+ * centres; dst/src[nlocal] (host arrays, points numbered as in ica_comm_plan) are the halo
+ * copies whose two points it owns.  nlocal < 0 returns the context to the whole grid.
+ * ica_advect_fast_part_dev: part 1 runs the boundary pass, part 2 the rest of the step and
+ * the local halo copies; arguments as ica_advect_fast_dev. */
+int ica_shard_set(ica_ctx *ctx, int l0, int l1, int poles, int nlocal, const int *dst, const int *src);
+int ica_advect_fast_part_dev(ica_ctx *ctx, int part, int ntr, double dt,
+                             const double *rhog_in, const double *rhog_in_pl,
+                             const double *rhogq_in, const double *rhogq_in_pl,
+                             double *rhog_out, double *rhog_out_pl,
+                             double *rhogq_out, double *rhogq_out_pl,
+                             const float *rhogvx, const float *rhogvx_pl,
+                             const float *rhogvy, const float *rhogvy_pl,
+                             const float *rhogvz, const float *rhogvz_pl,
+                             const float *rhogw, const float *rhogw_pl);
+/* Pack / unpack, device pointers, context stream: the boundary values of the boundary indices
+ * bidx[n] (as ica_boundary_tables numbers them) between the context's boundary buffer and
+ * buf(5, n, kall, ntr); the points pts[n] of var(gall,kmax,lall,vmax) + var_pl(6,kmax,2,vmax)
+ * and buf(n, kmax, vmax). */
+int ica_shard_bval_pack(ica_ctx *ctx, int ntr, int n, const int *bidx, double *buf);
+int ica_shard_bval_unpack(ica_ctx *ctx, int ntr, int n, const int *bidx, const double *buf);
+int ica_shard_points_pack(ica_ctx *ctx, int n, const int *pts, int kmax, int vmax,
+                          const double *var, const double *var_pl, double *buf);
+int ica_shard_points_unpack(ica_ctx *ctx, int n, const int *pts, int kmax, int vmax,
+                            double *var, double *var_pl, const double *buf);
 /* FP64 variant of the batched step: the same kernels with every face value, bound,
  * Courant number and limiter in FP64 and FP64 fields, so the result follows the plain
  * FP64 step to FP64 rounding (the FP32 variant differs from it at FP32 rounding). */

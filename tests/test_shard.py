@@ -198,3 +198,112 @@ def test_boundary_tables(built, glevel, rlevel):
     unwritten = halo.copy()
     unwritten[dst[rd]] = False
     assert (bsrc[unwritten] == -2).all()
+
+
+class _FakeCtx:
+    """Stands in for a sharded context on CPU: part 1 puts the rank's boundary values (those its
+    own regions and, on rank 0, the pole centres compute) into its boundary buffer, part 2 the
+    rank's own points of the next state, then the rank's own halo copies; the values come from a
+    whole-grid reference, so after the runner's exchanges every rank must hold the reference's
+    values wherever it reads."""
+
+    def __init__(self, ref_state, ref_bval, blist, gall, nrgn, backend):
+        self.ref, self.ref_b, self.blist, self.gall, self.nrgn, self.be = ref_state, ref_bval, blist, gall, nrgn, backend
+
+    def shard_set(self, l0, l1, poles, dst, src):
+        self.l0, self.l1, self.poles = l0, l1, poles
+        import torch
+        self.local = (torch.as_tensor(np.asarray(dst, np.int64)), torch.as_tensor(np.asarray(src, np.int64)))
+
+    def _own(self, pts):
+        pts = np.asarray(pts)
+        l = pts // self.gall
+        return np.where(pts >= self.nrgn * self.gall, bool(self.poles), (l >= self.l0) & (l < self.l1))
+
+    def advect_fast_part_dev(self, part, dt, a, b, f):
+        import torch
+        if part == 1:
+            own = torch.as_tensor(self._own(self.blist))
+            self.be.bbuf[:, :, own] = self.ref_b[:, :, own]
+            return
+        npt = self.nrgn * self.gall + 12
+        own = torch.as_tensor(self._own(np.arange(npt)))
+        for k, kp in (("rhog", "rhog_pl"), ("rhogq", "rhogq_pl")):
+            v, vp = (b[k].unsqueeze(0), b[kp].unsqueeze(0)) if k == "rhog" else (b[k], b[kp])
+            rv, rvp = (self.ref[k].unsqueeze(0), self.ref[kp].unsqueeze(0)) if k == "rhog" else (self.ref[k], self.ref[kp])
+            fl = self.be._flat(v, vp)
+            fl[:, :, own] = self.be._flat(rv, rvp)[:, :, own]
+            fl[:, :, self.local[0]] = fl[:, :, self.local[1]]
+            m, L, K, G = v.shape
+            v.copy_(fl[:, :, :L * G].reshape(m, K, L, G).permute(0, 2, 1, 3))
+            vp.copy_(fl[:, :, L * G:].reshape(m, K, 2, 6).permute(0, 2, 1, 3))
+
+
+def _runner_worker(rank, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, str(ROOT))
+    import torch
+    import torch.distributed as dist
+    from icoatmosbenchmark_v1_b200 import api, shard
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    try:
+        g, rl, K, T = 4, 0, 5, 3
+        plan = shard.ShardPlan.build(g, rl, 2)
+        L, gall = plan.nrgn, plan.gall
+        nb, bsrc, blist, ring = api.boundary_tables(g, rl)
+        gen = torch.Generator().manual_seed(5)
+        # the whole-grid reference: any values, halos filled by the composed plan
+        ref = {"rhog": torch.rand((L, K, gall), generator=gen, dtype=torch.float64),
+               "rhog_pl": torch.rand((2, K, 6), generator=gen, dtype=torch.float64),
+               "rhogq": torch.rand((T, L, K, gall), generator=gen, dtype=torch.float64),
+               "rhogq_pl": torch.rand((T, 2, K, 6), generator=gen, dtype=torch.float64)}
+        dst, src = api.comm_plan(g, rl)
+        be0 = shard.TorchBackend()
+        for k, kp in (("rhog", "rhog_pl"), ("rhogq", "rhogq_pl")):
+            v, vp = (ref[k].unsqueeze(0), ref[kp].unsqueeze(0)) if k == "rhog" else (ref[k], ref[kp])
+            fl = be0._flat(v, vp)
+            fl[:, :, torch.as_tensor(dst.astype(np.int64))] = fl[:, :, torch.as_tensor(src.astype(np.int64))]
+            m = v.shape[0]
+            v.copy_(fl[:, :, :L * gall].reshape(m, K, L, gall).permute(0, 2, 1, 3))
+            vp.copy_(fl[:, :, L * gall:].reshape(m, K, 2, 6).permute(0, 2, 1, 3))
+        ref_b = torch.rand((T, K, nb, 5), generator=gen, dtype=torch.float64)
+        nan = lambda t: torch.full_like(t, float("nan"))  # noqa: E731
+        state = {k: nan(v) for k, v in ref.items()}
+        fields = {k: torch.zeros((L, K, gall) if not k.endswith("_pl") else (2, K, 6)) for k in api.FIELD_KEYS}
+        be = shard.TorchBackend(torch.full((T, K, nb, 5), float("nan"), dtype=torch.float64))
+        ctx = _FakeCtx(ref, ref_b, blist, gall, L, be)
+        run = shard.ShardedRunner(ctx, plan, rank, state, fields, 1.0, backend=be)
+        run.step()
+        S = run.state
+        # every point this rank owns (its regions' interior and halo, and on rank 0 the poles)
+        own = plan.owned_points(rank)
+        ok_state = all(torch.equal(be0._flat(*((S[k].unsqueeze(0), S[kp].unsqueeze(0)) if k == "rhog"
+                                                 else (S[k], S[kp])))[:, :, own],
+                                   be0._flat(*((ref[k].unsqueeze(0), ref[kp].unsqueeze(0)) if k == "rhog"
+                                               else (ref[k], ref[kp])))[:, :, own])
+                       for k, kp in (("rhog", "rhog_pl"), ("rhogq", "rhogq_pl")))
+        # every boundary value it reads
+        a0, a1 = plan.blocks[rank]
+        need = bsrc[a0 * gall:a1 * gall]
+        need = need[need >= 0]
+        if rank == 0:
+            need = np.concatenate([need, ring.ravel(), nb - 2 + np.arange(2)])
+        need = torch.as_tensor(np.unique(need).astype(np.int64))
+        ok_bval = torch.equal(be.bbuf[:, :, need], ref_b[:, :, need])
+        Path(out, f"r{rank}.json").write_text(json.dumps({"state": bool(ok_state), "bval": bool(ok_bval),
+                                                          "backend": dist.get_backend()}))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_runner_step_two_ranks_gloo(tmp_path, built):
+    """ShardedRunner.step on two gloo ranks (the CPU stand-in of NCCL): its boundary-value and
+    halo exchanges (p2p_exchange along the plan's lists, torch pack / unpack) leave each rank
+    with the whole-grid values at every point it owns and every boundary value it reads, bit
+    for bit."""
+    import torch.multiprocessing as mp
+    os.environ["CUDA_VISIBLE_DEVICES"] = ""
+    mp.start_processes(_runner_worker, args=(_port(), str(tmp_path)), nprocs=2, start_method="spawn", join=True)
+    for r in (0, 1):
+        d = json.loads((tmp_path / f"r{r}.json").read_text())
+        assert d == {"state": True, "bval": True, "backend": "gloo"}, (r, d)
