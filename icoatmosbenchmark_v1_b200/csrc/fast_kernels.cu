@@ -31,6 +31,7 @@
 
 #include <cfloat>
 #include <cstdint>
+#include <mutex>
 #include <type_traits>
 
 #include "fast_common.cuh"
@@ -1042,6 +1043,7 @@ __device__ __forceinline__ void vert_block(const FastInst &I, long long blk) {
   }
   V4 cnext = V[slab];
   double rnext = dens ? RH[slab] : 0.0;
+#pragma unroll 3
   for (int k = 1; k <= K - 2; ++k) {
     const V4 c = cnext;
     double Qk[TV];
@@ -1310,16 +1312,15 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
 
 static EncodeTiledFn encode_tiled() {
   static EncodeTiledFn fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  static std::once_flag once;
+  std::call_once(once, [] {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
       fn = (EncodeTiledFn)p;
     cudaGetLastError();
-  }
+  });
   return fn;
 }
 
