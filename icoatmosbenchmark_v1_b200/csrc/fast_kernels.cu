@@ -953,8 +953,11 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
 
 template <int TX, int TY, int TB, typename R>
 __device__ __forceinline__ TileSmem<TX, TY, TB, R> &tile_smem(unsigned char *raw) {
-  // the dynamic allocation carries 128 bytes of slack for this alignment (TMA destinations)
-  const size_t a = ((size_t)raw + 127) & ~(size_t)127;
+  // The dynamic allocation carries 128 bytes of slack for this alignment (TMA destinations).
+  // The offset is applied to the shared array itself, not through an integer round trip, so
+  // the compiler keeps the shared address space: every access of the tile is an LDS/STS with a
+  // 32-bit address instead of a generic load with a 64-bit one (5% of the kernel's time).
+  unsigned char *a = raw + ((128u - (smem_u32(raw) & 127u)) & 127u);
   return *reinterpret_cast<TileSmem<TX, TY, TB, R> *>(a);
 }
 
