@@ -1006,8 +1006,8 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt, bool f64) {
   if (rc0) return rc0;
   if (!geo_set || !stepgeo_set) return set_error("advect_fast: geometry not registered"), ICA_ERR_STATE;
   if (sz.kall < 4 || sz.kall > 128) return set_error("advect_fast: kall must be in [4, 128]"), ICA_ERR_ARG;
-  if ((long long)sz.lall * (sz.kall - 2) * sz.gall >= (1LL << 31))  // 32-bit cell-level indices in the kernels
-    return set_error("advect_fast: grid too large (lall * (kall - 2) * gall >= 2^31)"), ICA_ERR_ARG;
+  if (3LL * sz.lall * sz.kall * sz.gall >= (1LL << 31))  // 32-bit face-level indices in the kernels
+    return set_error("advect_fast: grid too large (3 * lall * kall * gall >= 2^31)"), ICA_ERR_ARG;
   int rc = build_fast_tables();
   if (rc) return rc;
   int tx[16], ty[16], tg[16];
@@ -1027,7 +1027,7 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt, bool f64) {
   I.GRD_x = sg[0], I.GRD_x_pl = sg[1], I.cg = sg[2], I.cg_pl = sg[3], I.rdgz = sg[4], I.afact = sg[5], I.bfact = sg[6];
   I.cg32 = fast.cg32;
   if (!fast.off_ready) {
-    const size_t noff = (size_t)sz.lall * 18 * sz.gall;
+    const size_t noff = (size_t)sz.lall * (kOffPlanes + kFaceGeoPlanes) * sz.gall;
     if (!fast.off32 && cudaMalloc(&fast.off32, noff * sizeof(float)) != cudaSuccess)
       return set_error("cudaMalloc(fast remap offsets)"), ICA_ERR_NOMEM;
     cudaError_t e = fast_build_offsets(I, fast.off32, stream);
@@ -1037,7 +1037,7 @@ int Ctx::fast_inst(FastInst &I, int ntr, double dt, bool f64) {
   I.off32 = fast.off32;
   I.f64 = f64 ? 1 : 0;
   if (f64 && !fast.off64_ready) {
-    const size_t noff = (size_t)sz.lall * 18 * sz.gall;
+    const size_t noff = (size_t)sz.lall * (kOffPlanes + kFaceGeoPlanes) * sz.gall;
     if (!fast.off64 && cudaMalloc(&fast.off64, noff * sizeof(double)) != cudaSuccess)
       return set_error("cudaMalloc(fast remap offsets, FP64)"), ICA_ERR_NOMEM;
     cudaError_t e = fast_build_offsets64(I, fast.off64, stream);

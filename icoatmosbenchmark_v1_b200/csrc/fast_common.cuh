@@ -21,7 +21,10 @@ struct FastInst {
   const double *GMTR_p, *GMTR_t, *GMTR_a, *GRD_xr, *GRD_x, *cg;
   const double *GMTR_p_pl, *GMTR_t_pl, *GMTR_a_pl, *GRD_xr_pl, *GRD_x_pl, *cg_pl;
   const float *cg32;   // coef_grad in FP32, (lall, 3, 7, gall)
-  const float *off32;  // remap offsets GRD_xr - GRD_x per face, FP32, (lall, 18, gall)
+  // remap offsets GRD_xr - GRD_x per face, FP32, (lall, 18, gall), followed by the face
+  // geometry of each column, (lall, 16, gall): TI W1..W3, TJ W1..W3, HN x/y/z of the faces
+  // AI, AIJ, AJ, rarea (fast_face_geo)
+  const float *off32;
   const double *rdgz, *afact, *bfact;
   // fields: FP32 (the FP32 variant) or, when f64 is set, FP64 (the FP64 variant: every face
   // value, bound and limiter in FP64, so the batched step follows the plain FP64 step)
@@ -60,6 +63,13 @@ struct FastInst {
   // grid otherwise), and whether it computes the two pole centres
   int l0, l1, poles;
 };
+
+// Planes of the per-column tables that follow the remap offsets (see FastInst::off32).
+constexpr int kOffPlanes = 18, kFaceGeoPlanes = 16;
+template <typename T>
+__device__ __forceinline__ const T *fast_face_geo(const T *off, const FastInst &I) {
+  return off + (size_t)I.lall * kOffPlanes * I.gall;
+}
 
 // Is point p (region point l*gall + ij, or a pole point after them) computed by instance I?
 __device__ __forceinline__ bool owns_point(const FastInst &I, int p) {

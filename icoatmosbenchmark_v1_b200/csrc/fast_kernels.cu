@@ -342,7 +342,9 @@ __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
 
 // ---- per-face remap offsets GRD_xr - GRD_x of the owner and of the neighbour (FP32),
 // fixed per face, so an interior face value does not depend on the tile that computes it.
-// off32 (lall, 18, gall): [a*6 + x] owner side, [a*6 + 3 + x] neighbour side, a = face 0..2
+// off32 (lall, 18, gall): [a*6 + x] owner side, [a*6 + 3 + x] neighbour side, a = face 0..2.
+// After them the face geometry k_fast_faces reads, in the arithmetic type (lall, 16, gall):
+// TI W1..W3, TJ W1..W3 (GMTR_t), HNX..HNZ of faces AI, AIJ, AJ (GMTR_a), rarea (GMTR_p).
 template <typename T>
 __global__ void k_fast_offsets(FastInst I, T *off) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -354,10 +356,18 @@ __global__ void k_fast_offsets(FastInst I, T *off) {
     const bool nok = ni <= G && nj <= G;
     for (int x = 0; x < 3; ++x) {
       const double xr = gxr(I, l, i, j, a, x + 1);
-      off[((size_t)l * 18 + (a - 1) * 6 + x) * I.gall + c] = (T)(xr - gx(I, l, i, j, x));
-      off[((size_t)l * 18 + (a - 1) * 6 + 3 + x) * I.gall + c] = nok ? (T)(xr - gx(I, l, ni, nj, x)) : T(0);
+      off[((size_t)l * kOffPlanes + (a - 1) * 6 + x) * I.gall + c] = (T)(xr - gx(I, l, i, j, x));
+      off[((size_t)l * kOffPlanes + (a - 1) * 6 + 3 + x) * I.gall + c] = nok ? (T)(xr - gx(I, l, ni, nj, x)) : T(0);
     }
   }
+  T *geo = off + (size_t)I.lall * kOffPlanes * I.gall + (size_t)l * kFaceGeoPlanes * I.gall + c;
+  for (int w = 0; w < 3; ++w) {
+    geo[(size_t)w * I.gall] = (T)gt(I, l, i, j, TI, W1 + w);
+    geo[(size_t)(3 + w) * I.gall] = (T)gt(I, l, i, j, TJ, W1 + w);
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int h = 0; h < 3; ++h) geo[(size_t)(6 + 3 * a + h) * I.gall] = (T)ga(I, l, i, j, a + 1, HNX + h);
+  geo[(size_t)15 * I.gall] = (T)rarea(I, l, i, j);
 }
 
 // Threshold of the upwind masks (0.5 - sign(0.5, ch - EPS)) and of the zero-outflow guards
@@ -385,33 +395,16 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
   const int ii = find_inst(M, w, [](const FastInst &I) { return (long long)(I.l1 - I.l0) * (I.K - 2) * I.gall; });
   if (ii < 0) return;
   const FastInst &I = M.inst[ii];
-  // 32-bit index arithmetic (a 64-bit division is several times the cost of this thread's
-  // work); the host keeps lall * (K - 2) * gall below 2^31
+  // 32-bit index arithmetic throughout (a 64-bit division or product is several times the
+  // cost of this thread's arithmetic); the host keeps 3 * lall * kall * gall below 2^31
   const unsigned wu = (unsigned)w, gall = (unsigned)I.gall, kin = (unsigned)(I.K - 2), Gu = (unsigned)I.G;
   const int G = I.G, c = (int)(wu % gall);
   const unsigned lk = wu / gall;
   const int k = 1 + (int)(lk % kin), l = I.l0 + (int)(lk / kin);
   const int i = (int)((unsigned)c % Gu) + 1, j = (int)((unsigned)c / Gu) + 1;
-  const size_t n3 = (size_t)I.lall * I.K * I.gall, o = ((size_t)l * I.K + k) * I.gall + c;
+  const unsigned n3 = (unsigned)I.lall * (unsigned)I.K * gall, o = ((unsigned)l * (unsigned)I.K + (unsigned)k) * gall + c;
   const R dtf = (R)I.dt;
   auto interior = [&](int a, int b) { return a >= I.gmin && a <= I.gmax && b >= I.gmin && b <= I.gmax; };
-  // rho, rhovx, rhovy, rhovz of cell (a, b) of this slab, in the arithmetic type
-  auto cellf = [&](int a, int b, R f[4]) {
-    const size_t q = ((size_t)l * I.K + k) * I.gall + (size_t)(b - 1) * G + (a - 1);
-    f[0] = (R)I.rho_in[q], f[1] = (R)fld(I, 0, q), f[2] = (R)fld(I, 1, q), f[3] = (R)fld(I, 2, q);
-  };
-  // triangle TI (t = 0: cells (a,b), (a+1,b), (a+1,b+1)) or TJ (t = 1: (a,b), (a+1,b+1), (a,b+1))
-  auto tri = [&](int a, int b, int t, R v[4]) {
-    const R w1 = (R)gt(I, l, a, b, t + 1, W1), w2 = (R)gt(I, l, a, b, t + 1, W2),
-                w3 = (R)gt(I, l, a, b, t + 1, W3);
-    R f0[4], f1[4], f2[4];
-    cellf(a, b, f0);
-    cellf(a + 1, b + 1, t == 0 ? f2 : f1);
-    if (t == 0) cellf(a + 1, b, f1);
-    else cellf(a, b + 1, f2);
-#pragma unroll
-    for (int x = 0; x < 4; ++x) v[x] = f0[x] * w1 + f1[x] * w2 + f2[x] * w3;
-  };
   // faces between interior cells take the FP32 triangle form, seam faces the FP64 value of
   // k_fast_seam; AI = TJ(i,j-1) + TI(i,j), AIJ = TI(i,j) + TJ(i,j), AJ = TJ(i,j) + TI(i-1,j),
   // so the four triangles are formed once each, before any store
@@ -422,11 +415,35 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
     ex[a] = i < G && j < G && face_exists(I, i, j, a + 1);
     inner[a] = ex[a] && interior(i, j) && interior(ni, nj);
   }
+  // the per-column face geometry of this region (see k_fast_offsets) and the fields of the six
+  // cells the four triangles touch: (i,j), (i+1,j), (i+1,j+1), (i,j+1), (i,j-1), (i-1,j); an
+  // inner face has all six inside the region's array
+  const R *geo = fast_face_geo(sizeof(R) == 8 ? (const R *)(const void *)I.off64 : (const R *)(const void *)I.off32, I) +
+                 (unsigned)l * kFaceGeoPlanes * gall + c;
+  auto cellf = [&](int off, R f[4]) {
+    const unsigned q = (unsigned)((int)o + off);
+    f[0] = (R)I.rho_in[q];
+    if (sizeof(R) == 8) f[1] = (R)I.vx64[q], f[2] = (R)I.vy64[q], f[3] = (R)I.vz64[q];
+    else f[1] = (R)I.vx[q], f[2] = (R)I.vy[q], f[3] = (R)I.vz[q];
+  };
+  // triangle value v = f0 w1 + f1 w2 + f2 w3 with the weights at geometry offset gofs
+  auto tri = [&](const R f0[4], const R f1[4], const R f2[4], int gofs, int wp, R v[4]) {
+    const R w1 = geo[(int)wp * (int)gall + gofs], w2 = geo[(int)(wp + 1) * (int)gall + gofs],
+            w3 = geo[(int)(wp + 2) * (int)gall + gofs];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) v[x] = f0[x] * w1 + f1[x] * w2 + f2[x] * w3;
+  };
   R tIij[4] = {}, tJij[4] = {}, tJm[4] = {}, tIm[4] = {};
-  if (inner[0] || inner[1]) tri(i, j, 0, tIij);
-  if (inner[1] || inner[2]) tri(i, j, 1, tJij);
-  if (inner[0]) tri(i, j - 1, 1, tJm);
-  if (inner[2]) tri(i - 1, j, 0, tIm);
+  if (inner[0] || inner[1] || inner[2]) {
+    R f00[4], f10[4], f11[4], f01[4], f0m[4], fm0[4];
+    cellf(0, f00), cellf(1, f10), cellf(G + 1, f11), cellf(G, f01);
+    if (inner[0]) cellf(-G, f0m);
+    if (inner[2]) cellf(-1, fm0);
+    if (inner[0] || inner[1]) tri(f00, f10, f11, 0, 0, tIij);   // TI(i,j)
+    if (inner[1] || inner[2]) tri(f00, f11, f01, 0, 3, tJij);   // TJ(i,j)
+    if (inner[0]) tri(f0m, f10, f00, -G, 3, tJm);               // TJ(i,j-1)
+    if (inner[2]) tri(fm0, f00, f01, -1, 0, tIm);               // TI(i-1,j)
+  }
   double F[3];
   R d[3][3];
 #pragma unroll
@@ -438,36 +455,36 @@ __global__ void k_fast_faces(const __grid_constant__ MultiInst M) {
       const R *q = (a == 0) ? tIij : (a == 1 ? tJij : tIm);
       const R vx = p[1] + q[1], vy = p[2] + q[2], vz = p[3] + q[3];
       const R rr = R(1.0) / A::mx(p[0] + q[0], A::RR_EPS);
-      const R Ff = R(0.5) * (vx * (R)ga(I, l, i, j, a + 1, HNX) + vy * (R)ga(I, l, i, j, a + 1, HNY) +
-                               vz * (R)ga(I, l, i, j, a + 1, HNZ));
+      const R Ff = R(0.5) * (vx * geo[(6 + 3 * a) * gall] + vy * geo[(7 + 3 * a) * gall] + vz * geo[(8 + 3 * a) * gall]);
       F[a] = (double)Ff;
       d[a][0] = -(vx * rr * dtf * R(0.5));
       d[a][1] = -(vy * rr * dtf * R(0.5));
       d[a][2] = -(vz * rr * dtf * R(0.5));
     } else if (ex[a]) {  // seam face
-      const int sid = I.seam_id[((size_t)l * I.gall + c) * 3 + a];
-      F[a] = I.sflux[(size_t)k * I.ns + sid];
+      const int sid = I.seam_id[((unsigned)l * gall + c) * 3 + a];
+      F[a] = I.sflux[(unsigned)k * (unsigned)I.ns + sid];
     }
   }
   // the owner's Courant number of each face and its upwind mask, in the form the tile kernel
   // used to form them (FP32 flux, rarea and 1/rho of the owner), and the upwind side's offset
-  const R ra = (R)rarea(I, l, i, j), rinv = (R)(1.0 / I.rho_in[o]);
+  const R ra = geo[15 * gall], rinv = (R)(1.0 / I.rho_in[o]);
   const R EPSf = eps_thr<R>();
+  const R *offs = (sizeof(R) == 8 ? (const R *)(const void *)I.off64 : (const R *)(const void *)I.off32) +
+                  (unsigned)l * kOffPlanes * gall + c;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    I.Fg[(size_t)a * n3 + o] = F[a];
+    I.Fg[a * n3 + o] = F[a];
     const R chown = ((R)F[a] * ra * dtf) * rinv;
     const bool cm = (R(0.5) - A::sgn(R(0.5), chown - EPSf)) != R(0.0);
     R v[3] = {R(0.0), R(0.0), R(0.0)};
     if (inner[a]) {
-      const size_t ob = ((size_t)l * 18 + a * 6 + (cm ? 3 : 0)) * I.gall + c;
+      const R *ob = offs + (a * 6 + (cm ? 3 : 0)) * gall;
 #pragma unroll
-      for (int x = 0; x < 3; ++x)
-        v[x] = (sizeof(R) == 8 ? (R)I.off64[ob + (size_t)x * I.gall] : (R)I.off32[ob + (size_t)x * I.gall]) + d[a][x];
+      for (int x = 0; x < 3; ++x) v[x] = ob[x * gall] + d[a][x];
     }
-    const R w = cm ? R(1.0) : R(0.0);
-    if (sizeof(R) == 8) I.dupc64[(size_t)a * n3 + o] = make_double4(v[0], v[1], v[2], w);
-    else I.dupc[(size_t)a * n3 + o] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)w);
+    const R wm = cm ? R(1.0) : R(0.0);
+    if (sizeof(R) == 8) I.dupc64[a * n3 + o] = make_double4(v[0], v[1], v[2], wm);
+    else I.dupc[a * n3 + o] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)wm);
   }
 }
 
