@@ -302,17 +302,25 @@ __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
   const double rn = 1.0 / I.rho_in[slab + on];
   const double BIG = DBL_MAX;
   // the tracer's inputs one tracer ahead: the next tracer's loads are issued before this
-  // tracer's store (which the compiler may not move them across)
+  // tracer's store (which the compiler may not move them across).  Per-tracer strides are
+  // applied to base pointers (the index products stay out of the tracer loop).
   double rq[5], rgo[5], rgn[5];
-  auto fetch = [&](int t) {
-    const double *Qt = I.Q_in + t * tstride + slab;
+  const double *Qt = I.Q_in + slab;
+  const size_t bstride = (size_t)I.K * I.nb * 5, vstride = (size_t)I.K * I.ns;
+  const double *bvo = I.bbuf + ((size_t)k * I.nb + (bo >= 0 ? bo : 0)) * 5;
+  const double *bvn = I.bbuf + ((size_t)k * I.nb + (bn >= 0 ? bn : 0)) * 5;
+  auto fetch = [&]() {
 #pragma unroll
     for (int n = 0; n < 4; ++n) rq[n] = Qt[pc[n] - 1];
     rq[4] = Qt[on];
 #pragma unroll
-    for (int x = 0; x < 5; ++x) rgo[x] = bo >= 0 ? bval(I, t, k, bo)[x] : 0.0, rgn[x] = bn >= 0 ? bval(I, t, k, bn)[x] : 0.0;
+    for (int x = 0; x < 5; ++x) rgo[x] = bo >= 0 ? bvo[x] : 0.0, rgn[x] = bn >= 0 ? bvn[x] : 0.0;
+    Qt += tstride, bvo += bstride, bvn += bstride;
   };
-  fetch(0);
+  fetch();
+  const size_t vbase = (size_t)k * I.ns + sidx;
+  float *sv32 = I.f64 ? nullptr : I.sval + vbase;
+  double *sv64 = I.f64 ? I.sval64 + vbase : nullptr;
   for (int t = 0; t < I.ntr; ++t) {
     double qv[4];
 #pragma unroll
@@ -324,7 +332,7 @@ __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
     else go[3] = go[4] = qo;  // halo point no list reaches: Qout = q, grad = 0 (as after the reference fill)
     if (bn >= 0) for (int x = 0; x < 5; ++x) gn[x] = rgn[x];
     else gn[3] = gn[4] = qn;
-    if (t + 1 < I.ntr) fetch(t + 1);
+    if (t + 1 < I.ntr) fetch();
     double vu = qn, vs = qo;
     for (int x = 0; x < 3; ++x) vu = vu + gn[x] * dxn[x];
     for (int x = 0; x < 3; ++x) vs = vs + go[x] * dxo[x];
@@ -335,8 +343,8 @@ __global__ void k_fast_seam(const __grid_constant__ MultiInst M) {
     const double nb_min = cm * BIG + (1.0 - cm) * lo, nb_max = cm * (-BIG) + (1.0 - cm) * hi;
     v = cm * mn64(mx64(v, own_min), own_max) + (1.0 - cm) * mn64(mx64(v, nb_min), nb_max);
     v = cm * mx64(mn64(v, gn[4]), gn[3]) + (1.0 - cm) * mx64(mn64(v, go[4]), go[3]);
-    if (I.f64) I.sval64[((size_t)t * I.K + k) * I.ns + sidx] = v;
-    else I.sval[((size_t)t * I.K + k) * I.ns + sidx] = (float)v;
+    if (I.f64) *sv64 = v, sv64 += vstride;
+    else *sv32 = (float)v, sv32 += vstride;
   }
 }
 
