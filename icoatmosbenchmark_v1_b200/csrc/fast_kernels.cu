@@ -6,8 +6,9 @@
 //                    region-boundary cell and both pole centres, into bbuf.  These
 //                    are exactly the values the reference's two mid-step halo
 //                    exchanges (grad q and Qout, mod_src_tracer.f90:371) would move
-//                    into other regions' halos, so no exchange is needed.  One
-//                    thread per (cell, level): the face geometry once, then the tracers.
+//                    into other regions' halos, so no exchange is needed; the seam
+//                    and pole passes read them.  One thread per (cell, level): the
+//                    face geometry once, then the tracers.
 //   k_fast_seam      FP64 flux and limited value of every seam face (below), all tracers.
 //   k_fast_pole      the two pole centres (horizontal + vertical), FP64.
 //   k_fast_horiz     horizontal sub-step: one CTA per (region tile, level), one thread per
@@ -670,7 +671,13 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
   auto in_tile = [&](int a, int b) { return a >= 0 && a < TX && b >= 0 && b < TY; };
   const bool c_int = in_arr && interior(ci, cj);
   const int bs = in_arr ? I.bsrc[(size_t)l * I.gall + (cj - 1) * G + (ci - 1)] : -3;
-  const bool tile_cell = c_int && bs == -1;  // gradient / Qout formed in the tile
+  // Gradient and Qout are formed in the tile for every interior cell, region-boundary cells
+  // included: their halo neighbours are in the window, and the fluxes and masks of their seam
+  // faces come from k_fast_faces.  The one exception is the corner (gmin, gmin) of a region with
+  // the singular point, whose face-5 bounds take the shifted stencil of the singular point; it
+  // reads its FP64 values from k_fast_boundary.  (Reading every region-boundary cell's values
+  // from that DRAM-resident buffer stalled the edge tiles at every batch barrier.)
+  const bool tile_cell = c_int && !(sgp && ci == I.gmin && cj == I.gmin);
   const bool active = c_int && in_tile(x, y);  // updated by this thread
   const size_t ccell = in_arr ? (size_t)(cj - 1) * G + (ci - 1) : 0;
   const size_t oc = base + ccell;
@@ -834,7 +841,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
     const int ntg = min(TB, ntr - t0);
     if (t0 + TB < ntr) prefetch_batch(t0 + TB);
     // ---- (B) per interior ring cell and tracer: gradient and Qout (formed here, or the FP64
-    // boundary values of a region-boundary cell), the 4-point bounds of its 6 faces, and the
+    // boundary values at a singular corner), the 4-point bounds of its 6 faces, and the
     // limited value of each of its outflow faces; owners fill their seam and absent faces
     if (c_int) {
 #pragma unroll
@@ -882,7 +889,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
             }
             qmn_c[h] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
             qmx_c[h] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
-          } else {  // region-boundary cell: the FP64 boundary values (k_fast_boundary)
+          } else {  // singular corner: the FP64 boundary values (k_fast_boundary)
             const bool okt = 2 * pp + h < ntg;
             const double *bv = bval(I, okt ? t0 + 2 * pp + h : t0, k, bs);
             g[h][0] = okt ? (R)bv[0] : R(0.0);
