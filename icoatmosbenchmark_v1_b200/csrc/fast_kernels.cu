@@ -610,6 +610,15 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *m, int
       "l"((unsigned long long)m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
 }
+// one element global -> shared without a register (cp.async; 4 or 8 bytes, naturally aligned)
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async copies 4, 8 or 16 bytes");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_u32(dst)), "l"(src), "n"((int)sizeof(T))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 template <int TX, int TY, int TB, typename R>
 __device__ __forceinline__ void tile_smem_init(TileSmem<TX, TY, TB, R> &s) {
   if (threadIdx.x == 0) {
@@ -807,8 +816,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
   const int st7[7] = {ew, ew + 1, ew + WW + 1, ew + WW, ew - 1, ew - WW - 1, ew - WW};
   const int fslot[7] = {0, tid, tid, tid, tid - 1, tid - RW - 1, tid - RW};  // owner thread of face m
   auto cx = [](const V2 &v, int h) { return h ? v.y : v.x; };
-  // global values a batch reads that nothing stages: the FP64 boundary values of a region-boundary
-  // cell (5 per tracer) and the seam faces' values; they come from DRAM (bbuf and sval are
+  // the FP64 boundary values a singular corner reads (5 per tracer) come from DRAM (bbuf is
   // larger than L2), so the next batch's are prefetched into L1 one batch ahead
   auto prefetch_batch = [&](int tb) {
     const int nt = min(TB, ntr - tb);
@@ -821,25 +829,30 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
           asm volatile("prefetch.global.L1 [%0];\n" ::"l"(bv + 4));
         }
     }
+  };
+  prefetch_batch(0);
+  const R *svals = (const R *)(sizeof(R) == 8 ? (const void *)I.sval64 : (const void *)I.sval);
+  for (int t0 = 0, b = 0; t0 < ntr; t0 += TB, ++b) {
+    const int ntg = min(TB, ntr - t0);
+    if (t0 + TB < ntr) prefetch_batch(t0 + TB);
+    // seam faces: their values (k_fast_seam) are copied straight into the owner's qa slots,
+    // asynchronously, while phase B runs (no register holds them, and the DRAM latency no
+    // longer sits between phase B and its barrier).  Phase B writes no seam slot; the copies
+    // are waited for before that barrier.
     if (seam_own) {
 #pragma unroll
       for (int a = 0; a < 3; ++a)
         if ((seam_own >> a) & 1u) {
           const int sid = I.seam_id[((size_t)l * I.gall + ccell) * 3 + a];
+          const R *src = svals + ((size_t)t0 * K + k) * I.ns + sid;
+          const size_t tstep = (size_t)K * I.ns;  // next tracer
 #pragma unroll
-          for (int tt = 0; tt < TB; ++tt)
-            if (tt < nt) {
-              const void *pv = (sizeof(R) == 8) ? (const void *)(I.sval64 + ((size_t)(tb + tt) * K + k) * I.ns + sid)
-                                                : (const void *)(I.sval + ((size_t)(tb + tt) * K + k) * I.ns + sid);
-              asm volatile("prefetch.global.L1 [%0];\n" ::"l"(pv));
-            }
+          for (int pp = 0; pp < TP; ++pp) {
+            if (2 * pp < ntg) cp_async_elem(&s.qa[pp][a][tid].x, src + (size_t)(2 * pp) * tstep);
+            if (2 * pp + 1 < ntg) cp_async_elem(&s.qa[pp][a][tid].y, src + (size_t)(2 * pp + 1) * tstep);
+          }
         }
     }
-  };
-  prefetch_batch(0);
-  for (int t0 = 0, b = 0; t0 < ntr; t0 += TB, ++b) {
-    const int ntg = min(TB, ntr - t0);
-    if (t0 + TB < ntr) prefetch_batch(t0 + TB);
     // ---- (B) per interior ring cell and tracer: gradient and Qout (formed here, or the FP64
     // boundary values at a singular corner), the 4-point bounds of its 6 faces, and the
     // limited value of each of its outflow faces; owners fill their seam and absent faces
@@ -920,27 +933,15 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
         }
       }
     }
-    if (seam_own | zero_own) {
+    if (zero_own) {
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
+      for (int a = 0; a < 3; ++a)
         if ((zero_own >> a) & 1u) {
 #pragma unroll
           for (int pp = 0; pp < TP; ++pp) s.qa[pp][a][tid] = A::v2(R(0.0), R(0.0));
-        } else if ((seam_own >> a) & 1u) {
-          const int sid = I.seam_id[((size_t)l * I.gall + ccell) * 3 + a];
-#pragma unroll
-          for (int pp = 0; pp < TP; ++pp) {
-            R v[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-              v[h] = (2 * pp + h < ntg) ? (sizeof(R) == 8 ? (R)I.sval64[((size_t)(t0 + 2 * pp + h) * K + k) * I.ns + sid]
-                                                          : (R)I.sval[((size_t)(t0 + 2 * pp + h) * K + k) * I.ns + sid])
-                                        : R(0.0);
-            s.qa[pp][a][tid] = A::v2(v[0], v[1]);
-          }
         }
-      }
     }
+    cp_async_wait_all();  // this thread's seam copies
     __syncthreads();
     // ---- (D) horizontal update of the tile cells (FP64): rhogq after the horizontal sub-step
     if (active) {
@@ -1430,7 +1431,7 @@ static cudaError_t launch_tile(const MultiInst &M, cudaStream_t st) {
 }
 
 int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax) {
-  static const int shapes[][3] = {{16, 16, 4}, {16, 16, 8}, {16, 16, 2}, {14, 14, 4}, {32, 8, 4}};
+  static const int shapes[][3] = {{16, 16, 4}, {16, 16, 8}, {16, 16, 2}, {14, 14, 4}, {32, 8, 4}, {16, 12, 4}, {12, 16, 4}};
   const int n = sizeof(shapes) / sizeof(shapes[0]);
   if (tx)
     for (int i = 0; i < n; ++i) tx[i] = shapes[i][0], ty[i] = shapes[i][1], tg[i] = shapes[i][2];
@@ -1494,6 +1495,8 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
       case 2: e = launch_tile<16, 16, 2, float>(M, st); break;
       case 3: e = launch_tile<14, 14, 4, float>(M, st); break;
       case 4: e = launch_tile<32, 8, 4, float>(M, st); break;
+      case 5: e = launch_tile<16, 12, 4, float>(M, st); break;
+      case 6: e = launch_tile<12, 16, 4, float>(M, st); break;
       default: return cudaErrorInvalidValue;
     }
   } else {  // FP64 variant: the same tiles, 2 tracers per batch (FP64 shared data and registers)
@@ -1502,6 +1505,8 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
       case 0: case 1: case 2: e = launch_tile<16, 16, 2, double>(M, st); break;
       case 3: e = launch_tile<14, 14, 2, double>(M, st); break;
       case 4: e = launch_tile<32, 8, 2, double>(M, st); break;
+      case 5: e = launch_tile<16, 12, 2, double>(M, st); break;
+      case 6: e = launch_tile<12, 16, 2, double>(M, st); break;
       default: return cudaErrorInvalidValue;
     }
   }
