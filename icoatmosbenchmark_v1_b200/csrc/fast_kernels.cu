@@ -629,11 +629,20 @@ __device__ __forceinline__ void tile_smem_init(TileSmem<TX, TY, TB, R> &s) {
   __syncthreads();
 }
 
+// Does the tile with first cell (i0, j0) need the region-edge code?  An interior tile's ring
+// lies strictly inside [gmin, gmax]^2: every ring cell and its neighbours are interior cells,
+// no face of the tile is a seam face or absent, and the singular corner is not in it.
+template <int TX, int TY>
+__device__ __forceinline__ bool edge_tile(const FastInst &I, int i0, int j0) {
+  return !(i0 - 1 > I.gmin && i0 + TX < I.gmax && j0 - 1 > I.gmin && j0 + TY < I.gmax);
+}
+
 // one work item (tile, level) of instance I; `phase` holds the parity each stage barrier waits
 // for next (bit b: barrier b).  Returns false if a wait for a TMA copy gave up (the error word
 // is set; the caller stops).  I is taken by value and the body inlined once per call site, so
-// every field of I stays a constant-bank operand.
-template <int TX, int TY, int TB, typename R>
+// every field of I stays a constant-bank operand.  EDGE = false is the interior-tile form
+// (edge_tile false): the checks and the seam, absent-face and singular-corner paths compile away.
+template <int TX, int TY, int TB, typename R, bool EDGE>
 __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, const int tile, const int k,
                                            TileSmem<TX, TY, TB, R> &s, unsigned &phase) {
   using A = Arith<R>;
@@ -675,18 +684,20 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
   const int x = ring ? tid % RW - 1 : TX + 8, y = ring ? tid / RW - 1 : TY + 8;
   const int ci = i0 + x, cj = j0 + y;
   const int ew = ring ? (y + 2) * WW + (x + 3) : 0;  // window slot of the cell
-  const bool in_arr = ring && ci >= 1 && ci <= G && cj >= 1 && cj <= G;
-  auto interior = [&](int i, int j) { return i >= I.gmin && i <= I.gmax && j >= I.gmin && j <= I.gmax; };
+  const bool in_arr = EDGE ? ring && ci >= 1 && ci <= G && cj >= 1 && cj <= G : ring;
+  auto interior = [&](int i, int j) {
+    return !EDGE || (i >= I.gmin && i <= I.gmax && j >= I.gmin && j <= I.gmax);
+  };
   auto in_tile = [&](int a, int b) { return a >= 0 && a < TX && b >= 0 && b < TY; };
   const bool c_int = in_arr && interior(ci, cj);
-  const int bs = in_arr ? I.bsrc[(size_t)l * I.gall + (cj - 1) * G + (ci - 1)] : -3;
+  const int bs = (EDGE && in_arr) ? I.bsrc[(size_t)l * I.gall + (cj - 1) * G + (ci - 1)] : -3;
   // Gradient and Qout are formed in the tile for every interior cell, region-boundary cells
   // included: their halo neighbours are in the window, and the fluxes and masks of their seam
   // faces come from k_fast_faces.  The one exception is the corner (gmin, gmin) of a region with
   // the singular point, whose face-5 bounds take the shifted stencil of the singular point; it
   // reads its FP64 values from k_fast_boundary.  (Reading every region-boundary cell's values
   // from that DRAM-resident buffer stalled the edge tiles at every batch barrier.)
-  const bool tile_cell = c_int && !(sgp && ci == I.gmin && cj == I.gmin);
+  const bool tile_cell = c_int && !(EDGE && sgp && ci == I.gmin && cj == I.gmin);
   const bool active = c_int && in_tile(x, y);  // updated by this thread
   const size_t ccell = in_arr ? (size_t)(cj - 1) * G + (ci - 1) : 0;
   const size_t oc = base + ccell;
@@ -756,7 +767,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
       if (need && interior(ci + DX[m], cj + DY[m]) && ((upm >> m) & 1u)) dom |= 1u << m;
     }
   }
-  if (in_arr && x < TX && y < TY) {
+  if (EDGE && in_arr && x < TX && y < TY) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const int nx = x + DX[a + 1], ny = y + DY[a + 1];
@@ -820,7 +831,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
   // larger than L2), so the next batch's are prefetched into L1 one batch ahead
   auto prefetch_batch = [&](int tb) {
     const int nt = min(TB, ntr - tb);
-    if (c_int && !tile_cell) {
+    if (EDGE && c_int && !tile_cell) {
 #pragma unroll
       for (int tt = 0; tt < TB; ++tt)
         if (tt < nt) {
@@ -839,7 +850,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
     // asynchronously, while phase B runs (no register holds them, and the DRAM latency no
     // longer sits between phase B and its barrier).  Phase B writes no seam slot; the copies
     // are waited for before that barrier.
-    if (seam_own) {
+    if (EDGE && seam_own) {
 #pragma unroll
       for (int a = 0; a < 3; ++a)
         if ((seam_own >> a) & 1u) {
@@ -902,7 +913,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
             }
             qmn_c[h] = (c0 - CQmax - qnmax * omc) * rden + c0 * zsw;
             qmx_c[h] = (c0 - CQmin - qnmin * omc) * rden + c0 * zsw;
-          } else {  // singular corner: the FP64 boundary values (k_fast_boundary)
+          } else if (EDGE) {  // singular corner: the FP64 boundary values (k_fast_boundary)
             const bool okt = 2 * pp + h < ntg;
             const double *bv = bval(I, okt ? t0 + 2 * pp + h : t0, k, bs);
             g[h][0] = okt ? (R)bv[0] : R(0.0);
@@ -933,7 +944,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
         }
       }
     }
-    if (zero_own) {
+    if (EDGE && zero_own) {
 #pragma unroll
       for (int a = 0; a < 3; ++a)
         if ((zero_own >> a) & 1u) {
@@ -984,6 +995,16 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
   return ok;
 }
 
+// work item (tile, level) in the form its position needs (uniform over the CTA)
+template <int TX, int TY, int TB, typename R>
+__device__ __forceinline__ bool horiz_tile(const FastInst I, const TileMaps *T, const int tile, const int k,
+                                           TileSmem<TX, TY, TB, R> &s, unsigned &phase) {
+  const int tr = tile % (I.ntx * I.nty);
+  if (edge_tile<TX, TY>(I, I.gmin + (tr % I.ntx) * TX, I.gmin + (tr / I.ntx) * TY))
+    return horiz_item<TX, TY, TB, R, true>(I, T, tile, k, s, phase);
+  return horiz_item<TX, TY, TB, R, false>(I, T, tile, k, s, phase);
+}
+
 template <int TX, int TY, int TB, typename R>
 __device__ __forceinline__ TileSmem<TX, TY, TB, R> &tile_smem(unsigned char *raw) {
   // The dynamic allocation carries 128 bytes of slack for this alignment (TMA destinations).
@@ -1016,17 +1037,18 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
     const int tile = M.inst[ii].l0 * tpr + (int)(wi % ntl), k = 1 + (int)(wi / ntl);
     bool ok;
     switch (ii) {
-      case 0: ok = horiz_item<TX, TY, TB, R>(M.inst[0], &T.m[0], tile, k, s, phase); break;
-      case 1: ok = horiz_item<TX, TY, TB, R>(M.inst[1], &T.m[1], tile, k, s, phase); break;
-      case 2: ok = horiz_item<TX, TY, TB, R>(M.inst[2], &T.m[2], tile, k, s, phase); break;
-      default: ok = horiz_item<TX, TY, TB, R>(M.inst[3], &T.m[3], tile, k, s, phase); break;
+      case 0: ok = horiz_tile<TX, TY, TB, R>(M.inst[0], &T.m[0], tile, k, s, phase); break;
+      case 1: ok = horiz_tile<TX, TY, TB, R>(M.inst[1], &T.m[1], tile, k, s, phase); break;
+      case 2: ok = horiz_tile<TX, TY, TB, R>(M.inst[2], &T.m[2], tile, k, s, phase); break;
+      default: ok = horiz_tile<TX, TY, TB, R>(M.inst[3], &T.m[3], tile, k, s, phase); break;
     }
     // the next item's data overwrite this item's shared data; s_item is reread
     if (__syncthreads_or(!ok)) break;
   }
 }
 
-// one grid: one CTA per (tile, level) (grid x = tile, y = level - 1)
+// one grid: one CTA per (tile, level) (grid x = level - 1, y = tile: the levels of a tile run
+// side by side, so its level-invariant coefficients are read from L2 by all but the first)
 template <int TX, int TY, int TB, typename R>
 __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
     k_fast_horiz1(const __grid_constant__ FastInst I, const __grid_constant__ TileMaps T) {
@@ -1034,7 +1056,7 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
   auto &s = tile_smem<TX, TY, TB, R>(smem_raw);
   tile_smem_init(s);
   unsigned phase = 0;
-  horiz_item<TX, TY, TB, R>(I, &T, I.l0 * I.ntx * I.nty + (int)blockIdx.x, 1 + (int)blockIdx.y, s, phase);
+  horiz_tile<TX, TY, TB, R>(I, &T, I.l0 * I.ntx * I.nty + (int)blockIdx.y, 1 + (int)blockIdx.x, s, phase);
 }
 
 // ---- vertical sub-step: one thread per (interior column, TV tracers), streaming the
@@ -1414,7 +1436,8 @@ static cudaError_t launch_tile_n(const MultiInst &M, cudaStream_t st) {
     nwork += (long long)(M.inst[i].l1 - M.inst[i].l0) * M.inst[i].ntx * M.inst[i].nty * (M.inst[i].K - 2);
   if (ONE) {
     const FastInst &I = M.inst[0];
-    k_fast_horiz1<TX, TY, TB, R><<<dim3((unsigned)((I.l1 - I.l0) * I.ntx * I.nty), (unsigned)(I.K - 2)), NT, smem, st>>>(
+    if ((long long)(I.l1 - I.l0) * I.ntx * I.nty > 65535) return cudaErrorInvalidConfiguration;  // grid y
+    k_fast_horiz1<TX, TY, TB, R><<<dim3((unsigned)(I.K - 2), (unsigned)((I.l1 - I.l0) * I.ntx * I.nty)), NT, smem, st>>>(
         I, T.m[0]);
   } else {
     const long long grid = nwork < (long long)nsm * per_sm[dev] ? nwork : (long long)nsm * per_sm[dev];
