@@ -52,9 +52,10 @@ def measured_traffic(kernel, shape, updates):
     if not p.exists():
         return None, None
     d = json.loads(p.read_text()).get(kernel)
-    if not d or list(d["tile_txtytg"]) != list(shape):
-        return None, None
-    return d["bytes_per_update"] * updates, "ncu " + d["capture"] + ", scaled by updates"
+    for c in (d or {}).get("captures", []):
+        if list(c["tile_txtytg"]) == list(shape):
+            return c["bytes_per_update"] * updates, "ncu " + c["capture"] + ", scaled by updates"
+    return None, None
 
 
 class ClockSampler:
