@@ -644,7 +644,9 @@ __device__ __forceinline__ bool edge_tile(const FastInst &I, int i0, int j0) {
 // (edge_tile false): the checks and the seam, absent-face and singular-corner paths compile away.
 template <int TX, int TY, int TB, typename R, bool EDGE>
 __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, const int tile, const int k,
-                                           TileSmem<TX, TY, TB, R> &s, unsigned &phase) {
+                                           TileSmem<TX, TY, TB, R> &s, unsigned &phase, R (&cgr)[21],
+                                           const bool load_cg = true, const bool pre = false,
+                                           const int knext = -1) {
   using A = Arith<R>;
   using V2 = typename A::V2;
   using V4 = typename A::V4;
@@ -669,7 +671,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
   // TMA coordinates of the window (0-based column, row, slab l*K + k): x = -3, y = -2
   const int wx = i0 - 4, wy = j0 - 3, wsl = l * K + k;
   bool ok = true;
-  if (tid == 0) {  // rhog and the first two batches' rhogq stream in during the set-up below
+  if (tid == 0 && !pre) {  // rhog and the first two batches' rhogq stream in during the set-up below
     mbar_expect_tx(&s.mbar[0], QBYTES + RBYTES);
     tma_load_3d(&s.rho[0], &T->rho, wx, wy, wsl, &s.mbar[0]);
     tma_load_4d(&s.stage[0][0][0], &T->q, wx, wy, wsl, 0, &s.mbar[0]);
@@ -721,12 +723,13 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
     rho_c = I.rho_in[oc], ra64 = rarea(I, l, ci, cj);
   }
   if (active) wk = fld(I, 3, oc), wk1 = fld(I, 3, oc + slab);
-  R cgr[21];
+  if (load_cg) {  // level-invariant: loaded once per CTA (horiz_levels)
 #pragma unroll
-  for (int n = 0; n < 21; ++n)
-    cgr[n] = tile_cell ? (sizeof(R) == 8 ? (R)I.cg[((size_t)l * 21 + n) * I.gall + ccell]
-                                         : (R)I.cg32[((size_t)l * 21 + n) * I.gall + ccell])
-                       : R(0);
+    for (int n = 0; n < 21; ++n)
+      cgr[n] = tile_cell ? (sizeof(R) == 8 ? (R)I.cg[((size_t)l * 21 + n) * I.gall + ccell]
+                                           : (R)I.cg32[((size_t)l * 21 + n) * I.gall + ccell])
+                         : R(0);
+  }
 #pragma unroll
   for (int a = 0; a < 3; ++a) s.dup[a][tid] = d4[a];
   // Courant numbers, upwind sides and the Thuburn outflow sums of the cell
@@ -985,10 +988,22 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
       load_q(nb1);
     }
     __syncthreads();
-    // every read of stage[b & 1] is done: batch b + 2 streams into it
+    // every read of stage[b & 1] is done: batch b + 2 streams into it, or, for an even count of
+    // batches, the next level's batch b + 2 - nbat (with its rhog for the first: the current
+    // level's rhog window was last read when 1/rhog was formed in the set-up)
     if (tid == 0 && b + 2 < nbat) {
       mbar_expect_tx(&s.mbar[b & 1], QBYTES);
       tma_load_4d(&s.stage[b & 1][0][0], &T->q, wx, wy, wsl, (b + 2) * TB, &s.mbar[b & 1]);
+    } else if (tid == 0 && knext >= 0) {
+      const int wsn = l * K + knext;
+      if (b + 2 == nbat) {
+        mbar_expect_tx(&s.mbar[0], QBYTES + RBYTES);
+        tma_load_3d(&s.rho[0], &T->rho, wx, wy, wsn, &s.mbar[0]);
+        tma_load_4d(&s.stage[0][0][0], &T->q, wx, wy, wsn, 0, &s.mbar[0]);
+      } else {
+        mbar_expect_tx(&s.mbar[1], QBYTES);
+        tma_load_4d(&s.stage[1][0][0], &T->q, wx, wy, wsn, TB, &s.mbar[1]);
+      }
     }
   }
   if (!ok && tid == 0) atomicOr(I.err, 1);
@@ -999,10 +1014,27 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
 template <int TX, int TY, int TB, typename R>
 __device__ __forceinline__ bool horiz_tile(const FastInst I, const TileMaps *T, const int tile, const int k,
                                            TileSmem<TX, TY, TB, R> &s, unsigned &phase) {
+  R cgr[21];
   const int tr = tile % (I.ntx * I.nty);
   if (edge_tile<TX, TY>(I, I.gmin + (tr % I.ntx) * TX, I.gmin + (tr / I.ntx) * TY))
-    return horiz_item<TX, TY, TB, R, true>(I, T, tile, k, s, phase);
-  return horiz_item<TX, TY, TB, R, false>(I, T, tile, k, s, phase);
+    return horiz_item<TX, TY, TB, R, true>(I, T, tile, k, s, phase, cgr);
+  return horiz_item<TX, TY, TB, R, false>(I, T, tile, k, s, phase, cgr);
+}
+
+// levels [k0, k1) of a tile in one CTA: the gradient coefficients stay in registers, and (for an
+// even count of tracer batches) each level's first copies are issued as the previous level
+// frees the stage buffers
+template <int TX, int TY, int TB, typename R, bool EDGE>
+__device__ __forceinline__ void horiz_levels(const FastInst &I, const TileMaps *T, const int tile, const int k0,
+                                             const int k1, TileSmem<TX, TY, TB, R> &s, unsigned &phase) {
+  R cgr[21];
+  const int nbat = (I.ntr + TB - 1) / TB;
+  const bool chain = nbat >= 2 && (nbat & 1) == 0;
+  for (int k = k0; k < k1; ++k) {
+    const bool ok = horiz_item<TX, TY, TB, R, EDGE>(I, T, tile, k, s, phase, cgr, k == k0, chain && k > k0,
+                                                    chain && k + 1 < k1 ? k + 1 : -1);
+    if (__syncthreads_or(!ok)) break;  // also: this level's shared data is read before the next set-up
+  }
 }
 
 template <int TX, int TY, int TB, typename R>
@@ -1047,8 +1079,10 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
   }
 }
 
-// one grid: one CTA per (tile, level) (grid x = level - 1, y = tile: the levels of a tile run
-// side by side, so its level-invariant coefficients are read from L2 by all but the first)
+// one grid: one CTA per (tile, kLevelsPerCta consecutive levels) (grid x = level block, y = tile:
+// a tile's level blocks run side by side, so its level-invariant coefficients are read from L2
+// by all but the first, and a CTA keeps them in registers over its levels)
+constexpr int kLevelsPerCta = 8;
 template <int TX, int TY, int TB, typename R>
 __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
     k_fast_horiz1(const __grid_constant__ FastInst I, const __grid_constant__ TileMaps T) {
@@ -1056,7 +1090,12 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
   auto &s = tile_smem<TX, TY, TB, R>(smem_raw);
   tile_smem_init(s);
   unsigned phase = 0;
-  horiz_tile<TX, TY, TB, R>(I, &T, I.l0 * I.ntx * I.nty + (int)blockIdx.y, 1 + (int)blockIdx.x, s, phase);
+  const int tile = I.l0 * I.ntx * I.nty + (int)blockIdx.y, tr = (int)blockIdx.y % (I.ntx * I.nty);
+  const int k0 = 1 + (int)blockIdx.x * kLevelsPerCta, k1 = min(k0 + kLevelsPerCta, I.K - 1);
+  if (edge_tile<TX, TY>(I, I.gmin + (tr % I.ntx) * TX, I.gmin + (tr / I.ntx) * TY))
+    horiz_levels<TX, TY, TB, R, true>(I, &T, tile, k0, k1, s, phase);
+  else
+    horiz_levels<TX, TY, TB, R, false>(I, &T, tile, k0, k1, s, phase);
 }
 
 // ---- vertical sub-step: one thread per (interior column, TV tracers), streaming the
@@ -1437,8 +1476,9 @@ static cudaError_t launch_tile_n(const MultiInst &M, cudaStream_t st) {
   if (ONE) {
     const FastInst &I = M.inst[0];
     if ((long long)(I.l1 - I.l0) * I.ntx * I.nty > 65535) return cudaErrorInvalidConfiguration;  // grid y
-    k_fast_horiz1<TX, TY, TB, R><<<dim3((unsigned)(I.K - 2), (unsigned)((I.l1 - I.l0) * I.ntx * I.nty)), NT, smem, st>>>(
-        I, T.m[0]);
+    k_fast_horiz1<TX, TY, TB, R>
+        <<<dim3((unsigned)((I.K - 2 + kLevelsPerCta - 1) / kLevelsPerCta), (unsigned)((I.l1 - I.l0) * I.ntx * I.nty)),
+           NT, smem, st>>>(I, T.m[0]);
   } else {
     const long long grid = nwork < (long long)nsm * per_sm[dev] ? nwork : (long long)nsm * per_sm[dev];
     e = cudaMemsetAsync(M.inst[0].work_next, 0, sizeof(unsigned long long), st);
