@@ -49,9 +49,10 @@ def test_fast_matches_fp64_oracle(O, glevel, rlevel, kall, ntr, nsteps):
         ctx.close()
 
 
-def test_fast_every_tile_shape(O):
+@pytest.mark.parametrize("ntr", [9, 8])  # odd and even counts of 4-tracer batches (a CTA's levels chain their copies)
+def test_fast_every_tile_shape(O, ntr):
     import torch
-    c = case(5, 0, 12, 9)
+    c = case(5, 0, 12, ntr)
     g, f = c["grid"], c["fields"]
     S = {k: v.copy() for k, v in c["state"].items()}
     O.step(c["dims"], g.have_sgp, c["topo"], c["dt"], S, f, g.arrays, nthreads=8)
