@@ -1507,7 +1507,8 @@ static cudaError_t launch_tile(const MultiInst &M, cudaStream_t st) {
 }
 
 int fast_tile_shapes(int *tx, int *ty, int *tg, int nmax) {
-  static const int shapes[][3] = {{16, 16, 4}, {16, 16, 8}, {16, 16, 2}, {14, 14, 4}, {32, 8, 4}, {16, 12, 4}, {12, 16, 4}};
+  static const int shapes[][3] = {{16, 16, 4}, {16, 16, 8}, {16, 16, 2}, {14, 14, 4}, {32, 8, 4}, {16, 12, 4}, {12, 16, 4},
+                                  {16, 12, 8}};
   const int n = sizeof(shapes) / sizeof(shapes[0]);
   if (tx)
     for (int i = 0; i < n; ++i) tx[i] = shapes[i][0], ty[i] = shapes[i][1], tg[i] = shapes[i][2];
@@ -1573,6 +1574,7 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
       case 4: e = launch_tile<32, 8, 4, float>(M, st); break;
       case 5: e = launch_tile<16, 12, 4, float>(M, st); break;
       case 6: e = launch_tile<12, 16, 4, float>(M, st); break;
+      case 7: e = launch_tile<16, 12, 8, float>(M, st); break;
       default: return cudaErrorInvalidValue;
     }
   } else {  // FP64 variant: the same tiles, 2 tracers per batch (FP64 shared data and registers)
@@ -1583,6 +1585,7 @@ cudaError_t fast_step_multi(const MultiInst &M, int shape, cudaStream_t st, cuda
       case 4: e = launch_tile<32, 8, 2, double>(M, st); break;
       case 5: e = launch_tile<16, 12, 2, double>(M, st); break;
       case 6: e = launch_tile<12, 16, 2, double>(M, st); break;
+      case 7: e = launch_tile<16, 12, 2, double>(M, st); break;
       default: return cudaErrorInvalidValue;
     }
   }
