@@ -11,11 +11,16 @@
 //                    face geometry once, then the tracers.
 //   k_fast_seam      FP64 flux and limited value of every seam face (below), all tracers.
 //   k_fast_pole      the two pole centres (horizontal + vertical), FP64.
-//   k_fast_horiz     horizontal sub-step: one CTA per (region tile, level), one thread per
-//                    cell of the tile and its 1-wide ring; the tracer-independent part
-//                    (triangle values, face fluxes, Courant numbers, upwind masks, remap
-//                    offsets) once, then per batch of TB tracers three phases (q;
-//                    gradient + Qout; limited face values) and the FP64 update.
+//   k_fast_faces     per (owner cell, level): the flux of its three faces (FP32 triangle
+//                    values; the seam pass's FP64 value on seams), the owner-side upwind
+//                    mask and the remap displacement of each face's upwind cell.
+//   k_fast_horiz     horizontal sub-step: one CTA per (region tile, 8 levels; one level per
+//                    work item in the persistent form for batches of grids), one thread per
+//                    cell of the tile and its 1-wide ring; the tracer-independent set-up of a
+//                    level (Courant numbers, outflow faces, Thuburn sums), then per batch of
+//                    TB tracers two phases with a barrier each: every ring cell's gradient,
+//                    Qout, face bounds and the limited values of its outflow faces; then the
+//                    FP64 update of the tile cells and q of the next batch from its TMA window.
 //   k_fast_vert      vertical sub-step: one thread per (column, 4 tracers) streaming the
 //                    levels, limiter two levels behind, FP64 update in place.
 //   k_fast_carry     halo points that no halo list writes keep their input values.
