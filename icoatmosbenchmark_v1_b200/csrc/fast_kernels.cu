@@ -647,7 +647,7 @@ __device__ __forceinline__ bool edge_tile(const FastInst &I, int i0, int j0) {
 // is set; the caller stops).  I is taken by value and the body inlined once per call site, so
 // every field of I stays a constant-bank operand.  EDGE = false is the interior-tile form
 // (edge_tile false): the checks and the seam, absent-face and singular-corner paths compile away.
-template <int TX, int TY, int TB, typename R, bool EDGE>
+template <int TX, int TY, int TB, typename R, bool EDGE, bool BWO = false>
 __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, const int tile, const int k,
                                            TileSmem<TX, TY, TB, R> &s, unsigned &phase, R (&cgr)[21],
                                            const bool load_cg = true, const bool pre = false,
@@ -686,9 +686,27 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
     }
   }
 
-  // this thread's ring cell
-  const bool ring = tid < NR;
-  const int x = ring ? tid % RW - 1 : TX + 8, y = ring ? tid / RW - 1 : TY + 8;
+  // this thread's ring cell, at ring position rp (row-major over the ring).  For 16 x 12 tiles the
+  // tile cells fill warps 0-5 and the ring border warps 6 (bottom row, left column) and 7 (top row,
+  // right column), so a border warp whose cells all lie downstream of the tile (no outflow face
+  // into it) skips phase B and leaves its issue slots to the rest (pair 27.7 -> 26.8 ms at gl8 with
+  // 4 tracers per batch).  Used by the per-level kernel (BWO) for batches of 16 bytes a cell: with
+  // 8 FP32 tracers a batch it measured slower (27.6 against 27.4 ms), and in the persistent kernel
+  // the extra registers spill.
+  constexpr bool kBorderWarps = BWO && TX == 16 && TY == 12 && TB * sizeof(R) == 16;
+  int rp = tid;  // without the border-warp order: thread t takes ring position t (t < NR)
+  if (kBorderWarps) {
+    if (tid < TX * TY) {
+      rp = (tid / TX + 1) * RW + (tid % TX + 1);
+    } else {
+      const int u = tid - TX * TY, v = u & 31;  // u < 30: warp 6, 32 <= u < 62: warp 7
+      if (v >= RW + TY) rp = -1;  // the last two lanes of each border warp
+      else if (u < 32) rp = (v < RW) ? v : (v - RW + 1) * RW;                        // y = -1, x = -1
+      else rp = (v < RW) ? (TY + 1) * RW + v : (v - RW + 1) * RW + (TX + 1);         // y = TY, x = TX
+    }
+  }
+  const bool ring = kBorderWarps ? rp >= 0 : tid < NR;
+  const int x = ring ? rp % RW - 1 : TX + 8, y = ring ? rp / RW - 1 : TY + 8;
   const int ci = i0 + x, cj = j0 + y;
   const int ew = ring ? (y + 2) * WW + (x + 3) : 0;  // window slot of the cell
   const bool in_arr = EDGE ? ring && ci >= 1 && ci <= G && cj >= 1 && cj <= G : ring;
@@ -736,7 +754,8 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
                          : R(0);
   }
 #pragma unroll
-  for (int a = 0; a < 3; ++a) s.dup[a][tid] = d4[a];
+  for (int a = 0; a < 3; ++a)
+    if (!kBorderWarps || ring) s.dup[a][rp] = d4[a];
   // Courant numbers, upwind sides and the Thuburn outflow sums of the cell
   const R ra32 = (R)ra64;
   R chm[7], omc = R(0.0), rden = R(0.0), zsw = R(1.0);
@@ -792,7 +811,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
 #pragma unroll
     for (int m = 1; m <= 6; ++m) {
       const double f = cell_flx(I, l, ci, cj, m, sgp, m <= 3 ? Fo[m - 1] : Fn[m - 4], ra64);
-      s.flx[m - 1][tid] = f;
+      s.flx[m - 1][rp] = f;
       sum = (m == 1) ? f : sum + f;
     }
     const double rho_h = rho_c - sum;
@@ -833,7 +852,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
   __syncthreads();
 
   const int st7[7] = {ew, ew + 1, ew + WW + 1, ew + WW, ew - 1, ew - WW - 1, ew - WW};
-  const int fslot[7] = {0, tid, tid, tid, tid - 1, tid - RW - 1, tid - RW};  // owner thread of face m
+  const int fslot[7] = {0, rp, rp, rp, rp - 1, rp - RW - 1, rp - RW};  // ring position of face m's owner
   auto cx = [](const V2 &v, int h) { return h ? v.y : v.x; };
   // the FP64 boundary values a singular corner reads (5 per tracer) come from DRAM (bbuf is
   // larger than L2), so the next batch's are prefetched into L1 one batch ahead
@@ -867,15 +886,16 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
           const size_t tstep = (size_t)K * I.ns;  // next tracer
 #pragma unroll
           for (int pp = 0; pp < TP; ++pp) {
-            if (2 * pp < ntg) cp_async_elem(&s.qa[pp][a][tid].x, src + (size_t)(2 * pp) * tstep);
-            if (2 * pp + 1 < ntg) cp_async_elem(&s.qa[pp][a][tid].y, src + (size_t)(2 * pp + 1) * tstep);
+            if (2 * pp < ntg) cp_async_elem(&s.qa[pp][a][rp].x, src + (size_t)(2 * pp) * tstep);
+            if (2 * pp + 1 < ntg) cp_async_elem(&s.qa[pp][a][rp].y, src + (size_t)(2 * pp + 1) * tstep);
           }
         }
     }
     // ---- (B) per interior ring cell and tracer: gradient and Qout (formed here, or the FP64
     // boundary values at a singular corner), the 4-point bounds of its 6 faces, and the
-    // limited value of each of its outflow faces; owners fill their seam and absent faces
-    if (c_int) {
+    // limited value of each of its outflow faces; owners fill their seam and absent faces.  In the
+    // border-warp order only cells with an outflow face that touches the tile (dom) take part.
+    if (kBorderWarps ? dom != 0u : c_int) {
 #pragma unroll
       for (int pp = 0; pp < TP; ++pp) {
         V2 q7[7];
@@ -957,7 +977,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
       for (int a = 0; a < 3; ++a)
         if ((zero_own >> a) & 1u) {
 #pragma unroll
-          for (int pp = 0; pp < TP; ++pp) s.qa[pp][a][tid] = A::v2(R(0.0), R(0.0));
+          for (int pp = 0; pp < TP; ++pp) s.qa[pp][a][rp] = A::v2(R(0.0), R(0.0));
         }
     }
     cp_async_wait_all();  // this thread's seam copies
@@ -973,7 +993,7 @@ __device__ __forceinline__ bool horiz_item(const FastInst I, const TileMaps *T, 
       const int dx = kCompactD ? tid % TX : x, dy = kCompactD ? tid / TX : y;
       const int di = i0 + dx, dj = j0 + dy;
       const bool dact = !kCompactD || !EDGE || (di <= I.gmax && dj <= I.gmax);  // a tile cell is >= gmin
-      const int dp = kCompactD ? (dy + 1) * RW + (dx + 1) : tid;  // ring position
+      const int dp = kCompactD ? (dy + 1) * RW + (dx + 1) : rp;  // ring position
       const int dew = kCompactD ? (dy + 2) * WW + (dx + 3) : ew;  // window slot
       const size_t doc = kCompactD ? base + (size_t)(dj - 1) * G + (di - 1) : oc;
       double fx[7];
@@ -1049,8 +1069,8 @@ __device__ __forceinline__ void horiz_levels(const FastInst &I, const TileMaps *
   const int nbat = (I.ntr + TB - 1) / TB;
   const bool chain = nbat >= 2 && (nbat & 1) == 0;
   for (int k = k0; k < k1; ++k) {
-    const bool ok = horiz_item<TX, TY, TB, R, EDGE>(I, T, tile, k, s, phase, cgr, k == k0, chain && k > k0,
-                                                    chain && k + 1 < k1 ? k + 1 : -1);
+    const bool ok = horiz_item<TX, TY, TB, R, EDGE, true>(I, T, tile, k, s, phase, cgr, k == k0,
+                                                          chain && k > k0, chain && k + 1 < k1 ? k + 1 : -1);
     if (__syncthreads_or(!ok)) break;  // also: this level's shared data is read before the next set-up
   }
 }
