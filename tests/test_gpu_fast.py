@@ -28,8 +28,12 @@ def _ctx(grid):
     return ctx
 
 
+# kall 4, 5, 7 and 8 with the others: each way the column kernel's level loop can end (its three
+# window slots for the top level, the remainder levels, no full three-level group at all), with
+# full and partial last tracer groups (5 and 9 tracers: groups of 4 then 1)
 @pytest.mark.parametrize("glevel,rlevel,kall,ntr,nsteps", [(5, 0, 42, 5, 3), (4, 1, 10, 3, 2), (6, 0, 12, 2, 2),
-                                                           (3, 0, 6, 1, 2)])
+                                                           (3, 0, 6, 1, 2), (4, 0, 4, 5, 2), (4, 0, 5, 9, 2),
+                                                           (4, 0, 7, 4, 2), (4, 0, 8, 6, 2)])
 def test_fast_matches_fp64_oracle(O, glevel, rlevel, kall, ntr, nsteps):
     c = case(glevel, rlevel, kall, ntr)
     g, f = c["grid"], c["fields"]
