@@ -1214,8 +1214,9 @@ static int advect_fast_impl(Ctx *c, int ntr, double dt, const double *rhog_in, c
 // chunk c, so a step costs about one pass of the state over the link instead of two, plus the
 // last chunk's way out.  By size: about 1 GiB of rhogq per chunk, 1 to 4 tracers (four
 // tracers are one batch of the horizontal kernel's widest shape).  At glevel 8, kall 96 that
-// is 2 tracers: 434 ms per 32-tracer step on a B200 against 602 ms with 1 tracer per chunk,
-// whose step no longer keeps up with its copies, and 453 ms with 4.
+// is 2 tracers: 405 ms per 32-tracer step on a B200 against 424 ms with 1 tracer per chunk and
+// 423 ms with 4 (on the same GPU; 384-412 ms for 2 tracers across GPUs).  The copies bound it:
+// a chunk's step (about 8 ms for 2 tracers) is shorter than its 23 ms of copies each way.
 static int host_chunk_tracers(const Ctx *c, int ntr) {
   if (c->host_chunk > 0) return std::min(ntr, c->host_chunk);
   const size_t per = (size_t)c->sz.gall * c->sz.kall * c->sz.lall * sizeof(double);
