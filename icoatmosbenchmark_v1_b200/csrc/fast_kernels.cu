@@ -1144,7 +1144,7 @@ __global__ void __launch_bounds__(TileGeo<TX, TY>::NT, (sizeof(R) == 8 ? 1 : 2))
 }
 
 // ---- vertical sub-step: one thread per (interior column, TV tracers), streaming the
-// levels with the limiter two levels behind and the next level's loads in flight; FP32
+// levels with the limiter two levels behind and the next two levels' inputs in flight; FP32
 // limiter, FP64 update.  rhogq after the horizontal sub-step is read from (and the result
 // written to) Q_out; the threads of the first tracer group also finish rhog.
 // The tracer groups of a column block are consecutive blocks, so they run together and
