@@ -147,6 +147,25 @@ __global__ void k_adj_vrho(Dims D, double *a_rho, double *a_rho_pl, double *a_rh
 //   ck1(k) = -w(k) dt rdgz(k) / rh(k), ck2(k) = w(k+1) dt rdgz(k) / rh(k), ck1(kall) likewise
 //   qh(k) = afact(k) qc(k) + bfact(k) qc(k-1), clamped to the Qout bounds of level k-1 or k
 //   Q(k) = Qh(k) - (w(k+1) qh(k+1) - w(k) qh(k)) dt rdgz(k), ghosts copied
+// The column adjoint's per-level inputs stream through a shared-memory ring of kAdjStages
+// levels, filled by each thread's own cp.async copies (no barrier: a thread reads only what it
+// copied), so kAdjStages - 1 levels of a column are in flight while a level is worked on
+// (a 4-step sweep at gl7, 4 tracers: 124.2 -> 118.5 ms against plain loads of each level).
+constexpr int kAdjStages = 4, kAdjThreads = 128;
+struct AdjRing {
+  double v[kAdjStages][6][kAdjThreads];  // Qh(kk), rh(kk), rh(k), w(k), w(k+1), aQ(k)
+};
+__device__ __forceinline__ unsigned adj_smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void adj_cp8(double *dst, const double *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(adj_smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void adj_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void adj_drain() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void adj_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 struct VLev {  // one level's inputs
   double qc, R, w, c1, c2, aO;
 };
@@ -231,7 +250,7 @@ __device__ __forceinline__ void vlim_level_adj(const VLim &v, double qm, double 
   ac2 += a2;
 }
 
-__global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const double *__restrict__ Qh,
+__global__ void __launch_bounds__(kAdjThreads) k_adj_vert(Dims D, double dt, const double *__restrict__ Qh,
                                                   const double *__restrict__ rh, const double *__restrict__ w,
                                                   double *__restrict__ aQ, double *__restrict__ a_rh,
                                                   const double *__restrict__ Qh_pl, const double *__restrict__ rh_pl,
@@ -258,17 +277,39 @@ __global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const doubl
   const int K = D.kall, kmin = D.kmin, kmax = D.kmax;  // 1-based levels below
   auto X = [&](int k) { return (size_t)(k - 1) * s; };
   const double aTop = AQ[X(K)], aBot = AQ[X(1)];
+  extern __shared__ __align__(16) unsigned char adj_raw[];
+  AdjRing &ring = *reinterpret_cast<AdjRing *>(adj_raw);
+  const int th = threadIdx.x;
+  // the levels are taken in the order K, K-1, ..., 1: level j's inputs into slot j % kAdjStages
+  auto issue = [&](int j) {
+    if (j >= 1) {
+      const int sl = j % kAdjStages, kk = (j < kmin) ? kmin : ((j > kmax) ? kmax : j);
+      adj_cp8(&ring.v[sl][0][th], QH + X(kk));
+      adj_cp8(&ring.v[sl][1][th], R + X(kk));
+      adj_cp8(&ring.v[sl][2][th], R + X(j));
+      adj_cp8(&ring.v[sl][3][th], W + X(j));
+      adj_cp8(&ring.v[sl][4][th], W + X(j < K ? j + 1 : K));
+      adj_cp8(&ring.v[sl][5][th], AQ + X(j));
+    }
+    adj_commit();
+  };
+#pragma unroll
+  for (int d = 0; d < kAdjStages - 1; ++d) issue(K - d);
   auto level = [&](int k) {
+    adj_wait<kAdjStages - 2>();  // level k's copies are complete
+    const int sl = k % kAdjStages;
+    const double vq = ring.v[sl][0][th], vrk = ring.v[sl][1][th], vr = ring.v[sl][2][th];
+    const double vw = ring.v[sl][3][th], vw1 = ring.v[sl][4][th], va = ring.v[sl][5][th];
+    issue(k - (kAdjStages - 1));  // into the slot of level k + 1, read in the previous call
     VLev v;
-    const int kk = (k < kmin) ? kmin : ((k > kmax) ? kmax : k);
-    v.qc = QH[X(kk)] / R[X(kk)];
-    v.R = R[X(k)];
-    v.w = W[X(k)];
+    v.qc = vq / vrk;
+    v.R = vr;
+    v.w = vw;
     v.c1 = v.c2 = v.aO = 0.0;
     if (k >= kmin && k <= kmax) {
       v.c1 = -v.w * dt * rdgz[k - 1] / v.R;
-      v.c2 = W[X(k + 1)] * dt * rdgz[k - 1] / v.R;
-      double a = AQ[X(k)];
+      v.c2 = vw1 * dt * rdgz[k - 1] / v.R;
+      double a = va;
       if (k == kmax) a = a + aTop;
       if (k == kmin) a = a + aBot;
       v.aO = a;
@@ -362,6 +403,7 @@ __global__ void __launch_bounds__(128) k_adj_vert(Dims D, double dt, const doubl
   }
   AQ[X(1)] = 0.0;
   AQ[X(K)] = 0.0;
+  adj_drain();
 }
 
 // ---------------------------------------------------------------------------
@@ -1013,7 +1055,7 @@ int step_adjoint(StepCtx &S, const AdjScratch &A, int ntr, double dt, const doub
     k_adj_qh<<<slab(D, T), T, 0, st>>>(D, S.q, S.qa, S.qout, S.cm, S.flx, Q, A.Qh);
     k_adj_qh_pl<<<nbl, 128, 0, st>>>(D.kall, S.qa_pl, S.cm_pl, S.qout_pl, S.qin_pl, S.flx_pl, Qp, A.Qh_pl);
     // vertical sub-step: aQ becomes the adjoint of rhogq after the horizontal sub-step
-    k_adj_vert<<<(ncol + 127) / 128, 128, 0, st>>>(D, dt, A.Qh, A.rh, w, aQ, A.a_rh, A.Qh_pl, A.rh_pl, w_pl, aQp,
+    k_adj_vert<<<(ncol + kAdjThreads - 1) / kAdjThreads, kAdjThreads, (int)sizeof(AdjRing), st>>>(D, dt, A.Qh, A.rh, w, aQ, A.a_rh, A.Qh_pl, A.rh_pl, w_pl, aQp,
                                                    A.a_rh_pl, S.rdgz, S.afact, S.bfact);
     cudaMemsetAsync(A.a_q, 0, n3 * B, st);
     cudaMemsetAsync(A.a_q_pl, 0, n3p * B, st);
